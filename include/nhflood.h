@@ -1,0 +1,163 @@
+/*
+ * nhflood — B200 (sm_100a) local-inertial flood step, C ABI.
+ *
+ * Drop-in boundary for the Taichi fields, kernels and compiled ti.graph
+ * inside the reference's _evolve (nh-flood-2d,
+ * src/nh_flood_2d/core/solver_compact.py:179-1008). The reference has no
+ * FFI of its own: every entry point below replaces one host call on a
+ * Taichi field or kernel, cited beside it. A Python host binds it with
+ * ctypes (nhflood/native.py); INTEGRATION.md shows the binding.
+ *
+ * Conventions
+ *  - Arrays keep the reference's layout: cell and side index 0 is the
+ *    exterior sentinel (README.md:407); face CSR is [cells][4] in
+ *    l, r, b, t order (preprocess/domain.py:83-174); topology is
+ *    [sides][3] = (orient, lower, higher) (preprocess/domain.py:452-460).
+ *  - Large arrays are DEVICE pointers owned by the caller (for example
+ *    torch CUDA tensors) and must stay alive until nhf_destroy. Scalars,
+ *    forcing coefficients, clock words, traces and budget totals are HOST
+ *    pointers.
+ *  - All device work is ordered after the caller's stream (given at
+ *    nhf_create) and the caller's stream is ordered after it, so tensors
+ *    written by the caller are visible to the next call and vice versa.
+ *  - Every function returns NHF_OK (0) or a negative NHF_E* code; the
+ *    message is in nhf_last_error(handle) (or nhf_last_error(NULL) when
+ *    creation failed). Device clock statuses are reported, as in the
+ *    reference, in column 3 of the batch trace (core/clock.py:42-46).
+ *  - One host thread per handle; handles on different streams may run
+ *    concurrently.
+ */
+#ifndef NHFLOOD_H
+#define NHFLOOD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NHF_OK 0
+#define NHF_EINVAL (-1)
+#define NHF_ECUDA (-2)
+#define NHF_ENOMEM (-3)
+#define NHF_ESTATE (-4)
+
+/* Trace columns: the reference's nine (core/clock.py:35-40) plus the number
+ * of wet cells (depth >= min_h, solver_compact.py:359) after the step. */
+#define NHF_TRACE_COLS 10
+#define NHF_MAX_BATCH 64
+
+/* Clock status values in trace column 3 (core/clock.py:42-46). */
+#define NHF_STEP_DONE 0
+#define NHF_STEP_COMPLETED 1
+#define NHF_STEP_BAD_CFL 2
+#define NHF_STEP_BAD_DT 3
+#define NHF_STEP_OVERSHOOT 4
+
+typedef struct nhf_mesh {
+    int32_t e_num;      /* cells including sentinel 0 */
+    int32_t s_num;      /* sides including sentinel 0 */
+    int32_t b_num;      /* boundaries (level or discharge) */
+    int32_t n_rates;    /* unique rain pixels */
+    int32_t isl_len;    /* length of isl_data */
+    int32_t hang_cells; /* hanging-edge gradient cells (0: aligned mesh) */
+    int32_t hang_edges; /* hanging edges */
+    /* static cell arrays [e_num], device */
+    const float *x, *y, *area, *width, *height;
+    const float *f0, *fc, *k; /* Horton, m/s and 1/h (hydraulics.py:63-93) */
+    const float *weight;      /* boundary cell weight */
+    const int32_t *boundary_id, *rain_index;
+    const int32_t *face_ptr, *face_count; /* [e_num*4] */
+    const int32_t *isl_data;              /* [isl_len] */
+    /* static side arrays [s_num], device */
+    const int32_t *topology; /* [s_num*3] */
+    const float *length, *side_n;
+    const uint8_t *sbf; /* 1 = closed exterior side */
+    /* boundaries [max(1,b_num)], device: 0 level, 1 discharge */
+    const int32_t *kind;
+    /* theta < 1 only: open-face fractions [e_num*4], device (NULL if theta == 1) */
+    const float *open_face;
+    /* hanging-edge reconstruction (core/pressure.py:19-45), device */
+    const int32_t *edge_index; /* [s_num] */
+    const float *offsets;      /* [hang_edges*2] */
+    const int32_t *slots;      /* [hang_edges*2] */
+    const int32_t *hcells;     /* [hang_cells] */
+    const int32_t *axes;       /* [hang_cells*2] */
+    /* mutable state, device */
+    float *bed, *depth, *q, *rain_time, *infiltration, *max_depth, *max_speed, *u, *v;
+    uint32_t *peak_hi, *peak_lo;
+} nhf_mesh;
+
+typedef struct nhf_params {
+    float g;          /* 9.81 */
+    float afa;        /* Courant number */
+    float sita;       /* theta time weighting */
+    float min_h;      /* wet threshold */
+    float min_dt;     /* F32(1e-4) CFL floor (solver_compact.py:31) */
+    int32_t batch_size; /* steps per batch, 1..64 (clock.py:48-51) */
+} nhf_params;
+
+typedef struct nhf_handle nhf_handle;
+
+/* Allocate the step's scratch (donor factors, reductions, budget partials,
+ * clock control block, trace) and capture nothing yet. `stream` is the
+ * caller's cudaStream_t (NULL: legacy default stream). Replaces the field
+ * allocation and ti.graph build in solver_compact.py:209-336,894-909. */
+int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf_handle **out);
+int nhf_destroy(nhf_handle *h);
+const char *nhf_last_error(const nhf_handle *h);
+const char *nhf_version(void);
+
+/* initialize() (solver_compact.py:398-410): depth = 0, infiltration = f0,
+ * per-side centre distance. */
+int nhf_initialize(nhf_handle *h);
+/* Clock words (clock.py:60-69): set after a checkpoint restore. */
+int nhf_set_clock(nhf_handle *h, const uint32_t now[2]);
+int nhf_get_clock(nhf_handle *h, uint32_t now[2]);
+/* clock.active[None] = 1 before the first compute_cfl (solver_compact.py:884). */
+int nhf_set_active(nhf_handle *h, int32_t active);
+/* upload_forcing (solver_compact.py:769-790): coefficients [max(1,b_num)][2]
+ * F32 and rain rates [n_rates] F32, both host; rain_rates may be NULL to keep
+ * the previous rates. */
+int nhf_set_forcing(nhf_handle *h, const float *coefficients, const float *rain_rates, int32_t raining);
+/* apply_initial_levels (solver_compact.py:412-420, 876-883): targets is a
+ * device [e_num] F32 array; the level diagnostics enter the budget. */
+int nhf_apply_initial_levels(nhf_handle *h, const float *targets);
+/* compute_cfl (solver_compact.py:617-641). */
+int nhf_compute_cfl(nhf_handle *h);
+/* initial_diagnostics (solver_compact.py:657-672). */
+int nhf_initial_diagnostics(nhf_handle *h);
+/* reset_extrema (solver_compact.py:674-679). */
+int nhf_reset_extrema(nhf_handle *h);
+/* clock.begin + graph.run + clock.read_trace (clock.py:75-92,187-203;
+ * solver_compact.py:939-942): runs batch_size prepare/tick/cfl/finish steps
+ * towards `target` ticks with batch origin `origin` (two U32 words each,
+ * host) and copies the [batch_size][NHF_TRACE_COLS] trace to `trace` (host).
+ * Synchronous. */
+int nhf_run_batch(nhf_handle *h, const uint32_t target[2], const uint32_t origin[2], uint32_t *trace);
+/* Same batch without the host synchronisation: the trace stays on the
+ * device until nhf_read_trace (which synchronises). */
+int nhf_run_batch_async(nhf_handle *h, const uint32_t target[2], const uint32_t origin[2]);
+int nhf_read_trace(nhf_handle *h, uint32_t *trace);
+/* DeviceBudget.flush (device_budget.py:68-84): adds this interval's FP64
+ * per-block partials into totals[4 + 6*b_num] (host) and clears them. */
+int nhf_budget_flush(nhf_handle *h, double *totals);
+int nhf_budget_terms(const nhf_handle *h);
+/* ndt_t / cfl_arg_t / flow_depth_t[cfl_arg] (solver_compact.py:644-655). */
+int nhf_get_cfl(nhf_handle *h, float *ndt, int32_t *arg, float *flow_depth);
+/* limit_value_t / limit_ids_t (solver_compact.py:330-331,839,854). */
+int nhf_limits(nhf_handle *h, float values[5], int32_t ids[3]);
+int nhf_reset_limits(nhf_handle *h);
+/* sample_stations (solver_compact.py:681-687): ids host [n], out host [n][4]
+ * = depth, level, u, v. */
+int nhf_sample_stations(nhf_handle *h, const int32_t *ids, int32_t n, float *out);
+/* Face flux sums eq_t [e_num][4] (device destination). */
+int nhf_read_eq(nhf_handle *h, float *eq);
+/* Hanging-edge gradients [hang_cells][2] (device destination). */
+int nhf_read_gradients(nhf_handle *h, float *gradients);
+int nhf_synchronize(nhf_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

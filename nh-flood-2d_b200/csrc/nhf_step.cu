@@ -1,0 +1,1208 @@
+// nhflood: local-inertial step of the nh-flood-2d compact solver on sm_100a.
+//
+// One physical step follows the reference's global passes
+// (solver_compact.py:364-391 prepare/finish, 422-613 tick, 617-641 CFL):
+//   k_prepare   clock choice, boundary values, limiting-edge snapshot
+//   k_pressure  hanging-edge tangential gradients (multi-resolution meshes)
+//   k_face_qn   length-weighted face discharge (theta < 1 only)
+//   k_sides     theta-weighted momentum with semi-implicit Manning friction
+//   k_donor     per-cell positivity donor factor
+//   k_scale     q *= donor factor of the upwind cell
+//   k_cells     fluxes, rain, Horton, depth update, level cells, extrema,
+//               FP64 per-block budget partials, wet count
+//   k_cfl       CFL packed (value, side) minimum; the last block commits the
+//               clock and writes the trace row
+// A batch of up to 64 steps plus the begin/trace copies is captured once into
+// a CUDA graph and replayed per batch. Every scalar the steps need (dt, clock
+// words, boundary values) lives in a device control block, so the graph is
+// static. Arithmetic follows the reference's F32 operation order; the build
+// uses --fmad=false so that the CPU restatement reproduces every bit.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "../../include/nhflood.h"
+#include "nhf_math.cuh"
+
+namespace {
+
+constexpr int kBlock = 256;          // budget block = reference ei // 256
+constexpr float kDh = -999.0f;       // dh_t without gates (solver_compact.py:405)
+constexpr uint32_t kSnapTicks = 1099512u;  // ceil(1e-6 * 2**40) (clock.py:11)
+constexpr unsigned long long kCflEmpty = 0xFFFFFFFFFFFFFFFFULL;
+
+struct Ctl {
+    uint32_t now[2], next[2], origin[2], step_end[2];
+    float dt, local, end_local, ndt;
+    int32_t active, slot, raining, cfl_arg;
+    uint32_t limited_cells, limited_faces, min_scale_bits, wet;
+    unsigned long long cfl_packed;
+    uint32_t done_blocks;
+    uint32_t pad;
+    float limit_value[5];
+    int32_t limit_ids[3];
+    uint32_t trace[NHF_MAX_BATCH * NHF_TRACE_COLS];
+};
+
+struct Dev {
+    nhf_mesh m;
+    float g, neg_g, afa, sita, half_rest, seven_thirds, min_h, min_dt;
+    int32_t terms, blocks, batch_size, theta_one;
+    Ctl *ctl;
+    const float *coef;
+    float *values, *level_values, *rain_rates, *sdc, *donor_scale, *face_qn, *eq, *gradients;
+    double *acc_sum, *acc_comp;
+    const uint32_t *begin;  // device copy of {next_hi, next_lo, origin_hi, origin_lo}
+};
+
+__device__ __forceinline__ float maxf(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float minf(float a, float b) { return b < a ? b : a; }
+
+// ---------------------------------------------------------------- reductions
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long w = __shfl_down_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+
+// Canonical pairwise tree over the 256 cells of one budget block:
+// slot i += slot i + stride for stride 128 .. 1. Returns the sum in thread 0.
+__device__ double block_tree(double v, double *sh)
+{
+    const int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int stride = 128; stride >= 32; stride >>= 1) {
+        if (t < stride) sh[t] += sh[t + stride];
+        __syncthreads();
+    }
+    double r = 0.0;
+    if (t < 32) {
+        r = sh[t];
+        for (int stride = 16; stride >= 1; stride >>= 1) r += __shfl_down_sync(0xffffffffu, r, stride);
+    }
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ void acc_add(double *sum, double *comp, double p)
+{
+    double s0 = *sum;
+    double s = s0 + p;
+    double bp = s - s0;
+    double err = (s0 - (s - bp)) + (p - bp);
+    *comp += err;
+    *sum = s;
+}
+
+// --------------------------------------------------------------- small kernels
+
+__global__ void k_initialize(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 1 && i < m.e_num) {
+        m.depth[i] = 0.0f;
+        m.infiltration[i] = m.f0[i];
+    }
+    if (i >= 1 && i < m.s_num) {
+        int so = m.topology[3 * i], el = m.topology[3 * i + 1], eh = m.topology[3 * i + 2];
+        d.sdc[i] = so == 2 ? maxf(fabsf(m.x[eh] - m.x[el]), 0.01f) : maxf(fabsf(m.y[eh] - m.y[el]), 0.01f);
+    }
+}
+
+__global__ void k_begin(Dev d)
+{
+    Ctl *c = d.ctl;
+    int t = threadIdx.x;
+    if (t == 0) {
+        c->next[0] = d.begin[0]; c->next[1] = d.begin[1];
+        c->origin[0] = d.begin[2]; c->origin[1] = d.begin[3];
+        c->slot = 0;
+    }
+    for (int i = t; i < NHF_MAX_BATCH * NHF_TRACE_COLS; i += blockDim.x) c->trace[i] = 0u;
+}
+
+// Recompute flow_depth_t[si] (solver_compact.py:628-630) from the unchanged
+// state; side 0 keeps the field's initial zero.
+__device__ __forceinline__ float flow_depth_of(const nhf_mesh &m, int si)
+{
+    if (si == 0) return 0.0f;
+    int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
+    float head = maxf(m.bed[el] + m.depth[el], m.bed[eh] + m.depth[eh]);
+    return maxf(head - maxf(maxf(m.bed[el], m.bed[eh]), kDh), 0.01f);
+}
+
+__device__ void clock_choose(const Dev &d, Ctl *c, float candidate, int slot)
+{
+    uint32_t *row = c->trace + slot * NHF_TRACE_COLS;
+    c->active = 0; c->dt = 0.0f; c->local = 0.0f; c->end_local = 0.0f;
+    uint32_t now_hi = c->now[0], now_lo = c->now[1];
+    uint32_t target_hi = c->next[0], target_lo = c->next[1];
+    if (!(now_hi < target_hi || (now_hi == target_hi && now_lo < target_lo))) return;
+    if (!(candidate >= d.min_dt)) { row[3] = NHF_STEP_BAD_CFL; return; }
+    uint32_t borrow = now_lo > target_lo ? 1u : 0u;
+    uint32_t rem_hi = target_hi - now_hi - borrow;
+    uint32_t rem_lo = target_lo - now_lo;
+    float remaining = __uint2float_rn(rem_hi) * (1.0f / 256.0f) + __uint2float_rn(rem_lo) * 0x1p-40f;
+    float chosen = minf(minf(candidate, 1.0f), remaining);
+    row[4] = __float_as_uint(candidate);
+    row[5] = chosen < minf(candidate, 1.0f) ? 1u : 0u;
+    uint32_t bits = __float_as_uint(chosen);
+    int exponent = (int)((bits >> 23) & 255u) - 127;
+    uint32_t mantissa = (bits & 0x7fffffu) | 0x800000u;
+    uint32_t dt_hi = 0, dt_lo = 0;
+    if (!(chosen > 0.0f) || exponent < -40 || exponent > 0) { row[3] = NHF_STEP_BAD_DT; return; }
+    int shift = exponent + 17;
+    if (shift >= 0) {
+        dt_lo = mantissa << shift;
+        if (shift >= 9) dt_hi = mantissa >> (32 - shift);
+    } else {
+        int right = -shift;
+        dt_lo = mantissa >> right;
+        uint32_t dropped = mantissa & ((1u << right) - 1u);
+        uint32_t half = 1u << (right - 1);
+        if (dropped > half || (dropped == half && (dt_lo & 1u) != 0)) dt_lo += 1;
+    }
+    if (dt_hi == 0 && dt_lo == 0) { row[3] = NHF_STEP_BAD_DT; return; }
+    bool exceeds = dt_hi > rem_hi || (dt_hi == rem_hi && dt_lo > rem_lo);
+    uint32_t diff_hi, diff_lo;
+    if (exceeds) {
+        diff_hi = dt_hi - rem_hi - (dt_lo < rem_lo ? 1u : 0u);
+        diff_lo = dt_lo - rem_lo;
+    } else {
+        diff_hi = rem_hi - dt_hi - (rem_lo < dt_lo ? 1u : 0u);
+        diff_lo = rem_lo - dt_lo;
+    }
+    uint32_t end_hi = now_hi, end_lo = now_lo;
+    if (diff_hi == 0 && diff_lo < kSnapTicks) { end_hi = target_hi; end_lo = target_lo; }
+    else if (exceeds) { row[3] = NHF_STEP_OVERSHOOT; return; }
+    else {
+        end_lo = now_lo + dt_lo;
+        end_hi = now_hi + dt_hi + (end_lo < now_lo ? 1u : 0u);
+    }
+    uint32_t origin_hi = c->origin[0], origin_lo = c->origin[1];
+    uint32_t local_hi = now_hi - origin_hi - (now_lo < origin_lo ? 1u : 0u);
+    uint32_t local_lo = now_lo - origin_lo;
+    uint32_t end_local_hi = end_hi - origin_hi - (end_lo < origin_lo ? 1u : 0u);
+    uint32_t end_local_lo = end_lo - origin_lo;
+    c->local = __uint2float_rn(local_hi) * (1.0f / 256.0f) + __uint2float_rn(local_lo) * 0x1p-40f;
+    c->end_local = __uint2float_rn(end_local_hi) * (1.0f / 256.0f) + __uint2float_rn(end_local_lo) * 0x1p-40f;
+    c->dt = chosen;
+    c->step_end[0] = end_hi; c->step_end[1] = end_lo;
+    c->active = 1;
+}
+
+// prepare_step (solver_compact.py:364-382)
+__global__ void k_prepare(Dev d)
+{
+    if (threadIdx.x != 0) return;
+    Ctl *c = d.ctl;
+    const nhf_mesh &m = d.m;
+    clock_choose(d, c, c->ndt, c->slot);
+    if (!c->active) return;
+    c->limited_cells = 0; c->limited_faces = 0;
+    c->min_scale_bits = __float_as_uint(1.0f);
+    c->wet = 0;
+    for (int bi = 0; bi < m.b_num; ++bi) {
+        d.values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * (c->local + c->dt / 2.0f);
+        d.level_values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * c->end_local;
+    }
+    if (c->ndt < c->limit_value[0]) {
+        int si = c->cfl_arg;
+        int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
+        float h = flow_depth_of(m, si);
+        c->limit_value[0] = c->ndt;
+        c->limit_value[1] = m.depth[el]; c->limit_value[2] = m.depth[eh];
+        c->limit_value[3] = h;
+        c->limit_value[4] = m.q[si] / maxf(h, 1e-30f);
+        c->limit_ids[0] = si; c->limit_ids[1] = el; c->limit_ids[2] = eh;
+    }
+}
+
+// ------------------------------------------------------ pressure (pressure.py)
+
+__device__ void face_difference(const Dev &d, int cell, int direction, int axis,
+                                float &value_out, float &distance_out, int &usable_out)
+{
+    const nhf_mesh &m = d.m;
+    float value = 0.0f, distance = 0.0f, total = 0.0f;
+    int usable = 1;
+    float eta = m.bed[cell] + m.depth[cell];
+    int start = m.face_ptr[4 * cell + direction];
+    int count = m.face_count[4 * cell + direction];
+    for (int j = 0; j < count; ++j) {
+        int side = m.isl_data[start + j];
+        int other = m.topology[3 * side + 1] + m.topology[3 * side + 2] - cell;
+        if (other == 0 || m.depth[other] <= d.min_h) {
+            usable = 0;
+        } else {
+            float weight = m.length[side];
+            value += weight * ((m.bed[other] + m.depth[other]) - eta);
+            float delta = axis == 1 ? m.y[other] - m.y[cell] : m.x[other] - m.x[cell];
+            distance += weight * delta;
+            total += weight;
+        }
+    }
+    if (total > 0.0f) { value /= total; distance /= total; }
+    else usable = 0;
+    value_out = value; distance_out = distance; usable_out = usable;
+}
+
+__global__ void k_pressure(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    if (!d.ctl->active) return;
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= m.hang_cells) return;
+    int cell = m.hcells[slot];
+    for (int axis = 0; axis < 2; ++axis) {
+        if (m.axes[2 * slot + axis] != 1) continue;
+        float value = 0.0f;
+        if (m.depth[cell] > d.min_h) {
+            int minus = axis == 1 ? 2 : 0, plus = axis == 1 ? 3 : 1;
+            float dm, xm, dp, xp; int okm, okp;
+            face_difference(d, cell, minus, axis, dm, xm, okm);
+            face_difference(d, cell, plus, axis, dp, xp, okp);
+            if (okm && okp) value = (dp - dm) / (xp - xm);
+            else if (okm) value = dm / xm;
+            else if (okp) value = dp / xp;
+        }
+        d.gradients[2 * slot + axis] = value;
+    }
+}
+
+__device__ __forceinline__ float pressure_difference(const Dev &d, int side, int lower, int higher, float raw)
+{
+    const nhf_mesh &m = d.m;
+    float result = raw;
+    int index = m.edge_index[side];
+    if (index >= 0 && m.depth[lower] > d.min_h && m.depth[higher] > d.min_h) {
+        int axis = m.topology[3 * side] == 2 ? 1 : 0;
+        float o0 = m.offsets[2 * index], o1 = m.offsets[2 * index + 1];
+        if (o0 != 0.0f) result -= d.gradients[2 * m.slots[2 * index] + axis] * o0;
+        if (o1 != 0.0f) result += d.gradients[2 * m.slots[2 * index + 1] + axis] * o1;
+    }
+    return result;
+}
+
+// ----------------------------------------------------------- theta < 1 faces
+
+__global__ void k_face_qn(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    if (!d.ctl->active) return;
+    int ei = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ei >= m.e_num) return;
+    for (int dd = 0; dd < 4; ++dd) {
+        int start = m.face_ptr[4 * ei + dd], count = m.face_count[4 * ei + dd];
+        float result = 0.0f;
+        if (count == 1) {
+            result = m.q[m.isl_data[start]];
+        } else if (count > 1) {
+            float total = 0.0f, width = 0.0f;
+            for (int o = 0; o < count; ++o) {
+                int side = m.isl_data[start + o];
+                total += m.q[side] * m.length[side];
+                width += m.length[side];
+            }
+            result = total / width;
+        }
+        d.face_qn[4 * ei + dd] = result;
+    }
+}
+
+__device__ __forceinline__ float boundary_neighbor_sum(float q, float left, float right, float lext, float rext)
+{
+    float result = left + right;
+    if (lext > 0.0f || rext > 0.0f) {
+        if (lext == 1.0f || rext == 1.0f) {
+            result = 2.0f * q;
+        } else {
+            float product = lext * rext;
+            result = ((1.0f - rext) * left + (1.0f - lext) * right
+                      + 2.0f * q * (lext + rext - 2.0f * product)) / (1.0f - product);
+        }
+    }
+    return result;
+}
+
+// ------------------------------------------------------------ side momentum
+
+// tick side loop (solver_compact.py:439-486)
+template <bool kHanging, bool kThetaOne>
+__global__ void k_sides(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    int si = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (si >= m.s_num) return;
+    const Ctl *c = d.ctl;
+    if (!c->active) return;
+    const float dt = c->dt;
+    float bf = m.sbf[si] == 1 ? 0.0f : 1.0f;
+    int so = m.topology[3 * si], el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
+    float zl = m.bed[el], zh = m.bed[eh];
+    float hl = zl + m.depth[el], hr = zh + m.depth[eh];
+    float dx = d.sdc[si];
+    float xq = m.q[si];
+    float xwh = maxf(hl, hr) - maxf(maxf(zl, zh), kDh);
+    float difference = hr - hl;
+    if (kHanging) difference = pressure_difference(d, si, el, eh, difference);
+    float xdq = (d.neg_g * difference / dx) * maxf(xwh, 0.0f) * dt;
+    float n = m.side_n[si];
+    float ratio = 0.0f;
+    // xq / p with p = max(wh, 1e-5) ** f32(7/3) > 0: a zero discharge gives a
+    // zero ratio without evaluating the power (identical bits).
+    if (xq != 0.0f) ratio = xq / nhf::pow_f32(maxf(xwh, 0.00001f), d.seven_thirds);
+    float xf = 1.0f + d.g * dt * (n * n) * fabsf(ratio);
+    int dl = so == 2 ? 0 : 2, dr = so == 2 ? 1 : 3;
+    float nb;
+    if (kThetaOne) {
+        nb = 0.0f + 0.0f;
+    } else {
+        nb = boundary_neighbor_sum(xq, d.face_qn[4 * el + dl], d.face_qn[4 * eh + dr],
+                                   m.open_face[4 * el + dl], m.open_face[4 * eh + dr]);
+    }
+    float new_q = (d.sita * xq + d.half_rest * nb + xdq) / xf;
+    new_q = xwh < d.min_h ? 0.0f : new_q;
+    new_q *= bf;
+    m.q[si] = new_q;
+}
+
+// ----------------------------------------------------------- donor factor
+
+// tick cell loop 1 (solver_compact.py:491-514)
+__global__ void k_donor(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    Ctl *c = d.ctl;
+    int ei = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    bool valid = ei < m.e_num;
+    if (!c->active) return;
+    const float dt = c->dt;
+    bool limited = false;
+    float sc = 1.0f;
+    if (valid) {
+        int bi = m.boundary_id[ei];
+        float discharge = 0.0f;
+        int kind = bi >= 0 ? m.kind[bi] : -1;
+        if (kind == 1) discharge = d.values[bi] * m.weight[ei];
+        float rainq = 0.0f;
+        if (c->raining) rainq = d.rain_rates[m.rain_index[ei]];
+        float pipe = 0.0f;
+        float positive = (maxf(pipe, 0.0f) + maxf(discharge, 0.0f)) * dt;
+        float area = m.area[ei];
+        float available = m.depth[ei] * area + positive + rainq * dt * area;
+        float outgoing = (maxf(-pipe, 0.0f) + maxf(-discharge, 0.0f)) * dt;
+        for (int dd = 0; dd < 4; ++dd) {
+            int p = m.face_ptr[4 * ei + dd], cnt = m.face_count[4 * ei + dd];
+            for (int j = 0; j < cnt; ++j) {
+                int side = m.isl_data[p + j];
+                float signed_q = m.q[side] * m.length[side];
+                if (dd == 0 || dd == 2) signed_q = -signed_q;
+                outgoing += maxf(signed_q, 0.0f) * dt;
+            }
+        }
+        if (outgoing > available && kind != 0) {
+            sc = available / outgoing;
+            limited = true;
+        }
+        d.donor_scale[ei] = sc;
+    }
+    unsigned mask = __ballot_sync(0xffffffffu, limited);
+    if (mask) {
+        uint32_t bits = __float_as_uint(sc);  // scale >= 0: bit order is value order
+        for (int o = 16; o > 0; o >>= 1) {
+            uint32_t w = __shfl_down_sync(0xffffffffu, bits, o);
+            bits = w < bits ? w : bits;
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&c->limited_cells, (uint32_t)__popc(mask));
+            atomicMin(&c->min_scale_bits, bits);
+        }
+    }
+}
+
+// ------------------------------------------------------------ side scaling
+
+// tick side loop 2 (solver_compact.py:516-522)
+__global__ void k_scale(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    Ctl *c = d.ctl;
+    int si = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (!c->active) return;
+    bool counted = false;
+    if (si < m.s_num) {
+        int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
+        float q = m.q[si];
+        int donor = q >= 0.0f ? el : eh;
+        float sc = d.donor_scale[donor];
+        counted = q != 0.0f && sc < 1.0f;
+        m.q[si] = q * sc;
+    }
+    unsigned mask = __ballot_sync(0xffffffffu, counted);
+    if (mask && (threadIdx.x & 31) == 0) atomicAdd(&c->limited_faces, (uint32_t)__popc(mask));
+}
+
+// ------------------------------------------------------------- cell update
+
+// tick cell loops 2 and 3 (solver_compact.py:525-610) for one 256-cell budget
+// block; the per-block budget partials have one writer.
+__global__ void __launch_bounds__(kBlock) k_cells(Dev d)
+{
+    __shared__ double sh[kBlock];
+    const nhf_mesh &m = d.m;
+    Ctl *c = d.ctl;
+    if (!c->active) return;
+    const float dt = c->dt;
+    const int T = d.terms;
+    const int B = m.b_num;
+    const int blk = blockIdx.x;
+    const int ei = blk * kBlock + threadIdx.x;
+    const bool valid = ei >= 1 && ei < m.e_num;
+    float t_removed = 0.0f, t_pipe = 0.0f, t_floor = 0.0f;
+    float t_level[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    float t_discharge = 0.0f;
+    int bi = -1, kind = -1;
+    bool wet = false;
+    if (valid) {
+        bi = m.boundary_id[ei];
+        kind = bi >= 0 ? m.kind[bi] : -1;
+        float sc = d.donor_scale[ei];
+        float pq = 0.0f;
+        float pipe = maxf(pq, 0.0f) + minf(pq, 0.0f) * sc;
+        float discharge = 0.0f;
+        if (kind == 1) {
+            float requested = d.values[bi] * m.weight[ei];
+            discharge = maxf(requested, 0.0f) + minf(requested, 0.0f) * sc;
+            t_discharge = discharge * dt;
+        }
+        float ssq = pipe + discharge;
+        float rainq = 0.0f;
+        if (c->raining) rainq = d.rain_rates[m.rain_index[ei]];
+        float infil = m.infiltration[ei];
+        if (rainq > 0.0f) {
+            float rt = m.rain_time[ei] + dt;
+            m.rain_time[ei] = rt;
+            float f0 = m.f0[ei], fc = m.fc[ei];
+            float diff = f0 - fc;
+            // fc + 0 * e == fc for the finite e in (0, 1]: skip exp when f0 == fc.
+            infil = diff == 0.0f ? fc + 0.0f : fc + diff * nhf::exp_f32(-m.k[ei] * rt / 3600.0f);
+            m.infiltration[ei] = infil;
+        }
+        float fl[4];
+        for (int dd = 0; dd < 4; ++dd) {
+            float face_flux = 0.0f;
+            int p = m.face_ptr[4 * ei + dd], cnt = m.face_count[4 * ei + dd];
+            for (int j = 0; j < cnt; ++j) {
+                int si = m.isl_data[p + j];
+                face_flux += m.q[si] * m.length[si];
+            }
+            fl[dd] = face_flux;
+        }
+        float ql = fl[0], qr = fl[1], qb = fl[2], qt = fl[3];
+        float tq = ql - qr + qb - qt + ssq;
+        reinterpret_cast<float4 *>(d.eq)[ei] = make_float4(ql, qr, qb, qt);
+        float ea = m.area[ei];
+        float rain_depth = rainq * dt;
+        float increment = tq * dt / ea + rain_depth;
+        float previous = m.depth[ei];
+        float raw_depth = previous + increment;
+        float removed = minf(infil * dt, maxf(raw_depth, 0.0f));
+        raw_depth -= removed;
+        float floor_v = maxf(-raw_depth, 0.0f);
+        t_removed = removed * ea;
+        t_pipe = pipe * dt;
+        float depth;
+        if (kind == 0) {
+            t_floor = floor_v * ea;
+            float target = maxf(d.level_values[bi] - m.bed[ei], 0.0f);
+            t_level[0] = (target - previous) * ea;
+            t_level[1] = -(ql - qr + qb - qt) * dt;
+            t_level[2] = -pipe * dt;
+            t_level[3] = -rain_depth * ea;
+            t_level[4] = removed * ea;
+            depth = target;
+        } else {
+            t_floor = floor_v * ea;
+            depth = maxf(raw_depth, 0.0f);
+        }
+        m.depth[ei] = depth;
+        float h = maxf(depth, 0.01f);
+        float u = 0.0f, v = 0.0f;
+        if (depth >= d.min_h) {
+            u = (ql + qr) / m.height[ei] / h / 2.0f;
+            v = (qb + qt) / m.width[ei] / h / 2.0f;
+        }
+        m.u[ei] = u; m.v[ei] = v;
+        m.max_speed[ei] = maxf(m.max_speed[ei], sqrtf(u * u + v * v));
+        if (depth > m.max_depth[ei]) {
+            m.max_depth[ei] = depth;
+            m.peak_hi[ei] = c->step_end[0]; m.peak_lo[ei] = c->step_end[1];
+        }
+        wet = depth >= d.min_h;
+    }
+    int wet_count = __syncthreads_count(wet);
+    if (threadIdx.x == 0 && wet_count) atomicAdd(&c->wet, (uint32_t)wet_count);
+
+    double *acc_s = d.acc_sum + (size_t)blk * T;
+    double *acc_c = d.acc_comp + (size_t)blk * T;
+    for (int t = 0; t < T; ++t) {
+        float val = 0.0f;
+        if (t == 0) val = t_removed;
+        else if (t == 1) val = kind == 0 ? 0.0f : t_floor;
+        else if (t == 2) val = kind == 0 ? t_floor : 0.0f;
+        else if (t == 3) val = t_pipe;
+        else if (t < 4 + 5 * B) { int b = (t - 4) / 5; if (b == bi) val = t_level[(t - 4) % 5]; }
+        else { int b = t - 4 - 5 * B; if (b == bi) val = t_discharge; }
+        if (!__syncthreads_or(val != 0.0f)) continue;
+        double sum = block_tree((double)val, sh);
+        if (threadIdx.x == 0) acc_add(acc_s + t, acc_c + t, sum);
+    }
+}
+
+// --------------------------------------------------------------------- CFL
+
+__device__ void finish_step(const Dev &d, Ctl *c)
+{
+    uint32_t *row = c->trace + c->slot * NHF_TRACE_COLS;
+    if (c->active) {
+        row[6] = c->limited_cells;
+        row[7] = c->limited_faces;
+        row[8] = c->min_scale_bits;
+        row[9] = c->wet;
+        c->now[0] = c->step_end[0]; c->now[1] = c->step_end[1];
+        row[0] = __float_as_uint(c->dt);
+        row[1] = c->step_end[0]; row[2] = c->step_end[1];
+        row[3] = NHF_STEP_COMPLETED;
+    }
+    c->slot += 1;
+}
+
+// compute_cfl (solver_compact.py:617-641) + finish_step (384-391).
+// Packed key (cfl bits << 32 | side): the minimum is the smallest CFL and,
+// among equal values, the lowest side id, as the reference's second pass.
+__global__ void k_cfl(Dev d, int finish)
+{
+    __shared__ unsigned long long sh[32];
+    __shared__ bool last;
+    const nhf_mesh &m = d.m;
+    Ctl *c = d.ctl;
+    if (!c->active) {
+        if (finish && blockIdx.x == 0 && threadIdx.x == 0) c->slot += 1;
+        return;
+    }
+    unsigned long long best = kCflEmpty;
+    for (int si = blockIdx.x * blockDim.x + threadIdx.x + 1; si < m.s_num; si += gridDim.x * blockDim.x) {
+        int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
+        if (el != 0 && eh != 0) {
+            float zl = m.bed[el], zh = m.bed[eh];
+            float head = maxf(zl + m.depth[el], zh + m.depth[eh]);
+            float h = maxf(head - maxf(maxf(zl, zh), kDh), 0.01f);
+            float cfl = d.afa * m.length[si] / (sqrtf(d.g * h) + fabsf(m.q[si]) / h);
+            unsigned long long key = ((unsigned long long)__float_as_uint(cfl) << 32) | (unsigned)si;
+            best = key < best ? key : best;
+        }
+    }
+    best = warp_min_u64(best);
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sh[warp] = best;
+    __syncthreads();
+    if (warp == 0) {
+        best = lane < (int)(blockDim.x >> 5) ? sh[lane] : kCflEmpty;
+        best = warp_min_u64(best);
+        if (lane == 0) {
+            if (best != kCflEmpty) atomicMin(&c->cfl_packed, best);
+            __threadfence();
+            unsigned ticket = atomicAdd(&c->done_blocks, 1u);
+            last = ticket == gridDim.x - 1;
+        }
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    unsigned long long packed = atomicExch(&c->cfl_packed, kCflEmpty);
+    c->done_blocks = 0;
+    if (packed == kCflEmpty) {
+        c->ndt = __uint_as_float(0x7f800000u);
+        c->cfl_arg = 0;
+    } else {
+        c->ndt = __uint_as_float((uint32_t)(packed >> 32));
+        c->cfl_arg = (int32_t)(packed & 0xffffffffu);
+    }
+    if (finish) finish_step(d, c);
+}
+
+// ------------------------------------------------------- setup and sampling
+
+// apply_initial_levels (solver_compact.py:412-420)
+__global__ void __launch_bounds__(kBlock) k_apply_levels(Dev d, const float *targets)
+{
+    __shared__ double sh[kBlock];
+    const nhf_mesh &m = d.m;
+    const int T = d.terms;
+    int blk = blockIdx.x, ei = blk * kBlock + threadIdx.x;
+    int bi = -1;
+    float val = 0.0f;
+    if (ei >= 1 && ei < m.e_num) {
+        bi = m.boundary_id[ei];
+        if (bi >= 0 && m.kind[bi] == 0) {
+            float previous = m.depth[ei];
+            m.depth[ei] = targets[ei];
+            val = (targets[ei] - previous) * m.area[ei];
+        } else {
+            bi = -1;
+        }
+    }
+    for (int b = 0; b < m.b_num; ++b) {
+        float v = b == bi ? val : 0.0f;
+        if (!__syncthreads_or(v != 0.0f)) continue;
+        double sum = block_tree((double)v, sh);
+        int t = 4 + 5 * b;
+        if (threadIdx.x == 0) acc_add(d.acc_sum + (size_t)blk * T + t, d.acc_comp + (size_t)blk * T + t, sum);
+    }
+}
+
+// initial_diagnostics (solver_compact.py:657-672)
+__global__ void k_initial_diag(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    int ei = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (ei >= m.e_num) return;
+    float fl[4];
+    for (int dd = 0; dd < 4; ++dd) {
+        float total = 0.0f;
+        int p = m.face_ptr[4 * ei + dd], cnt = m.face_count[4 * ei + dd];
+        for (int j = 0; j < cnt; ++j) {
+            int si = m.isl_data[p + j];
+            total += m.q[si] * m.length[si];
+        }
+        fl[dd] = total;
+    }
+    reinterpret_cast<float4 *>(d.eq)[ei] = make_float4(fl[0], fl[1], fl[2], fl[3]);
+    float depth = m.depth[ei];
+    float h = maxf(depth, 0.01f);
+    float u = 0.0f, v = 0.0f;
+    if (depth >= d.min_h) {
+        u = (fl[0] + fl[1]) / m.height[ei] / h / 2.0f;
+        v = (fl[2] + fl[3]) / m.width[ei] / h / 2.0f;
+    }
+    m.u[ei] = u; m.v[ei] = v;
+    m.max_speed[ei] = maxf(m.max_speed[ei], sqrtf(u * u + v * v));
+    if (depth > m.max_depth[ei]) {
+        m.max_depth[ei] = depth;
+        m.peak_hi[ei] = d.ctl->now[0]; m.peak_lo[ei] = d.ctl->now[1];
+    }
+}
+
+// reset_extrema (solver_compact.py:674-679)
+__global__ void k_reset_extrema(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    int ei = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (ei >= m.e_num) return;
+    m.max_depth[ei] = m.depth[ei];
+    float u = m.u[ei], v = m.v[ei];
+    m.max_speed[ei] = sqrtf(u * u + v * v);
+    m.peak_hi[ei] = d.ctl->now[0]; m.peak_lo[ei] = d.ctl->now[1];
+}
+
+// sample_stations (solver_compact.py:681-687)
+__global__ void k_sample(Dev d, const int32_t *ids, int n, float *out)
+{
+    const nhf_mesh &m = d.m;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int ei = ids[i];
+    out[4 * i + 0] = m.depth[ei];
+    out[4 * i + 1] = m.bed[ei] + m.depth[ei];
+    out[4 * i + 2] = m.u[ei];
+    out[4 * i + 3] = m.v[ei];
+}
+
+__global__ void k_cfl_edge(Dev d, float *out)
+{
+    const Ctl *c = d.ctl;
+    out[0] = c->ndt;
+    out[1] = __int_as_float(c->cfl_arg);
+    out[2] = flow_depth_of(d.m, c->cfl_arg);
+}
+
+}  // namespace
+
+// ============================================================== host side
+
+struct nhf_handle {
+    nhf_mesh m{};
+    nhf_params p{};
+    Dev dev{};
+    cudaStream_t user = nullptr, s = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    Ctl *ctl = nullptr;
+    void *scratch = nullptr;
+    uint32_t *h_begin = nullptr;  // pinned {next, origin}
+    uint32_t *d_begin = nullptr;
+    uint32_t *h_trace = nullptr;  // pinned
+    float *h_small = nullptr;     // pinned staging for forcing / scalars
+    double *h_acc = nullptr;      // pinned budget staging
+    int32_t *d_ids = nullptr;
+    float *d_samples = nullptr;
+    int ids_cap = 0;
+    cudaGraphExec_t graph = nullptr;
+    std::string err;
+};
+
+namespace {
+
+std::string g_create_error;
+
+int fail(nhf_handle *h, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf; else g_create_error = buf;
+    return code;
+}
+
+#define CK(h, call)                                                                         \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail((h), NHF_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_));    \
+    } while (0)
+
+inline int grid_for(int n, int b) { return n <= 0 ? 1 : (n + b - 1) / b; }
+
+int enter(nhf_handle *h)
+{
+    CK(h, cudaEventRecord(h->ev_in, h->user));
+    CK(h, cudaStreamWaitEvent(h->s, h->ev_in, 0));
+    return NHF_OK;
+}
+
+int leave(nhf_handle *h)
+{
+    CK(h, cudaGetLastError());
+    CK(h, cudaEventRecord(h->ev_out, h->s));
+    CK(h, cudaStreamWaitEvent(h->user, h->ev_out, 0));
+    return NHF_OK;
+}
+
+void enqueue_step(nhf_handle *h)
+{
+    const Dev &d = h->dev;
+    const nhf_mesh &m = h->m;
+    cudaStream_t s = h->s;
+    k_prepare<<<1, 32, 0, s>>>(d);
+    if (m.hang_cells > 0) k_pressure<<<grid_for(m.hang_cells, 256), 256, 0, s>>>(d);
+    if (!d.theta_one) k_face_qn<<<grid_for(m.e_num, 256), 256, 0, s>>>(d);
+    int gs = grid_for(m.s_num - 1, 256);
+    if (m.hang_cells > 0) {
+        if (d.theta_one) k_sides<true, true><<<gs, 256, 0, s>>>(d);
+        else k_sides<true, false><<<gs, 256, 0, s>>>(d);
+    } else {
+        if (d.theta_one) k_sides<false, true><<<gs, 256, 0, s>>>(d);
+        else k_sides<false, false><<<gs, 256, 0, s>>>(d);
+    }
+    k_donor<<<grid_for(m.e_num - 1, 256), 256, 0, s>>>(d);
+    k_scale<<<gs, 256, 0, s>>>(d);
+    k_cells<<<d.blocks, kBlock, 0, s>>>(d);
+    int gc = grid_for(m.s_num - 1, 256);
+    if (gc > 148 * 8) gc = 148 * 8;
+    k_cfl<<<gc, 256, 0, s>>>(d, 1);
+}
+
+int build_graph(nhf_handle *h)
+{
+    cudaGraph_t g = nullptr;
+    CK(h, cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(h->d_begin, h->h_begin, 4 * sizeof(uint32_t), cudaMemcpyHostToDevice, h->s);
+    k_begin<<<1, 256, 0, h->s>>>(h->dev);
+    for (int i = 0; i < h->p.batch_size; ++i) enqueue_step(h);
+    cudaMemcpyAsync(h->h_trace, h->ctl->trace, sizeof(uint32_t) * NHF_TRACE_COLS * h->p.batch_size,
+                    cudaMemcpyDeviceToHost, h->s);
+    cudaError_t e = cudaStreamEndCapture(h->s, &g);
+    if (e != cudaSuccess) return fail(h, NHF_ECUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(h, NHF_ECUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    return NHF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *nhf_version(void) { return "nhflood-b200 0.1 (sm_100a)"; }
+
+const char *nhf_last_error(const nhf_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf_handle **out)
+{
+    if (!mesh || !params || !out) return fail(nullptr, NHF_EINVAL, "null argument");
+    *out = nullptr;
+    if (mesh->e_num < 1 || mesh->s_num < 1 || mesh->b_num < 0 || mesh->n_rates < 0)
+        return fail(nullptr, NHF_EINVAL, "invalid mesh sizes");
+    if (params->batch_size < 1 || params->batch_size > NHF_MAX_BATCH)
+        return fail(nullptr, NHF_EINVAL, "batch_size must be between 1 and %d", NHF_MAX_BATCH);
+    if (params->sita != 1.0f && !mesh->open_face)
+        return fail(nullptr, NHF_EINVAL, "theta < 1 needs open_face fractions");
+    if (mesh->hang_cells > 0 && (!mesh->edge_index || !mesh->offsets || !mesh->slots || !mesh->hcells || !mesh->axes))
+        return fail(nullptr, NHF_EINVAL, "hanging geometry arrays missing");
+    nhf_handle *h = new nhf_handle();
+    h->m = *mesh;
+    h->p = *params;
+    h->user = (cudaStream_t)stream;
+    int rc;
+#define CKC(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) {                                                                    \
+            rc = fail(nullptr, NHF_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_));          \
+            nhf_destroy(h);                                                                         \
+            return rc;                                                                              \
+        }                                                                                           \
+    } while (0)
+    CKC(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
+    CKC(cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
+    CKC(cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming));
+    const int e = mesh->e_num, sn = mesh->s_num, bb = mesh->b_num > 0 ? mesh->b_num : 1;
+    const int T = 4 + 6 * mesh->b_num;
+    const int blocks = (e + kBlock - 1) / kBlock;
+    const int hc = mesh->hang_cells > 0 ? mesh->hang_cells : 1;
+    const int nr = mesh->n_rates > 0 ? mesh->n_rates : 1;
+    const bool theta_one = params->sita == 1.0f;
+    // scratch layout (bytes, 256-aligned pieces)
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
+    size_t o_ctl = take(sizeof(Ctl));
+    size_t o_coef = take(sizeof(float) * 2 * bb);
+    size_t o_val = take(sizeof(float) * bb);
+    size_t o_lvl = take(sizeof(float) * bb);
+    size_t o_rain = take(sizeof(float) * nr);
+    size_t o_sdc = take(sizeof(float) * sn);
+    size_t o_donor = take(sizeof(float) * e);
+    size_t o_fqn = take(theta_one ? 16 : sizeof(float) * 4 * (size_t)e);
+    size_t o_eq = take(sizeof(float) * 4 * (size_t)e);
+    size_t o_grad = take(sizeof(float) * 2 * hc);
+    size_t o_accs = take(sizeof(double) * (size_t)blocks * T);
+    size_t o_accc = take(sizeof(double) * (size_t)blocks * T);
+    size_t o_begin = take(sizeof(uint32_t) * 4);
+    CKC(cudaMalloc(&h->scratch, off));
+    CKC(cudaMemsetAsync(h->scratch, 0, off, h->s));
+    char *base = (char *)h->scratch;
+    h->ctl = (Ctl *)(base + o_ctl);
+    h->d_begin = (uint32_t *)(base + o_begin);
+    CKC(cudaMallocHost(&h->h_begin, 4 * sizeof(uint32_t)));
+    CKC(cudaMallocHost(&h->h_trace, sizeof(uint32_t) * NHF_TRACE_COLS * NHF_MAX_BATCH));
+    CKC(cudaMallocHost(&h->h_small, sizeof(float) * (2 * bb + nr + 64)));
+    CKC(cudaMallocHost(&h->h_acc, sizeof(double) * 2 * (size_t)blocks * T + 16));
+    Dev &d = h->dev;
+    d.m = *mesh;
+    d.g = params->g;
+    d.neg_g = -params->g;
+    d.afa = params->afa;
+    d.sita = params->sita;
+    d.half_rest = (float)((1.0 - (double)params->sita) / 2.0);
+    d.seven_thirds = (float)(7.0 / 3.0);
+    d.min_h = params->min_h;
+    d.min_dt = params->min_dt;
+    d.terms = T;
+    d.blocks = blocks;
+    d.batch_size = params->batch_size;
+    d.theta_one = theta_one ? 1 : 0;
+    d.ctl = h->ctl;
+    d.coef = (const float *)(base + o_coef);
+    d.values = (float *)(base + o_val);
+    d.level_values = (float *)(base + o_lvl);
+    d.rain_rates = (float *)(base + o_rain);
+    d.sdc = (float *)(base + o_sdc);
+    d.donor_scale = (float *)(base + o_donor);
+    d.face_qn = (float *)(base + o_fqn);
+    d.eq = (float *)(base + o_eq);
+    d.gradients = (float *)(base + o_grad);
+    d.acc_sum = (double *)(base + o_accs);
+    d.acc_comp = (double *)(base + o_accc);
+    d.begin = h->d_begin;
+    // control block initial values
+    Ctl init{};
+    init.limit_value[0] = __builtin_inff();
+    init.cfl_packed = kCflEmpty;
+    init.ndt = 0.0f;
+    CKC(cudaMemcpyAsync(h->ctl, &init, sizeof(Ctl), cudaMemcpyHostToDevice, h->s));
+    CKC(cudaStreamSynchronize(h->s));
+#undef CKC
+    *out = h;
+    return NHF_OK;
+}
+
+int nhf_destroy(nhf_handle *h)
+{
+    if (!h) return NHF_OK;
+    if (h->s) cudaStreamSynchronize(h->s);
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->scratch) cudaFree(h->scratch);
+    if (h->h_begin) cudaFreeHost(h->h_begin);
+    if (h->h_trace) cudaFreeHost(h->h_trace);
+    if (h->h_small) cudaFreeHost(h->h_small);
+    if (h->h_acc) cudaFreeHost(h->h_acc);
+    if (h->d_ids) cudaFree(h->d_ids);
+    if (h->d_samples) cudaFree(h->d_samples);
+    if (h->ev_in) cudaEventDestroy(h->ev_in);
+    if (h->ev_out) cudaEventDestroy(h->ev_out);
+    if (h->s) cudaStreamDestroy(h->s);
+    delete h;
+    return NHF_OK;
+}
+
+int nhf_initialize(nhf_handle *h)
+{
+    if (!h) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    int n = h->m.e_num > h->m.s_num ? h->m.e_num : h->m.s_num;
+    k_initialize<<<grid_for(n, 256), 256, 0, h->s>>>(h->dev);
+    return leave(h);
+}
+
+int nhf_set_clock(nhf_handle *h, const uint32_t now[2])
+{
+    if (!h || !now) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    memcpy(h->h_small, now, 2 * sizeof(uint32_t));
+    CK(h, cudaMemcpyAsync(h->ctl->now, h->h_small, 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    return leave(h);
+}
+
+int nhf_get_clock(nhf_handle *h, uint32_t now[2])
+{
+    if (!h || !now) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    CK(h, cudaMemcpyAsync(h->h_small, h->ctl->now, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    memcpy(now, h->h_small, 2 * sizeof(uint32_t));
+    return leave(h);
+}
+
+int nhf_set_active(nhf_handle *h, int32_t active)
+{
+    if (!h) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    memcpy(h->h_small, &active, sizeof(int32_t));
+    CK(h, cudaMemcpyAsync(&h->ctl->active, h->h_small, sizeof(int32_t), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    return leave(h);
+}
+
+int nhf_set_forcing(nhf_handle *h, const float *coefficients, const float *rain_rates, int32_t raining)
+{
+    if (!h) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    const int bb = h->m.b_num > 0 ? h->m.b_num : 1;
+    float *stage = h->h_small;
+    if (coefficients) {
+        memcpy(stage, coefficients, sizeof(float) * 2 * bb);
+        CK(h, cudaMemcpyAsync((void *)h->dev.coef, stage, sizeof(float) * 2 * bb, cudaMemcpyHostToDevice, h->s));
+    }
+    if (rain_rates && h->m.n_rates > 0) {
+        memcpy(stage + 2 * bb, rain_rates, sizeof(float) * h->m.n_rates);
+        CK(h, cudaMemcpyAsync(h->dev.rain_rates, stage + 2 * bb, sizeof(float) * h->m.n_rates,
+                              cudaMemcpyHostToDevice, h->s));
+    }
+    memcpy(stage + 2 * bb + h->m.n_rates, &raining, sizeof(int32_t));
+    CK(h, cudaMemcpyAsync(&h->ctl->raining, stage + 2 * bb + h->m.n_rates, sizeof(int32_t),
+                          cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    return leave(h);
+}
+
+int nhf_apply_initial_levels(nhf_handle *h, const float *targets)
+{
+    if (!h || !targets) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    k_apply_levels<<<h->dev.blocks, kBlock, 0, h->s>>>(h->dev, targets);
+    return leave(h);
+}
+
+int nhf_compute_cfl(nhf_handle *h)
+{
+    if (!h) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    int gc = grid_for(h->m.s_num - 1, 256);
+    if (gc > 148 * 8) gc = 148 * 8;
+    k_cfl<<<gc, 256, 0, h->s>>>(h->dev, 0);
+    return leave(h);
+}
+
+int nhf_initial_diagnostics(nhf_handle *h)
+{
+    if (!h) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    k_initial_diag<<<grid_for(h->m.e_num - 1, 256), 256, 0, h->s>>>(h->dev);
+    return leave(h);
+}
+
+int nhf_reset_extrema(nhf_handle *h)
+{
+    if (!h) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    k_reset_extrema<<<grid_for(h->m.e_num - 1, 256), 256, 0, h->s>>>(h->dev);
+    return leave(h);
+}
+
+int nhf_run_batch_async(nhf_handle *h, const uint32_t target[2], const uint32_t origin[2])
+{
+    if (!h || !target || !origin) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    if (!h->graph) { rc = build_graph(h); if (rc) return rc; }
+    // The pinned staging words are read by the graph's first copy; wait for
+    // the previous replay before overwriting them.
+    CK(h, cudaStreamSynchronize(h->s));
+    h->h_begin[0] = target[0]; h->h_begin[1] = target[1];
+    h->h_begin[2] = origin[0]; h->h_begin[3] = origin[1];
+    CK(h, cudaGraphLaunch(h->graph, h->s));
+    return leave(h);
+}
+
+int nhf_read_trace(nhf_handle *h, uint32_t *trace)
+{
+    if (!h || !trace) return NHF_EINVAL;
+    CK(h, cudaStreamSynchronize(h->s));
+    memcpy(trace, h->h_trace, sizeof(uint32_t) * NHF_TRACE_COLS * h->p.batch_size);
+    return NHF_OK;
+}
+
+int nhf_run_batch(nhf_handle *h, const uint32_t target[2], const uint32_t origin[2], uint32_t *trace)
+{
+    int rc = nhf_run_batch_async(h, target, origin);
+    if (rc) return rc;
+    return nhf_read_trace(h, trace);
+}
+
+int nhf_budget_terms(const nhf_handle *h) { return h ? h->dev.terms : 0; }
+
+int nhf_budget_flush(nhf_handle *h, double *totals)
+{
+    if (!h || !totals) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    const int T = h->dev.terms, blocks = h->dev.blocks;
+    const size_t n = (size_t)blocks * T;
+    CK(h, cudaMemcpyAsync(h->h_acc, h->dev.acc_sum, sizeof(double) * n, cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaMemcpyAsync(h->h_acc + n, h->dev.acc_comp, sizeof(double) * n, cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaMemsetAsync(h->dev.acc_sum, 0, sizeof(double) * n, h->s));
+    CK(h, cudaMemsetAsync(h->dev.acc_comp, 0, sizeof(double) * n, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    // Host merge: blocks in order, (sum, comp) pairs, Neumaier compensation.
+    for (int t = 0; t < T; ++t) {
+        double s = 0.0, comp = 0.0;
+        for (int b = 0; b < blocks; ++b) {
+            double parts[2] = {h->h_acc[(size_t)b * T + t], h->h_acc[n + (size_t)b * T + t]};
+            for (int j = 0; j < 2; ++j) {
+                double p = parts[j];
+                double s2 = s + p;
+                if (fabs(s) >= fabs(p)) comp += (s - s2) + p; else comp += (p - s2) + s;
+                s = s2;
+            }
+        }
+        totals[t] = s + comp;
+    }
+    return leave(h);
+}
+
+int nhf_get_cfl(nhf_handle *h, float *ndt, int32_t *arg, float *flow_depth)
+{
+    if (!h) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    float *out = (float *)h->d_begin;  // 3 words of device staging; graph not running
+    CK(h, cudaStreamSynchronize(h->s));
+    k_cfl_edge<<<1, 1, 0, h->s>>>(h->dev, out);
+    CK(h, cudaMemcpyAsync(h->h_small, out, 3 * sizeof(float), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    if (ndt) *ndt = h->h_small[0];
+    if (arg) memcpy(arg, &h->h_small[1], sizeof(int32_t));
+    if (flow_depth) *flow_depth = h->h_small[2];
+    return leave(h);
+}
+
+int nhf_limits(nhf_handle *h, float values[5], int32_t ids[3])
+{
+    if (!h) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    CK(h, cudaMemcpyAsync(h->h_small, h->ctl->limit_value, 8 * sizeof(float), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    if (values) memcpy(values, h->h_small, 5 * sizeof(float));
+    if (ids) memcpy(ids, h->h_small + 5, 3 * sizeof(int32_t));
+    return leave(h);
+}
+
+int nhf_reset_limits(nhf_handle *h)
+{
+    if (!h) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    h->h_small[0] = __builtin_inff();
+    CK(h, cudaMemcpyAsync(&h->ctl->limit_value[0], h->h_small, sizeof(float), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    return leave(h);
+}
+
+int nhf_sample_stations(nhf_handle *h, const int32_t *ids, int32_t n, float *out)
+{
+    if (!h || n < 0 || (n > 0 && (!ids || !out))) return NHF_EINVAL;
+    if (n == 0) return NHF_OK;
+    int rc = enter(h); if (rc) return rc;
+    if (n > h->ids_cap) {
+        if (h->d_ids) cudaFree(h->d_ids);
+        if (h->d_samples) cudaFree(h->d_samples);
+        h->d_ids = nullptr; h->d_samples = nullptr;
+        CK(h, cudaMalloc(&h->d_ids, sizeof(int32_t) * n));
+        CK(h, cudaMalloc(&h->d_samples, sizeof(float) * 4 * n));
+        h->ids_cap = n;
+    }
+    for (int i = 0; i < n; ++i)
+        if (ids[i] < 1 || ids[i] >= h->m.e_num) return fail(h, NHF_EINVAL, "station cell %d out of range", ids[i]);
+    CK(h, cudaMemcpyAsync(h->d_ids, ids, sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->s));
+    k_sample<<<grid_for(n, 128), 128, 0, h->s>>>(h->dev, h->d_ids, n, h->d_samples);
+    CK(h, cudaMemcpyAsync(out, h->d_samples, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    return leave(h);
+}
+
+int nhf_read_eq(nhf_handle *h, float *eq)
+{
+    if (!h || !eq) return NHF_EINVAL;
+    int rc = enter(h); if (rc) return rc;
+    CK(h, cudaMemcpyAsync(eq, h->dev.eq, sizeof(float) * 4 * (size_t)h->m.e_num, cudaMemcpyDeviceToDevice, h->s));
+    return leave(h);
+}
+
+int nhf_read_gradients(nhf_handle *h, float *gradients)
+{
+    if (!h || !gradients) return NHF_EINVAL;
+    if (h->m.hang_cells <= 0) return NHF_OK;
+    int rc = enter(h); if (rc) return rc;
+    CK(h, cudaMemcpyAsync(gradients, h->dev.gradients, sizeof(float) * 2 * (size_t)h->m.hang_cells,
+                          cudaMemcpyDeviceToDevice, h->s));
+    return leave(h);
+}
+
+int nhf_synchronize(nhf_handle *h)
+{
+    if (!h) return NHF_EINVAL;
+    CK(h, cudaStreamSynchronize(h->s));
+    CK(h, cudaStreamSynchronize(h->user));
+    return NHF_OK;
+}
+
+}  // extern "C"

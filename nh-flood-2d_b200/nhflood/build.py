@@ -1,0 +1,58 @@
+"""Build the sm_100a step library in-tree (nhflood/_lib/libnhflood.so).
+
+Flags: --fmad=false keeps the reference's F32 operation sequence (no
+multiply-add contraction), which the CPU restatement reproduces bit for bit;
+IEEE division and square root are nvcc's defaults and stay on.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PACKAGE = Path(__file__).resolve().parent
+ROOT = PACKAGE.parent
+CSRC = ROOT / 'csrc'
+LIBDIR = PACKAGE / '_lib'
+LIBRARY = LIBDIR / 'libnhflood.so'
+INCLUDE = ROOT.parent / 'include'
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+
+
+def nvcc() -> str:
+    found = shutil.which('nvcc') or '/usr/local/cuda/bin/nvcc'
+    if not Path(found).exists():
+        raise RuntimeError('nvcc not found; the CUDA toolkit is required to build libnhflood.so')
+    return found
+
+
+def sources() -> list[Path]:
+    return sorted(CSRC.glob('*.cu'))
+
+
+def needs_build() -> bool:
+    if not LIBRARY.exists():
+        return True
+    stamp = LIBRARY.stat().st_mtime
+    deps = sources() + sorted(CSRC.glob('*.cuh')) + sorted(INCLUDE.glob('*.h'))
+    return any(p.stat().st_mtime > stamp for p in deps)
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    if not force and not needs_build():
+        return LIBRARY
+    LIBDIR.mkdir(exist_ok=True)
+    tmp = LIBDIR / f'.libnhflood.{os.getpid()}.so'
+    cmd = [nvcc(), *ARCH, '-lineinfo', '-O3', '--fmad=false', '-std=c++17', '-Xcompiler', '-fPIC',
+           '-shared', f'-I{INCLUDE}', '-o', str(tmp), *map(str, sources())]
+    if verbose:
+        print(' '.join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIBRARY)
+    return LIBRARY
+
+
+if __name__ == '__main__':
+    print(build(verbose=True, force='--force' in sys.argv))

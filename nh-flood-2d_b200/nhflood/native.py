@@ -1,0 +1,286 @@
+"""ctypes binding of libnhflood.so (include/nhflood.h) and the CUDA engine.
+
+Device arrays are torch CUDA tensors owned by ``CudaEngine``; the library
+receives their addresses and owns only its scratch. There is no CPU
+fallback: constructing the engine without a GPU or without the built
+library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_double, c_float, c_int32, c_uint32, c_void_p
+
+import numpy as np
+
+from .model import STATE_F32, STATE_U32, Engine, StepArrays, StepParams
+
+NHF_TRACE_COLS = 10
+
+_MESH_INTS = ('e_num', 's_num', 'b_num', 'n_rates', 'isl_len', 'hang_cells', 'hang_edges')
+_MESH_PTRS = ('x', 'y', 'area', 'width', 'height', 'f0', 'fc', 'k', 'weight', 'boundary_id', 'rain_index',
+              'face_ptr', 'face_count', 'isl_data', 'topology', 'length', 'side_n', 'sbf', 'kind',
+              'open_face', 'edge_index', 'offsets', 'slots', 'hcells', 'axes',
+              'bed', 'depth', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_speed', 'u', 'v',
+              'peak_hi', 'peak_lo')
+
+
+class NhfMesh(ctypes.Structure):
+    _fields_ = [(n, c_int32) for n in _MESH_INTS] + [(n, c_void_p) for n in _MESH_PTRS]
+
+
+class NhfParams(ctypes.Structure):
+    _fields_ = [('g', c_float), ('afa', c_float), ('sita', c_float), ('min_h', c_float),
+                ('min_dt', c_float), ('batch_size', c_int32)]
+
+
+_LIB = None
+
+
+def library(path=None):
+    """Load (and declare) libnhflood.so; raises if it is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    from .build import LIBRARY
+    path = path or LIBRARY
+    if not path.exists():
+        raise RuntimeError(f'{path} is missing: build it with `python -m nhflood.build` '
+                           '(the CUDA step has no CPU fallback)')
+    lib = ctypes.CDLL(str(path))
+    H = c_void_p
+    sig = {
+        'nhf_create': (c_int32, [POINTER(NhfMesh), POINTER(NhfParams), c_void_p, POINTER(c_void_p)]),
+        'nhf_destroy': (c_int32, [H]),
+        'nhf_last_error': (ctypes.c_char_p, [H]),
+        'nhf_version': (ctypes.c_char_p, []),
+        'nhf_initialize': (c_int32, [H]),
+        'nhf_set_clock': (c_int32, [H, POINTER(c_uint32)]),
+        'nhf_get_clock': (c_int32, [H, POINTER(c_uint32)]),
+        'nhf_set_active': (c_int32, [H, c_int32]),
+        'nhf_set_forcing': (c_int32, [H, POINTER(c_float), POINTER(c_float), c_int32]),
+        'nhf_apply_initial_levels': (c_int32, [H, c_void_p]),
+        'nhf_compute_cfl': (c_int32, [H]),
+        'nhf_initial_diagnostics': (c_int32, [H]),
+        'nhf_reset_extrema': (c_int32, [H]),
+        'nhf_run_batch': (c_int32, [H, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32)]),
+        'nhf_run_batch_async': (c_int32, [H, POINTER(c_uint32), POINTER(c_uint32)]),
+        'nhf_read_trace': (c_int32, [H, POINTER(c_uint32)]),
+        'nhf_budget_flush': (c_int32, [H, POINTER(c_double)]),
+        'nhf_budget_terms': (c_int32, [H]),
+        'nhf_get_cfl': (c_int32, [H, POINTER(c_float), POINTER(c_int32), POINTER(c_float)]),
+        'nhf_limits': (c_int32, [H, POINTER(c_float), POINTER(c_int32)]),
+        'nhf_reset_limits': (c_int32, [H]),
+        'nhf_sample_stations': (c_int32, [H, POINTER(c_int32), c_int32, POINTER(c_float)]),
+        'nhf_read_eq': (c_int32, [H, c_void_p]),
+        'nhf_read_gradients': (c_int32, [H, c_void_p]),
+        'nhf_synchronize': (c_int32, [H]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    """Names declared in include/nhflood.h that the library must export."""
+    return ['nhf_create', 'nhf_destroy', 'nhf_last_error', 'nhf_version', 'nhf_initialize', 'nhf_set_clock',
+            'nhf_get_clock', 'nhf_set_active', 'nhf_set_forcing', 'nhf_apply_initial_levels',
+            'nhf_compute_cfl', 'nhf_initial_diagnostics', 'nhf_reset_extrema', 'nhf_run_batch',
+            'nhf_run_batch_async', 'nhf_read_trace', 'nhf_budget_flush', 'nhf_budget_terms', 'nhf_get_cfl',
+            'nhf_limits', 'nhf_reset_limits', 'nhf_sample_stations', 'nhf_read_eq', 'nhf_read_gradients',
+            'nhf_synchronize']
+
+
+def _u32(a):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    return a, a.ctypes.data_as(POINTER(c_uint32))
+
+
+class CudaEngine(Engine):
+    """The step on one CUDA device through libnhflood.so."""
+
+    backend = 'cuda'
+
+    def __init__(self, arrays: StepArrays, params: StepParams, device='cuda:0'):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError('CudaEngine needs a CUDA device; the step has no CPU fallback')
+        self.torch = torch
+        self.lib = library()
+        self.arrays = arrays
+        self.params = params
+        self.device = torch.device(device)
+        self.device_name = torch.cuda.get_device_name(self.device)
+        self.batch_size = params.batch_size
+        dev = self.device
+
+        def put(a, dtype=None):
+            if a is None:
+                return None
+            t = torch.from_numpy(np.ascontiguousarray(a if dtype is None else a.astype(dtype)))
+            return t.to(dev)
+
+        e, s = arrays.e_num, arrays.s_num
+        self.t = {
+            'x': put(arrays.x), 'y': put(arrays.y), 'area': put(arrays.area), 'width': put(arrays.width),
+            'height': put(arrays.height), 'f0': put(arrays.f0), 'fc': put(arrays.fc), 'k': put(arrays.k),
+            'weight': put(arrays.weight), 'boundary_id': put(arrays.boundary_id),
+            'rain_index': put(arrays.rain_index), 'face_ptr': put(arrays.face_ptr),
+            'face_count': put(arrays.face_count),
+            'isl_data': put(arrays.isl_data if len(arrays.isl_data) else np.zeros(1, np.int32)),
+            'topology': put(arrays.topology), 'length': put(arrays.length), 'side_n': put(arrays.side_n),
+            'sbf': put(arrays.sbf), 'kind': put(arrays.kind), 'open_face': put(arrays.open_face),
+            'edge_index': put(arrays.edge_index), 'offsets': put(arrays.offsets), 'slots': put(arrays.slots),
+            'hcells': put(arrays.hcells), 'axes': put(arrays.axes),
+            'bed': put(arrays.bed),
+        }
+        with torch.cuda.device(dev):
+            for name in STATE_F32:
+                if name != 'bed':
+                    self.t[name] = torch.zeros(s if name == 'q' else e, dtype=torch.float32, device=dev)
+            for name in STATE_U32:
+                self.t[name] = torch.zeros(e, dtype=torch.int32, device=dev)
+        mesh = NhfMesh()
+        mesh.e_num, mesh.s_num, mesh.b_num = e, s, arrays.b_num
+        mesh.n_rates, mesh.isl_len = arrays.n_rates, len(arrays.isl_data)
+        mesh.hang_cells, mesh.hang_edges = arrays.hang_cells, arrays.hang_edges
+        for name in _MESH_PTRS:
+            tensor = self.t.get(name)
+            setattr(mesh, name, tensor.data_ptr() if tensor is not None else None)
+        self._mesh = mesh
+        p = NhfParams(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size)
+        handle = c_void_p()
+        with torch.cuda.device(dev):
+            stream = torch.cuda.current_stream(dev).cuda_stream
+            rc = self.lib.nhf_create(ctypes.byref(mesh), ctypes.byref(p), c_void_p(stream), ctypes.byref(handle))
+        if rc != 0:
+            raise RuntimeError(f'nhf_create failed ({rc}): {self.lib.nhf_last_error(None).decode()}')
+        self.h = handle
+        self.terms = self.lib.nhf_budget_terms(self.h)
+        self._trace = np.zeros((self.batch_size, NHF_TRACE_COLS), dtype=np.uint32)
+
+    # -- helpers ----------------------------------------------------------
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f'{what} failed ({rc}): {self.lib.nhf_last_error(self.h).decode()}')
+
+    def get(self, name):
+        t = self.t[name]
+        out = t.cpu().numpy()
+        return out.view(np.uint32) if name in STATE_U32 else out
+
+    def set(self, name, values):
+        t = self.t[name]
+        arr = np.ascontiguousarray(values)
+        if name in STATE_U32:
+            arr = arr.astype(np.uint32).view(np.int32)
+        else:
+            arr = arr.astype(np.float32)
+        if arr.shape != tuple(t.shape):
+            raise ValueError(f'{name}: shape {arr.shape} differs from {tuple(t.shape)}')
+        t.copy_(self.torch.from_numpy(arr))
+
+    def initialize(self):
+        self._check(self.lib.nhf_initialize(self.h), 'nhf_initialize')
+
+    def set_clock(self, words):
+        w, p = _u32(words)
+        self._check(self.lib.nhf_set_clock(self.h, p), 'nhf_set_clock')
+
+    def get_clock(self):
+        w = np.zeros(2, np.uint32)
+        self._check(self.lib.nhf_get_clock(self.h, w.ctypes.data_as(POINTER(c_uint32))), 'nhf_get_clock')
+        return w
+
+    def set_active(self, active):
+        self._check(self.lib.nhf_set_active(self.h, int(active)), 'nhf_set_active')
+
+    def set_forcing(self, coefficients, rain_rates, raining):
+        coef = np.ascontiguousarray(coefficients, dtype=np.float32)
+        rates = None if rain_rates is None else np.ascontiguousarray(rain_rates, dtype=np.float32)
+        self._check(self.lib.nhf_set_forcing(
+            self.h, coef.ctypes.data_as(POINTER(c_float)),
+            rates.ctypes.data_as(POINTER(c_float)) if rates is not None else None, int(bool(raining))),
+            'nhf_set_forcing')
+
+    def apply_initial_levels(self, targets):
+        t = self.torch.from_numpy(np.ascontiguousarray(targets, dtype=np.float32)).to(self.device)
+        self._check(self.lib.nhf_apply_initial_levels(self.h, c_void_p(t.data_ptr())), 'nhf_apply_initial_levels')
+        self.torch.cuda.synchronize(self.device)
+
+    def compute_cfl(self):
+        self._check(self.lib.nhf_compute_cfl(self.h), 'nhf_compute_cfl')
+
+    def initial_diagnostics(self):
+        self._check(self.lib.nhf_initial_diagnostics(self.h), 'nhf_initial_diagnostics')
+
+    def reset_extrema(self):
+        self._check(self.lib.nhf_reset_extrema(self.h), 'nhf_reset_extrema')
+
+    def run_batch(self, target_words, origin_words):
+        t, tp = _u32(target_words)
+        o, op = _u32(origin_words)
+        self._check(self.lib.nhf_run_batch(self.h, tp, op, self._trace.ctypes.data_as(POINTER(c_uint32))),
+                    'nhf_run_batch')
+        return self._trace.copy()
+
+    def run_batch_async(self, target_words, origin_words):
+        t, tp = _u32(target_words)
+        o, op = _u32(origin_words)
+        self._check(self.lib.nhf_run_batch_async(self.h, tp, op), 'nhf_run_batch_async')
+
+    def read_trace(self):
+        self._check(self.lib.nhf_read_trace(self.h, self._trace.ctypes.data_as(POINTER(c_uint32))), 'nhf_read_trace')
+        return self._trace.copy()
+
+    def budget_flush(self):
+        out = np.zeros(self.terms, dtype=np.float64)
+        self._check(self.lib.nhf_budget_flush(self.h, out.ctypes.data_as(POINTER(c_double))), 'nhf_budget_flush')
+        return out
+
+    def cfl(self):
+        ndt, arg, h = c_float(), c_int32(), c_float()
+        self._check(self.lib.nhf_get_cfl(self.h, ctypes.byref(ndt), ctypes.byref(arg), ctypes.byref(h)), 'nhf_get_cfl')
+        return float(ndt.value), int(arg.value), float(h.value)
+
+    def limits(self):
+        values = np.zeros(5, np.float32)
+        ids = np.zeros(3, np.int32)
+        self._check(self.lib.nhf_limits(self.h, values.ctypes.data_as(POINTER(c_float)),
+                                        ids.ctypes.data_as(POINTER(c_int32))), 'nhf_limits')
+        return values, ids
+
+    def reset_limits(self):
+        self._check(self.lib.nhf_reset_limits(self.h), 'nhf_reset_limits')
+
+    def sample_stations(self, ids):
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        out = np.zeros((len(ids), 4), np.float32)
+        if len(ids):
+            self._check(self.lib.nhf_sample_stations(self.h, ids.ctypes.data_as(POINTER(c_int32)), len(ids),
+                                                     out.ctypes.data_as(POINTER(c_float))), 'nhf_sample_stations')
+        return out
+
+    def read_eq(self):
+        out = self.torch.zeros((self.arrays.e_num, 4), dtype=self.torch.float32, device=self.device)
+        self._check(self.lib.nhf_read_eq(self.h, c_void_p(out.data_ptr())), 'nhf_read_eq')
+        return out.cpu().numpy()
+
+    def synchronize(self):
+        self._check(self.lib.nhf_synchronize(self.h), 'nhf_synchronize')
+
+    def peak_memory(self):
+        return int(self.torch.cuda.max_memory_allocated(self.device))
+
+    def close(self):
+        if getattr(self, 'h', None):
+            self.lib.nhf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

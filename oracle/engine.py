@@ -1,0 +1,239 @@
+"""ORACLE — test infrastructure only.
+
+ctypes wrapper that runs the CPU restatement (step_ref.c) behind the same
+engine interface the time loop uses for the CUDA step, so a whole solver run
+can be replayed on the CPU and compared bit for bit. Only tests/, the smoke
+check and bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import POINTER, c_double, c_float, c_int, c_int32, c_uint32, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / '_build' / 'liboracle.so'
+TRACE_COLS = 10
+STATE_F32 = ('bed', 'depth', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_speed', 'u', 'v')
+STATE_U32 = ('peak_hi', 'peak_lo')
+
+
+def build() -> Path:
+    sources = [HERE / 'step_ref.c', HERE / 'mathref.c', HERE / 'step_ref.h', HERE / 'Makefile']
+    if not LIB_PATH.exists() or any(p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in sources):
+        subprocess.run(['make', '-s', '-C', str(HERE)], check=True)
+    return LIB_PATH
+
+
+_PTRS = ('x', 'y', 'area', 'width', 'height', 'f0', 'fc', 'k', 'boundary_id', 'rain_index',
+         'face_ptr', 'face_count', 'isl_data', 'weight', 'topology', 'length', 'side_n', 'sbf', 'kind',
+         'open_face')
+_HANG = ('edge_index', 'offsets', 'slots', 'hcells', 'axes')
+_STATE = ('bed', 'depth', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_speed', 'u', 'v',
+          'peak_hi', 'peak_lo', 'pipe_q')
+
+
+class OraMesh(ctypes.Structure):
+    _fields_ = ([(n, c_int32) for n in ('e_num', 's_num', 'b_num', 'n_rates', 'isl_len', 'batch_size')]
+                + [(n, c_float) for n in ('g', 'afa', 'sita', 'min_h', 'min_dt')]
+                + [(n, c_void_p) for n in _PTRS]
+                + [('hang_cells', c_int32), ('hang_edges', c_int32)]
+                + [(n, c_void_p) for n in _HANG]
+                + [(n, c_void_p) for n in _STATE])
+
+
+_LIB = None
+
+
+def library():
+    global _LIB
+    if _LIB is None:
+        lib = ctypes.CDLL(str(build()))
+        H = c_void_p
+        U2 = POINTER(c_uint32)
+        for name, res, args in [
+            ('ora_create', H, [POINTER(OraMesh)]), ('ora_destroy', None, [H]), ('ora_initialize', None, [H]),
+            ('ora_set_threads', None, [c_int]), ('ora_set_clock', None, [H, U2]), ('ora_get_clock', None, [H, U2]),
+            ('ora_set_active', None, [H, c_int]),
+            ('ora_set_forcing', None, [H, POINTER(c_float), POINTER(c_float), c_int]),
+            ('ora_apply_initial_levels', None, [H, POINTER(c_float)]), ('ora_compute_cfl', None, [H]),
+            ('ora_initial_diagnostics', None, [H]), ('ora_reset_extrema', None, [H]),
+            ('ora_run_batch', None, [H, U2, U2, U2]), ('ora_budget_flush', None, [H, POINTER(c_double)]),
+            ('ora_budget_terms', c_int, [H]), ('ora_ndt', c_float, [H]), ('ora_cfl_arg', c_int32, [H]),
+            ('ora_limits', None, [H, POINTER(c_float), POINTER(c_int32)]), ('ora_reset_limits', None, [H]),
+            ('ora_read_eq', None, [H, POINTER(c_float)]), ('ora_read_flow_depth', None, [H, POINTER(c_float)]),
+            ('ora_read_gradients', None, [H, POINTER(c_float)]), ('ora_update_pressure', None, [H]),
+            ('ora_pressure_difference', c_float, [H, c_int, c_int, c_int, c_float]),
+            ('ora_ln', c_double, [c_double]), ('ora_exp', c_double, [c_double]),
+            ('ora_powf', c_float, [c_float, c_float]), ('ora_expf', c_float, [c_float]),
+        ]:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def set_threads(n: int) -> None:
+    library().ora_set_threads(int(n))
+
+
+class OracleEngine:
+    """The restated reference step on the CPU (OpenMP), engine interface."""
+
+    backend = 'cpu-oracle'
+
+    def __init__(self, arrays, params, threads: int | None = None):
+        self.lib = library()
+        if threads:
+            self.lib.ora_set_threads(int(threads))
+        self.device_name = f'CPU restatement ({os.cpu_count()} cores)'
+        self.arrays = arrays
+        self.batch_size = params.batch_size
+        self.keep = {}
+        e, s = arrays.e_num, arrays.s_num
+
+        def keep(name, a, dtype):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=dtype)
+            self.keep[name] = a
+            return a.ctypes.data
+
+        m = OraMesh()
+        m.e_num, m.s_num, m.b_num, m.n_rates = e, s, arrays.b_num, arrays.n_rates
+        m.isl_len, m.batch_size = len(arrays.isl_data), params.batch_size
+        m.g, m.afa, m.sita, m.min_h, m.min_dt = params.g, params.afa, params.sita, params.min_h, params.min_dt
+        f32 = np.float32
+        for name, dtype in [('x', f32), ('y', f32), ('area', f32), ('width', f32), ('height', f32), ('f0', f32),
+                            ('fc', f32), ('k', f32), ('boundary_id', np.int32), ('rain_index', np.int32),
+                            ('face_ptr', np.int32), ('face_count', np.int32), ('isl_data', np.int32),
+                            ('weight', f32), ('topology', np.int32), ('length', f32), ('side_n', f32),
+                            ('sbf', np.uint8), ('kind', np.int32), ('open_face', f32)]:
+            setattr(m, name, keep(name, getattr(arrays, name), dtype))
+        m.hang_cells, m.hang_edges = arrays.hang_cells, arrays.hang_edges
+        for name, dtype in [('edge_index', np.int32), ('offsets', f32), ('slots', np.int32),
+                            ('hcells', np.int32), ('axes', np.int32)]:
+            setattr(m, name, keep(name, getattr(arrays, name), dtype))
+        self.state = {'bed': np.ascontiguousarray(arrays.bed, dtype=f32).copy()}
+        for name in STATE_F32:
+            if name != 'bed':
+                self.state[name] = np.zeros(s if name == 'q' else e, dtype=f32)
+        for name in STATE_U32:
+            self.state[name] = np.zeros(e, dtype=np.uint32)
+        for name in _STATE:
+            setattr(m, name, self.state[name].ctypes.data if name in self.state else None)
+        self._mesh = m
+        self.h = self.lib.ora_create(ctypes.byref(m))
+        self.terms = self.lib.ora_budget_terms(self.h)
+        self._trace = np.zeros((self.batch_size, TRACE_COLS), np.uint32)
+
+    def get(self, name):
+        return self.state[name].copy()
+
+    def set(self, name, values):
+        arr = np.asarray(values)
+        if arr.shape != self.state[name].shape:
+            raise ValueError(f'{name}: shape {arr.shape} differs from {self.state[name].shape}')
+        self.state[name][...] = arr.astype(self.state[name].dtype)
+
+    def initialize(self):
+        self.lib.ora_initialize(self.h)
+
+    def set_clock(self, words):
+        w = np.ascontiguousarray(words, np.uint32)
+        self.lib.ora_set_clock(self.h, w.ctypes.data_as(POINTER(c_uint32)))
+
+    def get_clock(self):
+        w = np.zeros(2, np.uint32)
+        self.lib.ora_get_clock(self.h, w.ctypes.data_as(POINTER(c_uint32)))
+        return w
+
+    def set_active(self, active):
+        self.lib.ora_set_active(self.h, int(active))
+
+    def set_forcing(self, coefficients, rain_rates, raining):
+        coef = None if coefficients is None else np.ascontiguousarray(coefficients, np.float32)
+        rates = None if rain_rates is None else np.ascontiguousarray(rain_rates, np.float32)
+        self.lib.ora_set_forcing(self.h, coef.ctypes.data_as(POINTER(c_float)) if coef is not None else None,
+                                 rates.ctypes.data_as(POINTER(c_float)) if rates is not None else None,
+                                 int(bool(raining)))
+
+    def apply_initial_levels(self, targets):
+        t = np.ascontiguousarray(targets, np.float32)
+        self.lib.ora_apply_initial_levels(self.h, t.ctypes.data_as(POINTER(c_float)))
+
+    def compute_cfl(self):
+        self.lib.ora_compute_cfl(self.h)
+
+    def initial_diagnostics(self):
+        self.lib.ora_initial_diagnostics(self.h)
+
+    def reset_extrema(self):
+        self.lib.ora_reset_extrema(self.h)
+
+    def run_batch(self, target_words, origin_words):
+        t = np.ascontiguousarray(target_words, np.uint32)
+        o = np.ascontiguousarray(origin_words, np.uint32)
+        self.lib.ora_run_batch(self.h, t.ctypes.data_as(POINTER(c_uint32)), o.ctypes.data_as(POINTER(c_uint32)),
+                               self._trace.ctypes.data_as(POINTER(c_uint32)))
+        return self._trace.copy()
+
+    def budget_flush(self):
+        out = np.zeros(self.terms, np.float64)
+        self.lib.ora_budget_flush(self.h, out.ctypes.data_as(POINTER(c_double)))
+        return out
+
+    def cfl(self):
+        si = int(self.lib.ora_cfl_arg(self.h))
+        fd = np.zeros(self.arrays.s_num, np.float32)
+        self.lib.ora_read_flow_depth(self.h, fd.ctypes.data_as(POINTER(c_float)))
+        return float(self.lib.ora_ndt(self.h)), si, float(fd[si])
+
+    def limits(self):
+        values = np.zeros(5, np.float32)
+        ids = np.zeros(3, np.int32)
+        self.lib.ora_limits(self.h, values.ctypes.data_as(POINTER(c_float)), ids.ctypes.data_as(POINTER(c_int32)))
+        return values, ids
+
+    def reset_limits(self):
+        self.lib.ora_reset_limits(self.h)
+
+    def sample_stations(self, ids):
+        ids = np.asarray(ids, dtype=np.int64)
+        d, z = self.state['depth'], self.state['bed']
+        out = np.zeros((len(ids), 4), np.float32)
+        if len(ids):
+            out[:, 0] = d[ids]
+            out[:, 1] = z[ids] + d[ids]
+            out[:, 2] = self.state['u'][ids]
+            out[:, 3] = self.state['v'][ids]
+        return out
+
+    def read_eq(self):
+        out = np.zeros((self.arrays.e_num, 4), np.float32)
+        self.lib.ora_read_eq(self.h, out.ctypes.data_as(POINTER(c_float)))
+        return out
+
+    def read_gradients(self):
+        out = np.zeros((max(1, self.arrays.hang_cells), 2), np.float32)
+        self.lib.ora_read_gradients(self.h, out.ctypes.data_as(POINTER(c_float)))
+        return out[:self.arrays.hang_cells]
+
+    def peak_memory(self):
+        return None
+
+    def close(self):
+        if getattr(self, 'h', None):
+            self.lib.ora_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
