@@ -1,0 +1,258 @@
+"""Benchmark: cell-updates/s of the plain local-inertial step on B200.
+
+    python bench.py --gpus N --steps K --warmup W [--workload NAME] [--impl reference]
+
+A "step" of this benchmark is one batch of up to 32 device time steps (one
+replay of the captured step graph, the unit the reference's ti.graph runs
+per host round trip) of the plain single-run solver on the workload; the
+metric counts cells x completed time steps. ``value`` is device time with
+the state resident in HBM (CUDA events on the library's stream around each
+batch); ``e2e`` is the same metric through the public engine call with host
+forcing inputs and the host trace read-back inside the timed region.
+
+Multi-GPU: the plain solve does not shard (one domain per device); N ranks
+run N independent replicas ("replicas only", weak scaling), timed by device
+events with the max over ranks.
+
+``--impl reference`` times the reference algorithm's CPU implementation (the
+CPU restatement of the step, all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / 'nh-flood-2d_b200'))
+
+METRIC = 'cell-updates/s'
+PEAKS = ROOT / 'MEASURED_PEAKS.json'
+FALLBACK_HBM = 6650.0
+
+# Algorithmic bytes per cell-update (minimum unique state a fused step moves),
+# per workload: h r/w 8 + z 4 + q r/w of 2 sides 16 + n of 2 sides 8 +
+# max_depth r/w 8 + max_speed r/w 8 = 52 B; rain pixel index +4 B.
+ALGO_BYTES = {'dambreak_4096': 52, 'dambreak_2048': 52, 'plain_uniform_256': 56}
+
+
+def make_workload(name):
+    from nhflood import workloads
+    if name == 'plain_uniform_256':
+        return workloads.plain_uniform_256()
+    if name.startswith('dambreak_'):
+        return workloads.dambreak(n=int(name.split('_')[1]))
+    if name == 'multires_quadtree':
+        return workloads.multires_quadtree()
+    raise SystemExit(f'unknown workload {name}')
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.stop = threading.Event()
+        self.thread = None
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.FIELDS}',
+                                      '--format=csv,noheader,nounits'], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(',')])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.stop.set()
+        if self.thread:
+            self.thread.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unavailable']}
+        sm = [float(s[1]) for s in self.samples if s[1].replace('.', '').isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[i] for s in self.samples for i, v in enumerate(s[5:9]) if v.strip().lower() == 'active'})
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': max(mx) if mx else None,
+                'reasons': reasons, 'samples': len(self.samples)}
+
+
+def peak_hbm():
+    try:
+        return float(json.loads(PEAKS.read_text())['hbm_gbs']), 'measured'
+    except Exception:
+        return FALLBACK_HBM, 'fallback'
+
+
+def cpu_baseline(workload, seconds_budget=15.0, threads=None):
+    """The CPU restatement on the same workload, all host threads, bounded sample."""
+    sys.path.insert(0, str(ROOT / 'oracle'))
+    from engine import OracleEngine, set_threads  # oracle/engine.py
+    from nhflood.plain import PlainRun
+    threads = threads or os.cpu_count()
+    set_threads(threads)
+    run = PlainRun(workload, lambda a, p: OracleEngine(a, p), batch_size=1)
+    steps = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds_budget and not run.done:
+        steps += run.advance()
+    el = time.perf_counter() - t0
+    run.close()
+    return {'value': workload.cells * steps / el, 'unit': METRIC, 'cores': threads, 'kind': 'port',
+            'sample': f'{steps} time steps of {workload.name} from t=0 ({el:.1f} s of CPU restatement, OpenMP)'}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--workload', default=os.environ.get('NHF_BENCH_WORKLOAD', 'dambreak_4096'))
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--cpu-seconds', type=float, default=15.0)
+    args = ap.parse_args()
+
+    rank = int(os.environ.get('RANK', 0))
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+
+    if args.impl == 'reference':
+        if rank != 0:
+            return
+        w = make_workload(args.workload)
+        base = cpu_baseline(w, seconds_budget=max(5.0, args.cpu_seconds))
+        line = {'metric': METRIC, 'value': base['value'], 'unit': METRIC, 'impl': 'reference', 'n_gpus': args.gpus,
+                'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
+                'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+                'config': {'workload': w.name, 'cells': w.cells},
+                'cpu_baseline': base,
+                'e2e': {'value': base['value'], 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=120))
+        torch.cuda.set_device(local)
+    device = torch.device('cuda', local)
+    torch.cuda.set_device(device)
+    from nhflood.native import CudaEngine
+    from nhflood.plain import PlainRun
+
+    w = make_workload(args.workload)
+    run = PlainRun(w, lambda a, p: CudaEngine(a, p, device=str(device)))
+    eng = run.engine
+    stream = eng.stream()
+    # warm-up batches (untimed)
+    for _ in range(args.warmup):
+        run.advance()
+    torch.cuda.synchronize(device)
+    if world > 1:
+        dist.barrier()
+    # device-resident timing: events around each graph replay on the library stream
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    cell_steps = 0
+    launches = 0
+    per_step_kernels = 6 + (1 if run.arrays.hang_cells else 0) + (0 if w.sita == 1.0 else 1)
+    recorded = 0
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize(device)
+        for k in range(args.steps):
+            if run.done:
+                break
+            recorded += 1
+            tw, ow = run.begin()
+            starts[k].record(stream)
+            eng.run_batch_async(tw, ow)
+            ends[k].record(stream)
+            n = run.finish(eng.read_trace())
+            cell_steps += n * w.cells
+            launches += 1 + run.params.batch_size * per_step_kernels
+        torch.cuda.synchronize(device)
+    timed = [starts[i].elapsed_time(ends[i]) for i in range(recorded)]
+    device_ms = float(sum(timed))
+    # end-to-end through the public call: host inputs in, host trace out
+    e2e_cells = 0
+    e2e_batches = max(3, min(args.steps, 20))
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for _ in range(e2e_batches):
+        if run.done:
+            break
+        tw, ow = run.begin()
+        rows = eng.run_batch(tw, ow)
+        h2d += run.h2d_bytes
+        d2h += rows.nbytes
+        e2e_cells += run.finish(rows) * w.cells
+    torch.cuda.synchronize(device)
+    e2e_s = time.perf_counter() - t0
+    stats = torch.tensor([device_ms, float(cell_steps), e2e_s, float(e2e_cells)], dtype=torch.float64, device=device)
+    if world > 1:
+        mx = stats.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = stats.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        device_ms, e2e_s = float(mx[0]), float(mx[2])
+        cell_steps, e2e_cells = float(sm[1]), float(sm[3])
+    value = cell_steps / (device_ms / 1e3) if device_ms > 0 else 0.0
+    e2e = e2e_cells / e2e_s if e2e_s > 0 else 0.0
+    if rank == 0:
+        peak, kind = peak_hbm()
+        b_alg = ALGO_BYTES.get(w.name)
+        per_rank = value / world
+        achieved = per_rank * b_alg / 1e9 if b_alg else None
+        line = {
+            'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': device_ms / max(1, len(timed)), 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': w.name, 'cells': w.cells, 'sides': w.mesh.s_num - 1,
+                       'time_steps_per_bench_step': run.params.batch_size,
+                       'l2': 'inputs larger than L2' if run.arrays.nbytes() > 126e6 else 'inputs fit L2',
+                       'parallelism': f'replicas{world}'},
+            'gpu_launches': launches,
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak if achieved else None, 'traffic': None,
+                         'peak_kind': kind, 'algorithmic_bytes_per_cell_update': b_alg,
+                         'scope': 'whole step graph (all step kernels)'},
+            'e2e': {'value': e2e, 'unit': METRIC, 'h2d_bytes_per_step': h2d // max(1, e2e_batches),
+                    'd2h_bytes_per_step': d2h // max(1, e2e_batches)},
+            'clocks': clocks.summary(),
+            'simulated_seconds': run.elapsed,
+        }
+        if world == 1 and os.environ.get('NHF_BENCH_NO_CPU') != '1':
+            line['cpu_baseline'] = cpu_baseline(w, seconds_budget=args.cpu_seconds)
+        print(json.dumps(line))
+    run.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -156,6 +156,9 @@ int nhf_read_eq(nhf_handle *h, float *eq);
 /* Hanging-edge gradients [hang_cells][2] (device destination). */
 int nhf_read_gradients(nhf_handle *h, float *gradients);
 int nhf_synchronize(nhf_handle *h);
+/* The library's own stream (cudaStream_t) on which every batch runs; lets a
+ * caller time batches with events on the launching stream. */
+void *nhf_stream(nhf_handle *h);
 
 #ifdef __cplusplus
 }

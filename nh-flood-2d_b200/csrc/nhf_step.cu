@@ -119,13 +119,15 @@ __global__ void k_initialize(Dev d)
     }
 }
 
-__global__ void k_begin(Dev d)
+// clock.begin on the device (clock.py:75-92): the target and origin words are
+// kernel arguments, updated in the instantiated graph before each replay.
+__global__ void k_begin(Dev d, uint32_t next_hi, uint32_t next_lo, uint32_t origin_hi, uint32_t origin_lo)
 {
     Ctl *c = d.ctl;
     int t = threadIdx.x;
     if (t == 0) {
-        c->next[0] = d.begin[0]; c->next[1] = d.begin[1];
-        c->origin[0] = d.begin[2]; c->origin[1] = d.begin[3];
+        c->next[0] = next_hi; c->next[1] = next_lo;
+        c->origin[0] = origin_hi; c->origin[1] = origin_lo;
         c->slot = 0;
     }
     for (int i = t; i < NHF_MAX_BATCH * NHF_TRACE_COLS; i += blockDim.x) c->trace[i] = 0u;
@@ -757,7 +759,10 @@ struct nhf_handle {
     int32_t *d_ids = nullptr;
     float *d_samples = nullptr;
     int ids_cap = 0;
+    cudaGraph_t graph_def = nullptr;
     cudaGraphExec_t graph = nullptr;
+    cudaGraphNode_t begin_node = nullptr;
+    cudaKernelNodeParams begin_params{};
     std::string err;
 };
 
@@ -828,16 +833,32 @@ int build_graph(nhf_handle *h)
 {
     cudaGraph_t g = nullptr;
     CK(h, cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
-    cudaMemcpyAsync(h->d_begin, h->h_begin, 4 * sizeof(uint32_t), cudaMemcpyHostToDevice, h->s);
-    k_begin<<<1, 256, 0, h->s>>>(h->dev);
+    k_begin<<<1, 256, 0, h->s>>>(h->dev, 0u, 0u, 0u, 0u);
     for (int i = 0; i < h->p.batch_size; ++i) enqueue_step(h);
     cudaMemcpyAsync(h->h_trace, h->ctl->trace, sizeof(uint32_t) * NHF_TRACE_COLS * h->p.batch_size,
                     cudaMemcpyDeviceToHost, h->s);
     cudaError_t e = cudaStreamEndCapture(h->s, &g);
     if (e != cudaSuccess) return fail(h, NHF_ECUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    // Locate the begin kernel node: its arguments carry each batch's words.
+    size_t count = 0;
+    cudaGraphGetNodes(g, nullptr, &count);
+    cudaGraphNode_t *nodes = (cudaGraphNode_t *)malloc(sizeof(cudaGraphNode_t) * (count ? count : 1));
+    cudaGraphGetNodes(g, nodes, &count);
+    for (size_t i = 0; i < count && !h->begin_node; ++i) {
+        cudaGraphNodeType type;
+        cudaGraphNodeGetType(nodes[i], &type);
+        if (type != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        if (cudaGraphKernelNodeGetParams(nodes[i], &kp) == cudaSuccess && kp.func == (void *)k_begin) {
+            h->begin_node = nodes[i];
+            h->begin_params = kp;
+        }
+    }
+    free(nodes);
+    if (!h->begin_node) { cudaGraphDestroy(g); return fail(h, NHF_ECUDA, "begin node not found in graph"); }
     e = cudaGraphInstantiate(&h->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return fail(h, NHF_ECUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return fail(h, NHF_ECUDA, "graph instantiate failed: %s", cudaGetErrorString(e)); }
+    h->graph_def = g;
     return NHF_OK;
 }
 
@@ -953,6 +974,7 @@ int nhf_destroy(nhf_handle *h)
     if (!h) return NHF_OK;
     if (h->s) cudaStreamSynchronize(h->s);
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->graph_def) cudaGraphDestroy(h->graph_def);
     if (h->scratch) cudaFree(h->scratch);
     if (h->h_begin) cudaFreeHost(h->h_begin);
     if (h->h_trace) cudaFreeHost(h->h_trace);
@@ -1067,11 +1089,13 @@ int nhf_run_batch_async(nhf_handle *h, const uint32_t target[2], const uint32_t 
     if (!h || !target || !origin) return NHF_EINVAL;
     int rc = enter(h); if (rc) return rc;
     if (!h->graph) { rc = build_graph(h); if (rc) return rc; }
-    // The pinned staging words are read by the graph's first copy; wait for
-    // the previous replay before overwriting them.
-    CK(h, cudaStreamSynchronize(h->s));
-    h->h_begin[0] = target[0]; h->h_begin[1] = target[1];
-    h->h_begin[2] = origin[0]; h->h_begin[3] = origin[1];
+    Dev d = h->dev;
+    uint32_t w[4] = {target[0], target[1], origin[0], origin[1]};
+    void *args[5] = {&d, &w[0], &w[1], &w[2], &w[3]};
+    cudaKernelNodeParams kp = h->begin_params;
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    CK(h, cudaGraphExecKernelNodeSetParams(h->graph, h->begin_node, &kp));
     CK(h, cudaGraphLaunch(h->graph, h->s));
     return leave(h);
 }
@@ -1196,6 +1220,8 @@ int nhf_read_gradients(nhf_handle *h, float *gradients)
                           cudaMemcpyDeviceToDevice, h->s));
     return leave(h);
 }
+
+void *nhf_stream(nhf_handle *h) { return h ? (void *)h->s : nullptr; }
 
 int nhf_synchronize(nhf_handle *h)
 {

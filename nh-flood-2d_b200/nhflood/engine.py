@@ -56,24 +56,33 @@ def evolve(domain_cfg, force_cfg, record, coupling, end_time, engine_factory=Non
     mesh, side_flags = load_mesh(domain_cfg)
     geometry = MeshGeometry.from_mesh(mesh)
     forcing = Forcing.load(domain_cfg, force_cfg, geometry)
+    return evolve_loaded(domain_cfg, record, end_time, mesh, side_flags, geometry, forcing,
+                         engine_factory=engine_factory, batch_size=batch_size)
+
+
+def evolve_loaded(domain_cfg, record, end_time, mesh, side_flags, geometry, forcing, *, engine_factory=None,
+                  batch_size=32, state=None):
+    """The time loop on an already loaded mesh and forcing. ``state`` may be an
+    in-memory Checkpoint used instead of ``domain_cfg.restart_state``."""
     params = StepParams(afa=domain_cfg.afa, sita=domain_cfg.sita, min_h=domain_cfg.min_h, batch_size=batch_size)
     arrays = build_step_arrays(mesh, side_flags, geometry, forcing, domain_cfg.land_parameters, domain_cfg.sita)
     engine = (engine_factory or default_engine)(arrays, params)
     try:
         record.device(engine.backend, engine.device_name)
-        return _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, batch_size)
+        return _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, batch_size, state)
     finally:
         engine.close()
 
 
-def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, batch_size):
+def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, batch_size, state=None):
     e_num, s_num = mesh.e_num, mesh.s_num
     b_num = len(forcing.boundaries)
     afa, sita, min_h = domain_cfg.afa, domain_cfg.sita, domain_cfg.min_h
     record.data['budget_accumulator'].update(terms=4 + 6 * b_num, blocks=(e_num + 255) // 256)
 
     # -- restart state and clock origin (solver_compact.py:280-296)
-    state = read_checkpoint(domain_cfg.restart_state) if domain_cfg.restart_state else None
+    if state is None and domain_cfg.restart_state:
+        state = read_checkpoint(domain_cfg.restart_state)
     state_meta = json.loads(state.metadata_json) if state else {}
     continuation = bool(state_meta.get('run_state', False))
     origin_before_start = (state_meta['clock_origin_before_start_s'] if continuation

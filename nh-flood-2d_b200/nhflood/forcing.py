@@ -125,28 +125,30 @@ class Boundary:
         return self.weights * q
 
 
+def select_boundary(name, kind, lines, series, geometry, claimed) -> Boundary:
+    """Exterior edges overlapping ``lines`` with positive length; each cell is
+    weighted by its selected edge length (force.py:136-160)."""
+    edges = geometry.exterior_edges
+    selected = np.flatnonzero(overlap_lengths(edges.segments, lines) > 0)
+    side_ids = edges.side_ids[selected]
+    if len(side_ids) == 0:
+        raise ValueError(f'{name}: boundary selects no exterior edges; '
+                         'snap the line to mesh exterior edges in GIS')
+    cells, inverse = np.unique(edges.cell_ids[selected], return_inverse=True)
+    if np.any(claimed[cells]):
+        raise ValueError(f'{name}: boundary cells overlap another boundary')
+    claimed[cells] = True
+    lengths = np.bincount(inverse, weights=edges.lengths[selected])
+    weights = lengths / lengths.sum(dtype=np.float64)
+    return Boundary(name, kind, cells, weights, side_ids, series)
+
+
 def load_boundaries(config, geometry, epsg, origin, begin, end) -> list[Boundary]:
     if not config:
         return []
-    edges = geometry.exterior_edges
     claimed = np.zeros(len(geometry.x), dtype=bool)
-    boundaries = []
-    for b in config:
-        lines = load_line(b.line, epsg)
-        selected = np.flatnonzero(overlap_lengths(edges.segments, lines) > 0)
-        side_ids = edges.side_ids[selected]
-        if len(side_ids) == 0:
-            raise ValueError(f'{b.name}: boundary selects no exterior edges; '
-                             'snap the line to mesh exterior edges in GIS')
-        cells, inverse = np.unique(edges.cell_ids[selected], return_inverse=True)
-        if np.any(claimed[cells]):
-            raise ValueError(f'{b.name}: boundary cells overlap another boundary')
-        claimed[cells] = True
-        lengths = np.bincount(inverse, weights=edges.lengths[selected])
-        weights = lengths / lengths.sum(dtype=np.float64)
-        boundaries.append(Boundary(b.name, b.kind, cells, weights, side_ids,
-                                   TimeSeries.load(b.series, origin, begin, end)))
-    return boundaries
+    return [select_boundary(b.name, b.kind, load_line(b.line, epsg), TimeSeries.load(b.series, origin, begin, end),
+                            geometry, claimed) for b in config]
 
 
 @dataclass

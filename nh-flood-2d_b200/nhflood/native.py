@@ -74,6 +74,7 @@ def library(path=None):
         'nhf_read_eq': (c_int32, [H, c_void_p]),
         'nhf_read_gradients': (c_int32, [H, c_void_p]),
         'nhf_synchronize': (c_int32, [H]),
+        'nhf_stream': (c_void_p, [H]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -90,7 +91,7 @@ def exported_symbols() -> list[str]:
             'nhf_compute_cfl', 'nhf_initial_diagnostics', 'nhf_reset_extrema', 'nhf_run_batch',
             'nhf_run_batch_async', 'nhf_read_trace', 'nhf_budget_flush', 'nhf_budget_terms', 'nhf_get_cfl',
             'nhf_limits', 'nhf_reset_limits', 'nhf_sample_stations', 'nhf_read_eq', 'nhf_read_gradients',
-            'nhf_synchronize']
+            'nhf_synchronize', 'nhf_stream']
 
 
 def _u32(a):
@@ -198,10 +199,14 @@ class CudaEngine(Engine):
         self._check(self.lib.nhf_set_active(self.h, int(active)), 'nhf_set_active')
 
     def set_forcing(self, coefficients, rain_rates, raining):
-        coef = np.ascontiguousarray(coefficients, dtype=np.float32)
+        coef = None if coefficients is None else np.ascontiguousarray(coefficients, dtype=np.float32)
         rates = None if rain_rates is None else np.ascontiguousarray(rain_rates, dtype=np.float32)
+        if coef is not None and coef.shape != (max(1, self.arrays.b_num), 2):
+            raise ValueError(f'coefficients must be [{max(1, self.arrays.b_num)}, 2], got {coef.shape}')
+        if rates is not None and rates.shape != (self.arrays.n_rates,):
+            raise ValueError(f'rain rates must be [{self.arrays.n_rates}], got {rates.shape}')
         self._check(self.lib.nhf_set_forcing(
-            self.h, coef.ctypes.data_as(POINTER(c_float)),
+            self.h, coef.ctypes.data_as(POINTER(c_float)) if coef is not None else None,
             rates.ctypes.data_as(POINTER(c_float)) if rates is not None else None, int(bool(raining))),
             'nhf_set_forcing')
 
@@ -267,6 +272,10 @@ class CudaEngine(Engine):
         out = self.torch.zeros((self.arrays.e_num, 4), dtype=self.torch.float32, device=self.device)
         self._check(self.lib.nhf_read_eq(self.h, c_void_p(out.data_ptr())), 'nhf_read_eq')
         return out.cpu().numpy()
+
+    def stream(self):
+        """torch view of the library stream the batches run on."""
+        return self.torch.cuda.ExternalStream(self.lib.nhf_stream(self.h), device=self.device)
 
     def synchronize(self):
         self._check(self.lib.nhf_synchronize(self.h), 'nhf_synchronize')

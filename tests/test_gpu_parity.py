@@ -1,0 +1,104 @@
+"""CUDA step vs the CPU restatement, through the C ABI, bit for bit.
+
+Both engines run the same time loop on the same inputs. The bar is
+bit-exact: every trace row (dt bits, clock words, status, CFL candidate,
+event flag, limiter counts, minimum donor scale, wet-cell count), every
+state array at the end, the budget and step-statistics CSV files. Float
+arithmetic is deterministic on both sides (same F32 operation order, no
+contraction, FP64 budget partials in a fixed tree, order-free min/count
+reductions), so any difference is a defect.
+"""
+import filecmp
+
+import numpy as np
+import pytest
+
+from runner import run
+from scenarios import grid3_mesh, grid_cell, grid_horizontal, grid_vertical, seed_checkpoint, two_cell_case, domain
+
+pytestmark = pytest.mark.gpu
+
+STATE = ('depth', 'bed', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_speed', 'first_time_hi', 'first_time_lo')
+
+
+def assert_runs_identical(a, b):
+    assert a.trace.shape == b.trace.shape
+    np.testing.assert_array_equal(a.trace, b.trace)
+    for name in STATE:
+        x, y = getattr(a.state, name), getattr(b.state, name)
+        np.testing.assert_array_equal(np.asarray(x).view(np.uint32), np.asarray(y).view(np.uint32), err_msg=name)
+    for rel in ('mass_balance.csv', 'step_statistics.csv'):
+        assert filecmp.cmp(a.path / rel, b.path / rel, shallow=False), rel
+    assert a.manifest['dt_sequence_sha256'] == b.manifest['dt_sequence_sha256']
+
+
+CASES = {
+    'closed_basin': dict(bands=[[6, 6]], duration=60, q=.1, connected=True),
+    'horton_late': dict(bands=[[100, 0], [0, 100]], duration=120, land_type=1,
+                        infiltration=dict(f0_mm_h=76.2, fc_mm_h=2.54, k_per_h=2)),
+    'warmup_level_discharge': dict(bands=[[6, 6]], duration=60, q=.01, warmup=20, level=.1,
+                                   level_rows=[(0, .1), (60, .2)], q_rows=[(0, .01), (60, .03)], yield_step=10),
+    'negative_discharge': dict(bands=[[6, 6]], duration=60, q=-10.),
+    'level_knot': dict(bands=[[0, 0]], duration=1, level=0., level_rows=[(0, 0.), (.000002, 1.), (1, 0.)]),
+    'cfl_after_level': dict(bands=[[0, 0]], duration=1, connected=True, level=0,
+                            level_rows=[(0, 0), (.000002, 100), (1, 100)]),
+    'small_rain_high_bed': dict(bands=[[.01, .01]], duration=60, bed=100.),
+}
+
+
+@pytest.mark.parametrize('name', sorted(CASES))
+def test_two_cell_cases_bit_exact(tmp_path, cuda_available, name):
+    kw = dict(CASES[name])
+    bands, duration = kw.pop('bands'), kw.pop('duration')
+    dc, fc = two_cell_case(tmp_path / 'oracle', bands, duration, **kw)
+    a = run(dc, fc, 'oracle')
+    dc, fc = two_cell_case(tmp_path / 'cuda', bands, duration, **kw)
+    b = run(dc, fc, 'cuda')
+    assert b.manifest['backend'] == 'cuda'
+    assert_runs_identical(a, b)
+
+
+@pytest.mark.parametrize('sita', [1.0, 0.7])
+def test_grid_with_limiter_and_theta_bit_exact(tmp_path, cuda_available, sita):
+    results = []
+    for engine in ('oracle', 'cuda'):
+        path = tmp_path / engine
+        path.mkdir()
+        grid3_mesh(path)
+        from scenarios import write_rain
+        from nhflood.raster import from_origin
+        from nhflood.input import ForceConfig
+        rain = write_rain(path, [[[0]]], from_origin(0, 30, 30, 30), [(0, 20)])
+        q = np.zeros(25, np.float32)
+        for side, value in {grid_vertical(1, 1): -1, grid_vertical(1, 2): 1,
+                            grid_horizontal(1, 1): -1, grid_horizontal(2, 1): 1}.items():
+            q[side] = value
+        depth = np.zeros(10, np.float32)
+        depth[grid_cell(1, 1)] = .1
+        seed = seed_checkpoint(path / 'seed.fdb', path / 'ne.txt', path / 'ns.txt', depth=depth, q=q)
+        dc = domain(path, duration=20, yield_step=5, restart=seed, sita=sita,
+                    land={10: dict(manning_n=1e-3, infiltration='none')})
+        fc = ForceConfig(boundaries=[], rainfall=rain)
+        results.append(run(dc, fc, engine))
+    assert_runs_identical(*results)
+    assert results[1].manifest['limiter_activity']['limited_cell_steps'] > 0
+
+
+def test_plain_uniform_256_full_run_bit_exact(tmp_path, cuda_available):
+    """The 65,536-cell plain configuration for its whole 3600 s: identical
+    dt sequences and per-step wet counts; every 300 s frame identical."""
+    from nhflood.output import list_depth_frames, read_depth_frame
+    from nhflood.workloads import plain_uniform_256, simulate
+    from runner import cuda_factory, oracle_factory
+    w = plain_uniform_256()
+    row_a, rec_a = simulate(w, tmp_path / 'oracle', engine_factory=oracle_factory)
+    row_b, rec_b = simulate(w, tmp_path / 'cuda', engine_factory=cuda_factory)
+    assert rec_b.data['backend'] == 'cuda'
+    np.testing.assert_array_equal(rec_a.trace, rec_b.trace)
+    assert rec_a.trace[:, 9].max() > 1000  # the run does flood
+    fa = list_depth_frames(tmp_path / 'oracle' / 'output')
+    fb = list_depth_frames(tmp_path / 'cuda' / 'output')
+    assert [s for s, _ in fa] == [s for s, _ in fb]
+    for (_, pa), (_, pb) in zip(fa, fb):
+        np.testing.assert_array_equal(read_depth_frame(pa).view(np.uint32), read_depth_frame(pb).view(np.uint32))
+    assert row_a == row_b
