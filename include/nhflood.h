@@ -160,6 +160,25 @@ int nhf_synchronize(nhf_handle *h);
  * caller time batches with events on the launching stream. */
 void *nhf_stream(nhf_handle *h);
 
+/* No counterpart in the reference: an allocation-free CFL candidate for
+ * callers that may not allocate device memory (a host that reserves its HBM
+ * budget once at start-up, such as a serving process or a model coupler that
+ * hands out fixed pools). Same result as nhf_compute_cfl + nhf_get_cfl on
+ * the given state: ndt_out = min over interior sides of
+ * afa * L / (sqrt(g h) + |q| / h), arg_out = the lowest side id attaining it
+ * (+inf and 0 without interior sides); both outputs are DEVICE pointers, as
+ * are all inputs, and the call is asynchronous on `stream`. It allocates
+ * nothing: its scratch is a fixed 256 KiB array compiled into the library
+ * (held by every device that loads it until exit), which limits it to
+ * 67,108,864 sides (larger meshes: NHF_EINVAL). The first call on each
+ * device looks up that array's device address and must come before any
+ * stream capture. Calls share the array: calls that overlap on the GPU race.
+ * Errors are described by nhf_cfl_noalloc_error(). */
+int nhf_cfl_noalloc(const int32_t *topology, const float *bed, const float *depth, const float *length,
+                    const float *q, int32_t s_num, float afa, float g, void *stream, float *ndt_out,
+                    int32_t *arg_out);
+const char *nhf_cfl_noalloc_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,9 @@ def library(path=None):
         'nhf_read_gradients': (c_int32, [H, c_void_p]),
         'nhf_synchronize': (c_int32, [H]),
         'nhf_stream': (c_void_p, [H]),
+        'nhf_cfl_noalloc': (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_float, c_float,
+                                      c_void_p, c_void_p, c_void_p]),
+        'nhf_cfl_noalloc_error': (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -91,7 +94,7 @@ def exported_symbols() -> list[str]:
             'nhf_compute_cfl', 'nhf_initial_diagnostics', 'nhf_reset_extrema', 'nhf_run_batch',
             'nhf_run_batch_async', 'nhf_read_trace', 'nhf_budget_flush', 'nhf_budget_terms', 'nhf_get_cfl',
             'nhf_limits', 'nhf_reset_limits', 'nhf_sample_stations', 'nhf_read_eq', 'nhf_read_gradients',
-            'nhf_synchronize', 'nhf_stream']
+            'nhf_synchronize', 'nhf_stream', 'nhf_cfl_noalloc', 'nhf_cfl_noalloc_error']
 
 
 def _u32(a):
