@@ -95,6 +95,8 @@ typedef struct nhf_params {
     float min_h;      /* wet threshold */
     float min_dt;     /* F32(1e-4) CFL floor (solver_compact.py:31) */
     int32_t batch_size; /* steps per batch, 1..64 (clock.py:48-51) */
+    int32_t path;       /* 0: fused tiled step when the mesh allows it, else
+                           multi-pass; 1: always the multi-pass step */
 } nhf_params;
 
 typedef struct nhf_handle nhf_handle;
@@ -159,6 +161,8 @@ int nhf_synchronize(nhf_handle *h);
 /* The library's own stream (cudaStream_t) on which every batch runs; lets a
  * caller time batches with events on the launching stream. */
 void *nhf_stream(nhf_handle *h);
+/* Which step form the handle runs ("tiled(...)" or "multipass (reason)"). */
+const char *nhf_path(const nhf_handle *h);
 
 /* No counterpart in the reference: an allocation-free CFL candidate for
  * callers that may not allocate device memory (a host that reserves its HBM

@@ -1,0 +1,274 @@
+// Shared device-side definitions of the nhflood step: the control block, the
+// kernel parameter block, the device clock (clock.py:94-181) and the small
+// reductions used by both step forms (multi-pass and tiled).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/nhflood.h"
+
+namespace nhf {
+
+constexpr int kBlock = 256;                 // budget block = reference ei // 256
+constexpr float kDh = -999.0f;              // dh_t without gates (solver_compact.py:405)
+constexpr uint32_t kSnapTicks = 1099512u;   // ceil(1e-6 * 2**40) (clock.py:11)
+constexpr unsigned long long kCflEmpty = 0xFFFFFFFFFFFFFFFFULL;
+
+// Device control block: the reference's scalar fields (clock words, dt,
+// limiter counters, CFL result, limiting-edge snapshot) and the batch trace.
+struct Ctl {
+    uint32_t now[2], next[2], origin[2], step_end[2];
+    float dt, local, end_local, ndt;
+    int32_t active, slot, raining, cfl_arg;
+    uint32_t limited_cells, limited_faces, min_scale_bits, wet;
+    unsigned long long cfl_packed;
+    uint32_t done_blocks;
+    int32_t parity;  // 1: the current depth/q/rain_time live in the second buffers
+    float limit_value[5];
+    int32_t limit_ids[3];
+    uint32_t trace[NHF_MAX_BATCH * NHF_TRACE_COLS];
+};
+
+// Tile plan of the fused step (built on the host by nhf_tiled.cu).
+struct TilePlan {
+    int32_t n_tiles, tile, max_ext, max_sides, cells_per_thread;
+    const int32_t *tile_pattern, *tile_cbase, *tile_sbase;  // [n_tiles]
+    const int32_t *p_counts;   // [pattern][8]: n_ext, n_r0, n_r01, n_r012, n_sides, n_owned, n_qf, r0_first_offset
+    const int32_t *p_offsets;  // [pattern][4]: ext, side, face_desc, face_idx
+    const int32_t *ext_rel;    // relative cell ids by local slot (slot 0 = exterior sentinel)
+    const int32_t *side_rel;   // relative side ids by local side
+    const uint32_t *side_lohi; // local slots: lower | higher << 16
+    const uint32_t *face_desc; // per slot 0..n_r012: start | counts (4 x 4 bits) << 16
+    const uint16_t *face_idx;  // local side indices in the reference's CSR order
+};
+
+struct Dev {
+    nhf_mesh m;
+    float g, neg_g, afa, sita, half_rest, seven_thirds, min_h, min_dt;
+    int32_t terms, blocks, batch_size, theta_one;
+    Ctl *ctl;
+    const float *coef;
+    float *values, *level_values, *rain_rates, *sdc, *donor_scale, *face_qn, *eq, *gradients;
+    double *acc_sum, *acc_comp;
+    // second buffers of the double-buffered state (tiled form)
+    float *depth_b, *q_b, *rain_time_b;
+    TilePlan plan;
+};
+
+__device__ __forceinline__ float maxf(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float minf(float a, float b) { return b < a ? b : a; }
+
+__device__ __forceinline__ const float *cur_depth(const Dev &d, int parity) { return parity ? d.depth_b : d.m.depth; }
+__device__ __forceinline__ const float *cur_q(const Dev &d, int parity) { return parity ? d.q_b : d.m.q; }
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long w = __shfl_down_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+
+// Canonical pairwise tree over the 256 cells of one budget block:
+// slot i += slot i + stride for stride 128 .. 1. Returns the sum in thread 0.
+// Must be called by all 256 threads of the block.
+__device__ __forceinline__ double block_tree(double v, double *sh)
+{
+    const int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int stride = 128; stride >= 32; stride >>= 1) {
+        if (t < stride) sh[t] += sh[t + stride];
+        __syncthreads();
+    }
+    double r = 0.0;
+    if (t < 32) {
+        r = sh[t];
+        for (int stride = 16; stride >= 1; stride >>= 1) r += __shfl_down_sync(0xffffffffu, r, stride);
+    }
+    __syncthreads();
+    return r;
+}
+
+// TwoSum: exact error of sum + p accumulated in the compensation word.
+__device__ __forceinline__ void acc_add(double *sum, double *comp, double p)
+{
+    double s0 = *sum;
+    double s = s0 + p;
+    double bp = s - s0;
+    double err = (s0 - (s - bp)) + (p - bp);
+    *comp += err;
+    *sum = s;
+}
+
+// flow_depth_t[si] (solver_compact.py:628-630) from a depth array; side 0
+// keeps the field's initial zero.
+__device__ __forceinline__ float flow_depth_of(const nhf_mesh &m, const float *depth, int si)
+{
+    if (si == 0) return 0.0f;
+    int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
+    float zl = m.bed[el], zh = m.bed[eh];
+    float head = maxf(zl + __ldcg(depth + el), zh + __ldcg(depth + eh));
+    return maxf(head - maxf(maxf(zl, zh), kDh), 0.01f);
+}
+
+// StepClock.choose (clock.py:94-167)
+__device__ __forceinline__ void clock_choose(const Dev &d, Ctl *c, float candidate, int slot)
+{
+    uint32_t *row = c->trace + slot * NHF_TRACE_COLS;
+    c->active = 0; c->dt = 0.0f; c->local = 0.0f; c->end_local = 0.0f;
+    uint32_t now_hi = c->now[0], now_lo = c->now[1];
+    uint32_t target_hi = c->next[0], target_lo = c->next[1];
+    if (!(now_hi < target_hi || (now_hi == target_hi && now_lo < target_lo))) return;
+    if (!(candidate >= d.min_dt)) { row[3] = NHF_STEP_BAD_CFL; return; }
+    uint32_t borrow = now_lo > target_lo ? 1u : 0u;
+    uint32_t rem_hi = target_hi - now_hi - borrow;
+    uint32_t rem_lo = target_lo - now_lo;
+    float remaining = __uint2float_rn(rem_hi) * (1.0f / 256.0f) + __uint2float_rn(rem_lo) * 0x1p-40f;
+    float chosen = minf(minf(candidate, 1.0f), remaining);
+    row[4] = __float_as_uint(candidate);
+    row[5] = chosen < minf(candidate, 1.0f) ? 1u : 0u;
+    uint32_t bits = __float_as_uint(chosen);
+    int exponent = (int)((bits >> 23) & 255u) - 127;
+    uint32_t mantissa = (bits & 0x7fffffu) | 0x800000u;
+    uint32_t dt_hi = 0, dt_lo = 0;
+    if (!(chosen > 0.0f) || exponent < -40 || exponent > 0) { row[3] = NHF_STEP_BAD_DT; return; }
+    int shift = exponent + 17;
+    if (shift >= 0) {
+        dt_lo = mantissa << shift;
+        if (shift >= 9) dt_hi = mantissa >> (32 - shift);
+    } else {
+        int right = -shift;
+        dt_lo = mantissa >> right;
+        uint32_t dropped = mantissa & ((1u << right) - 1u);
+        uint32_t half = 1u << (right - 1);
+        if (dropped > half || (dropped == half && (dt_lo & 1u) != 0)) dt_lo += 1;
+    }
+    if (dt_hi == 0 && dt_lo == 0) { row[3] = NHF_STEP_BAD_DT; return; }
+    bool exceeds = dt_hi > rem_hi || (dt_hi == rem_hi && dt_lo > rem_lo);
+    uint32_t diff_hi, diff_lo;
+    if (exceeds) {
+        diff_hi = dt_hi - rem_hi - (dt_lo < rem_lo ? 1u : 0u);
+        diff_lo = dt_lo - rem_lo;
+    } else {
+        diff_hi = rem_hi - dt_hi - (rem_lo < dt_lo ? 1u : 0u);
+        diff_lo = rem_lo - dt_lo;
+    }
+    uint32_t end_hi = now_hi, end_lo = now_lo;
+    if (diff_hi == 0 && diff_lo < kSnapTicks) { end_hi = target_hi; end_lo = target_lo; }
+    else if (exceeds) { row[3] = NHF_STEP_OVERSHOOT; return; }
+    else {
+        end_lo = now_lo + dt_lo;
+        end_hi = now_hi + dt_hi + (end_lo < now_lo ? 1u : 0u);
+    }
+    uint32_t origin_hi = c->origin[0], origin_lo = c->origin[1];
+    uint32_t local_hi = now_hi - origin_hi - (now_lo < origin_lo ? 1u : 0u);
+    uint32_t local_lo = now_lo - origin_lo;
+    uint32_t end_local_hi = end_hi - origin_hi - (end_lo < origin_lo ? 1u : 0u);
+    uint32_t end_local_lo = end_lo - origin_lo;
+    c->local = __uint2float_rn(local_hi) * (1.0f / 256.0f) + __uint2float_rn(local_lo) * 0x1p-40f;
+    c->end_local = __uint2float_rn(end_local_hi) * (1.0f / 256.0f) + __uint2float_rn(end_local_lo) * 0x1p-40f;
+    c->dt = chosen;
+    c->step_end[0] = end_hi; c->step_end[1] = end_lo;
+    c->active = 1;
+}
+
+// prepare_step (solver_compact.py:364-382) for trace slot c->slot; `depth` and
+// `q` are the current state (read through L2: written by other blocks).
+__device__ __forceinline__ void prepare_step(const Dev &d, Ctl *c, const float *depth, const float *q)
+{
+    const nhf_mesh &m = d.m;
+    clock_choose(d, c, c->ndt, c->slot);
+    if (!c->active) return;
+    c->limited_cells = 0; c->limited_faces = 0;
+    c->min_scale_bits = __float_as_uint(1.0f);
+    c->wet = 0;
+    for (int bi = 0; bi < m.b_num; ++bi) {
+        d.values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * (c->local + c->dt / 2.0f);
+        d.level_values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * c->end_local;
+    }
+    if (c->ndt < c->limit_value[0]) {
+        int si = c->cfl_arg;
+        int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
+        float h = flow_depth_of(m, depth, si);
+        c->limit_value[0] = c->ndt;
+        c->limit_value[1] = __ldcg(depth + el); c->limit_value[2] = __ldcg(depth + eh);
+        c->limit_value[3] = h;
+        c->limit_value[4] = __ldcg(q + si) / maxf(h, 1e-30f);
+        c->limit_ids[0] = si; c->limit_ids[1] = el; c->limit_ids[2] = eh;
+    }
+}
+
+// finish_step + StepClock.commit (solver_compact.py:384-391, clock.py:173-181)
+__device__ __forceinline__ void finish_step(Ctl *c)
+{
+    uint32_t *row = c->trace + c->slot * NHF_TRACE_COLS;
+    if (c->active) {
+        row[6] = c->limited_cells;
+        row[7] = c->limited_faces;
+        row[8] = c->min_scale_bits;
+        row[9] = c->wet;
+        c->now[0] = c->step_end[0]; c->now[1] = c->step_end[1];
+        row[0] = __float_as_uint(c->dt);
+        row[1] = c->step_end[0]; row[2] = c->step_end[1];
+        row[3] = NHF_STEP_COMPLETED;
+    }
+    c->slot += 1;
+}
+
+// PressureReconstruction.difference (pressure.py:118-129)
+__device__ __forceinline__ float pressure_difference(const Dev &d, const float *depth, int side, int lower,
+                                                     int higher, float raw)
+{
+    const nhf_mesh &m = d.m;
+    float result = raw;
+    int index = m.edge_index[side];
+    if (index >= 0 && depth[lower] > d.min_h && depth[higher] > d.min_h) {
+        int axis = m.topology[3 * side] == 2 ? 1 : 0;
+        float o0 = m.offsets[2 * index], o1 = m.offsets[2 * index + 1];
+        if (o0 != 0.0f) result -= d.gradients[2 * m.slots[2 * index] + axis] * o0;
+        if (o1 != 0.0f) result += d.gradients[2 * m.slots[2 * index + 1] + axis] * o1;
+    }
+    return result;
+}
+
+// boundary_neighbor_sum (solver_compact.py:135-149)
+__device__ __forceinline__ float boundary_neighbor_sum(float q, float left, float right, float lext, float rext)
+{
+    float result = left + right;
+    if (lext > 0.0f || rext > 0.0f) {
+        if (lext == 1.0f || rext == 1.0f) {
+            result = 2.0f * q;
+        } else {
+            float product = lext * rext;
+            result = ((1.0f - rext) * left + (1.0f - lext) * right
+                      + 2.0f * q * (lext + rext - 2.0f * product)) / (1.0f - product);
+        }
+    }
+    return result;
+}
+
+// ---------------------------------------------------------------- host side
+
+struct TiledBuild {
+    TilePlan plan{};
+    void *device_memory = nullptr;   // owned plan arrays (cudaFree on destroy)
+    size_t shared_bytes = 0;
+    int patterns = 0;
+};
+
+// Build the tile plan from the caller's device arrays (copied to the host
+// once). Returns 0 on success; a nonzero value with `why` set when the mesh
+// does not fit the tiled form (the caller then keeps the multi-pass form).
+int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, size_t why_len);
+// Enqueue one fused step (plus the hanging/theta pre-passes when needed).
+void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s);
+// Enqueue the batch epilogue: bring the state back into the caller's
+// buffers and refresh u, v.
+void tiled_enqueue_batch_end(const Dev &d, cudaStream_t s);
+// Copy the caller's rain_time into the second buffer (batch start).
+void tiled_enqueue_batch_start(const Dev &d, cudaStream_t s);
+
+}  // namespace nhf

@@ -26,82 +26,12 @@
 #include <string>
 
 #include "../../include/nhflood.h"
+#include "nhf_common.cuh"
 #include "nhf_math.cuh"
 
+using namespace nhf;
+
 namespace {
-
-constexpr int kBlock = 256;          // budget block = reference ei // 256
-constexpr float kDh = -999.0f;       // dh_t without gates (solver_compact.py:405)
-constexpr uint32_t kSnapTicks = 1099512u;  // ceil(1e-6 * 2**40) (clock.py:11)
-constexpr unsigned long long kCflEmpty = 0xFFFFFFFFFFFFFFFFULL;
-
-struct Ctl {
-    uint32_t now[2], next[2], origin[2], step_end[2];
-    float dt, local, end_local, ndt;
-    int32_t active, slot, raining, cfl_arg;
-    uint32_t limited_cells, limited_faces, min_scale_bits, wet;
-    unsigned long long cfl_packed;
-    uint32_t done_blocks;
-    uint32_t pad;
-    float limit_value[5];
-    int32_t limit_ids[3];
-    uint32_t trace[NHF_MAX_BATCH * NHF_TRACE_COLS];
-};
-
-struct Dev {
-    nhf_mesh m;
-    float g, neg_g, afa, sita, half_rest, seven_thirds, min_h, min_dt;
-    int32_t terms, blocks, batch_size, theta_one;
-    Ctl *ctl;
-    const float *coef;
-    float *values, *level_values, *rain_rates, *sdc, *donor_scale, *face_qn, *eq, *gradients;
-    double *acc_sum, *acc_comp;
-    const uint32_t *begin;  // device copy of {next_hi, next_lo, origin_hi, origin_lo}
-};
-
-__device__ __forceinline__ float maxf(float a, float b) { return a > b ? a : b; }
-__device__ __forceinline__ float minf(float a, float b) { return b < a ? b : a; }
-
-// ---------------------------------------------------------------- reductions
-
-__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
-{
-    for (int o = 16; o > 0; o >>= 1) {
-        unsigned long long w = __shfl_down_sync(0xffffffffu, v, o);
-        v = w < v ? w : v;
-    }
-    return v;
-}
-
-// Canonical pairwise tree over the 256 cells of one budget block:
-// slot i += slot i + stride for stride 128 .. 1. Returns the sum in thread 0.
-__device__ double block_tree(double v, double *sh)
-{
-    const int t = threadIdx.x;
-    sh[t] = v;
-    __syncthreads();
-    for (int stride = 128; stride >= 32; stride >>= 1) {
-        if (t < stride) sh[t] += sh[t + stride];
-        __syncthreads();
-    }
-    double r = 0.0;
-    if (t < 32) {
-        r = sh[t];
-        for (int stride = 16; stride >= 1; stride >>= 1) r += __shfl_down_sync(0xffffffffu, r, stride);
-    }
-    __syncthreads();
-    return r;
-}
-
-__device__ __forceinline__ void acc_add(double *sum, double *comp, double p)
-{
-    double s0 = *sum;
-    double s = s0 + p;
-    double bp = s - s0;
-    double err = (s0 - (s - bp)) + (p - bp);
-    *comp += err;
-    *sum = s;
-}
 
 // --------------------------------------------------------------- small kernels
 
@@ -120,8 +50,10 @@ __global__ void k_initialize(Dev d)
 }
 
 // clock.begin on the device (clock.py:75-92): the target and origin words are
-// kernel arguments, updated in the instantiated graph before each replay.
-__global__ void k_begin(Dev d, uint32_t next_hi, uint32_t next_lo, uint32_t origin_hi, uint32_t origin_lo)
+// kernel arguments, updated in the instantiated graph before each replay. The
+// tiled form also prepares slot 0 here (each fused step prepares the next).
+__global__ void k_begin(Dev d, uint32_t next_hi, uint32_t next_lo, uint32_t origin_hi, uint32_t origin_lo,
+                        int prepare_first)
 {
     Ctl *c = d.ctl;
     int t = threadIdx.x;
@@ -131,124 +63,36 @@ __global__ void k_begin(Dev d, uint32_t next_hi, uint32_t next_lo, uint32_t orig
         c->slot = 0;
     }
     for (int i = t; i < NHF_MAX_BATCH * NHF_TRACE_COLS; i += blockDim.x) c->trace[i] = 0u;
+    __syncthreads();
+    if (prepare_first && t == 0) prepare_step(d, c, d.m.depth, d.m.q);
 }
 
-// Recompute flow_depth_t[si] (solver_compact.py:628-630) from the unchanged
-// state; side 0 keeps the field's initial zero.
-__device__ __forceinline__ float flow_depth_of(const nhf_mesh &m, int si)
-{
-    if (si == 0) return 0.0f;
-    int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
-    float head = maxf(m.bed[el] + m.depth[el], m.bed[eh] + m.depth[eh]);
-    return maxf(head - maxf(maxf(m.bed[el], m.bed[eh]), kDh), 0.01f);
-}
-
-__device__ void clock_choose(const Dev &d, Ctl *c, float candidate, int slot)
-{
-    uint32_t *row = c->trace + slot * NHF_TRACE_COLS;
-    c->active = 0; c->dt = 0.0f; c->local = 0.0f; c->end_local = 0.0f;
-    uint32_t now_hi = c->now[0], now_lo = c->now[1];
-    uint32_t target_hi = c->next[0], target_lo = c->next[1];
-    if (!(now_hi < target_hi || (now_hi == target_hi && now_lo < target_lo))) return;
-    if (!(candidate >= d.min_dt)) { row[3] = NHF_STEP_BAD_CFL; return; }
-    uint32_t borrow = now_lo > target_lo ? 1u : 0u;
-    uint32_t rem_hi = target_hi - now_hi - borrow;
-    uint32_t rem_lo = target_lo - now_lo;
-    float remaining = __uint2float_rn(rem_hi) * (1.0f / 256.0f) + __uint2float_rn(rem_lo) * 0x1p-40f;
-    float chosen = minf(minf(candidate, 1.0f), remaining);
-    row[4] = __float_as_uint(candidate);
-    row[5] = chosen < minf(candidate, 1.0f) ? 1u : 0u;
-    uint32_t bits = __float_as_uint(chosen);
-    int exponent = (int)((bits >> 23) & 255u) - 127;
-    uint32_t mantissa = (bits & 0x7fffffu) | 0x800000u;
-    uint32_t dt_hi = 0, dt_lo = 0;
-    if (!(chosen > 0.0f) || exponent < -40 || exponent > 0) { row[3] = NHF_STEP_BAD_DT; return; }
-    int shift = exponent + 17;
-    if (shift >= 0) {
-        dt_lo = mantissa << shift;
-        if (shift >= 9) dt_hi = mantissa >> (32 - shift);
-    } else {
-        int right = -shift;
-        dt_lo = mantissa >> right;
-        uint32_t dropped = mantissa & ((1u << right) - 1u);
-        uint32_t half = 1u << (right - 1);
-        if (dropped > half || (dropped == half && (dt_lo & 1u) != 0)) dt_lo += 1;
-    }
-    if (dt_hi == 0 && dt_lo == 0) { row[3] = NHF_STEP_BAD_DT; return; }
-    bool exceeds = dt_hi > rem_hi || (dt_hi == rem_hi && dt_lo > rem_lo);
-    uint32_t diff_hi, diff_lo;
-    if (exceeds) {
-        diff_hi = dt_hi - rem_hi - (dt_lo < rem_lo ? 1u : 0u);
-        diff_lo = dt_lo - rem_lo;
-    } else {
-        diff_hi = rem_hi - dt_hi - (rem_lo < dt_lo ? 1u : 0u);
-        diff_lo = rem_lo - dt_lo;
-    }
-    uint32_t end_hi = now_hi, end_lo = now_lo;
-    if (diff_hi == 0 && diff_lo < kSnapTicks) { end_hi = target_hi; end_lo = target_lo; }
-    else if (exceeds) { row[3] = NHF_STEP_OVERSHOOT; return; }
-    else {
-        end_lo = now_lo + dt_lo;
-        end_hi = now_hi + dt_hi + (end_lo < now_lo ? 1u : 0u);
-    }
-    uint32_t origin_hi = c->origin[0], origin_lo = c->origin[1];
-    uint32_t local_hi = now_hi - origin_hi - (now_lo < origin_lo ? 1u : 0u);
-    uint32_t local_lo = now_lo - origin_lo;
-    uint32_t end_local_hi = end_hi - origin_hi - (end_lo < origin_lo ? 1u : 0u);
-    uint32_t end_local_lo = end_lo - origin_lo;
-    c->local = __uint2float_rn(local_hi) * (1.0f / 256.0f) + __uint2float_rn(local_lo) * 0x1p-40f;
-    c->end_local = __uint2float_rn(end_local_hi) * (1.0f / 256.0f) + __uint2float_rn(end_local_lo) * 0x1p-40f;
-    c->dt = chosen;
-    c->step_end[0] = end_hi; c->step_end[1] = end_lo;
-    c->active = 1;
-}
-
-// prepare_step (solver_compact.py:364-382)
+// prepare_step (solver_compact.py:364-382), multi-pass form
 __global__ void k_prepare(Dev d)
 {
     if (threadIdx.x != 0) return;
-    Ctl *c = d.ctl;
-    const nhf_mesh &m = d.m;
-    clock_choose(d, c, c->ndt, c->slot);
-    if (!c->active) return;
-    c->limited_cells = 0; c->limited_faces = 0;
-    c->min_scale_bits = __float_as_uint(1.0f);
-    c->wet = 0;
-    for (int bi = 0; bi < m.b_num; ++bi) {
-        d.values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * (c->local + c->dt / 2.0f);
-        d.level_values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * c->end_local;
-    }
-    if (c->ndt < c->limit_value[0]) {
-        int si = c->cfl_arg;
-        int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
-        float h = flow_depth_of(m, si);
-        c->limit_value[0] = c->ndt;
-        c->limit_value[1] = m.depth[el]; c->limit_value[2] = m.depth[eh];
-        c->limit_value[3] = h;
-        c->limit_value[4] = m.q[si] / maxf(h, 1e-30f);
-        c->limit_ids[0] = si; c->limit_ids[1] = el; c->limit_ids[2] = eh;
-    }
+    prepare_step(d, d.ctl, d.m.depth, d.m.q);
 }
 
 // ------------------------------------------------------ pressure (pressure.py)
 
-__device__ void face_difference(const Dev &d, int cell, int direction, int axis,
+__device__ void face_difference(const Dev &d, const float *depth, int cell, int direction, int axis,
                                 float &value_out, float &distance_out, int &usable_out)
 {
     const nhf_mesh &m = d.m;
     float value = 0.0f, distance = 0.0f, total = 0.0f;
     int usable = 1;
-    float eta = m.bed[cell] + m.depth[cell];
+    float eta = m.bed[cell] + depth[cell];
     int start = m.face_ptr[4 * cell + direction];
     int count = m.face_count[4 * cell + direction];
     for (int j = 0; j < count; ++j) {
         int side = m.isl_data[start + j];
         int other = m.topology[3 * side + 1] + m.topology[3 * side + 2] - cell;
-        if (other == 0 || m.depth[other] <= d.min_h) {
+        if (other == 0 || depth[other] <= d.min_h) {
             usable = 0;
         } else {
             float weight = m.length[side];
-            value += weight * ((m.bed[other] + m.depth[other]) - eta);
+            value += weight * ((m.bed[other] + depth[other]) - eta);
             float delta = axis == 1 ? m.y[other] - m.y[cell] : m.x[other] - m.x[cell];
             distance += weight * delta;
             total += weight;
@@ -266,34 +110,21 @@ __global__ void k_pressure(Dev d)
     int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= m.hang_cells) return;
     int cell = m.hcells[slot];
+    const float *depth = cur_depth(d, d.ctl->parity);
     for (int axis = 0; axis < 2; ++axis) {
         if (m.axes[2 * slot + axis] != 1) continue;
         float value = 0.0f;
-        if (m.depth[cell] > d.min_h) {
+        if (depth[cell] > d.min_h) {
             int minus = axis == 1 ? 2 : 0, plus = axis == 1 ? 3 : 1;
             float dm, xm, dp, xp; int okm, okp;
-            face_difference(d, cell, minus, axis, dm, xm, okm);
-            face_difference(d, cell, plus, axis, dp, xp, okp);
+            face_difference(d, depth, cell, minus, axis, dm, xm, okm);
+            face_difference(d, depth, cell, plus, axis, dp, xp, okp);
             if (okm && okp) value = (dp - dm) / (xp - xm);
             else if (okm) value = dm / xm;
             else if (okp) value = dp / xp;
         }
         d.gradients[2 * slot + axis] = value;
     }
-}
-
-__device__ __forceinline__ float pressure_difference(const Dev &d, int side, int lower, int higher, float raw)
-{
-    const nhf_mesh &m = d.m;
-    float result = raw;
-    int index = m.edge_index[side];
-    if (index >= 0 && m.depth[lower] > d.min_h && m.depth[higher] > d.min_h) {
-        int axis = m.topology[3 * side] == 2 ? 1 : 0;
-        float o0 = m.offsets[2 * index], o1 = m.offsets[2 * index + 1];
-        if (o0 != 0.0f) result -= d.gradients[2 * m.slots[2 * index] + axis] * o0;
-        if (o1 != 0.0f) result += d.gradients[2 * m.slots[2 * index + 1] + axis] * o1;
-    }
-    return result;
 }
 
 // ----------------------------------------------------------- theta < 1 faces
@@ -304,37 +135,23 @@ __global__ void k_face_qn(Dev d)
     if (!d.ctl->active) return;
     int ei = blockIdx.x * blockDim.x + threadIdx.x;
     if (ei >= m.e_num) return;
+    const float *q = cur_q(d, d.ctl->parity);
     for (int dd = 0; dd < 4; ++dd) {
         int start = m.face_ptr[4 * ei + dd], count = m.face_count[4 * ei + dd];
         float result = 0.0f;
         if (count == 1) {
-            result = m.q[m.isl_data[start]];
+            result = q[m.isl_data[start]];
         } else if (count > 1) {
             float total = 0.0f, width = 0.0f;
             for (int o = 0; o < count; ++o) {
                 int side = m.isl_data[start + o];
-                total += m.q[side] * m.length[side];
+                total += q[side] * m.length[side];
                 width += m.length[side];
             }
             result = total / width;
         }
         d.face_qn[4 * ei + dd] = result;
     }
-}
-
-__device__ __forceinline__ float boundary_neighbor_sum(float q, float left, float right, float lext, float rext)
-{
-    float result = left + right;
-    if (lext > 0.0f || rext > 0.0f) {
-        if (lext == 1.0f || rext == 1.0f) {
-            result = 2.0f * q;
-        } else {
-            float product = lext * rext;
-            result = ((1.0f - rext) * left + (1.0f - lext) * right
-                      + 2.0f * q * (lext + rext - 2.0f * product)) / (1.0f - product);
-        }
-    }
-    return result;
 }
 
 // ------------------------------------------------------------ side momentum
@@ -357,7 +174,7 @@ __global__ void k_sides(Dev d)
     float xq = m.q[si];
     float xwh = maxf(hl, hr) - maxf(maxf(zl, zh), kDh);
     float difference = hr - hl;
-    if (kHanging) difference = pressure_difference(d, si, el, eh, difference);
+    if (kHanging) difference = pressure_difference(d, m.depth, si, el, eh, difference);
     float xdq = (d.neg_g * difference / dx) * maxf(xwh, 0.0f) * dt;
     float n = m.side_n[si];
     float ratio = 0.0f;
@@ -574,22 +391,6 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d)
 
 // --------------------------------------------------------------------- CFL
 
-__device__ void finish_step(const Dev &d, Ctl *c)
-{
-    uint32_t *row = c->trace + c->slot * NHF_TRACE_COLS;
-    if (c->active) {
-        row[6] = c->limited_cells;
-        row[7] = c->limited_faces;
-        row[8] = c->min_scale_bits;
-        row[9] = c->wet;
-        c->now[0] = c->step_end[0]; c->now[1] = c->step_end[1];
-        row[0] = __float_as_uint(c->dt);
-        row[1] = c->step_end[0]; row[2] = c->step_end[1];
-        row[3] = NHF_STEP_COMPLETED;
-    }
-    c->slot += 1;
-}
-
 // compute_cfl (solver_compact.py:617-641) + finish_step (384-391).
 // Packed key (cfl bits << 32 | side): the minimum is the smallest CFL and,
 // among equal values, the lowest side id, as the reference's second pass.
@@ -641,7 +442,7 @@ __global__ void k_cfl(Dev d, int finish)
         c->ndt = __uint_as_float((uint32_t)(packed >> 32));
         c->cfl_arg = (int32_t)(packed & 0xffffffffu);
     }
-    if (finish) finish_step(d, c);
+    if (finish) finish_step(c);
 }
 
 // ------------------------------------------------------- setup and sampling
@@ -736,7 +537,26 @@ __global__ void k_cfl_edge(Dev d, float *out)
     const Ctl *c = d.ctl;
     out[0] = c->ndt;
     out[1] = __int_as_float(c->cfl_arg);
-    out[2] = flow_depth_of(d.m, c->cfl_arg);
+    out[2] = flow_depth_of(d.m, d.m.depth, c->cfl_arg);
+}
+
+// eq_t from the current discharges (solver_compact.py:548-559 face sums)
+__global__ void k_eq(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    int ei = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (ei >= m.e_num) return;
+    float fl[4];
+    for (int dd = 0; dd < 4; ++dd) {
+        float total = 0.0f;
+        int p = m.face_ptr[4 * ei + dd], cnt = m.face_count[4 * ei + dd];
+        for (int j = 0; j < cnt; ++j) {
+            int si = m.isl_data[p + j];
+            total += m.q[si] * m.length[si];
+        }
+        fl[dd] = total;
+    }
+    reinterpret_cast<float4 *>(d.eq)[ei] = make_float4(fl[0], fl[1], fl[2], fl[3]);
 }
 
 }  // namespace
@@ -763,6 +583,9 @@ struct nhf_handle {
     cudaGraphExec_t graph = nullptr;
     cudaGraphNode_t begin_node = nullptr;
     cudaKernelNodeParams begin_params{};
+    TiledBuild tb{};
+    bool tiled = false;
+    std::string path = "multipass";
     std::string err;
 };
 
@@ -833,8 +656,14 @@ int build_graph(nhf_handle *h)
 {
     cudaGraph_t g = nullptr;
     CK(h, cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
-    k_begin<<<1, 256, 0, h->s>>>(h->dev, 0u, 0u, 0u, 0u);
-    for (int i = 0; i < h->p.batch_size; ++i) enqueue_step(h);
+    k_begin<<<1, 256, 0, h->s>>>(h->dev, 0u, 0u, 0u, 0u, h->tiled ? 1 : 0);
+    if (h->tiled) {
+        tiled_enqueue_batch_start(h->dev, h->s);
+        for (int i = 0; i < h->p.batch_size; ++i) tiled_enqueue_step(h->dev, h->tb, h->s);
+        tiled_enqueue_batch_end(h->dev, h->s);
+    } else {
+        for (int i = 0; i < h->p.batch_size; ++i) enqueue_step(h);
+    }
     cudaMemcpyAsync(h->h_trace, h->ctl->trace, sizeof(uint32_t) * NHF_TRACE_COLS * h->p.batch_size,
                     cudaMemcpyDeviceToHost, h->s);
     cudaError_t e = cudaStreamEndCapture(h->s, &g);
@@ -905,6 +734,22 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     const int hc = mesh->hang_cells > 0 ? mesh->hang_cells : 1;
     const int nr = mesh->n_rates > 0 ? mesh->n_rates : 1;
     const bool theta_one = params->sita == 1.0f;
+    // The caller may still be writing the mesh arrays on its stream.
+    CKC(cudaEventRecord(h->ev_in, h->user));
+    CKC(cudaStreamWaitEvent(h->s, h->ev_in, 0));
+    // Fused tiled step when the mesh allows it (params->path == 0).
+    if (params->path == 0) {
+        char why[256] = {0};
+        if (tiled_build(*mesh, h->s, &h->tb, why, sizeof(why)) == 0) {
+            h->tiled = true;
+            char buf[128];
+            snprintf(buf, sizeof(buf), "tiled(tile=%d,patterns=%d,smem=%zu)", h->tb.plan.tile, h->tb.patterns,
+                     h->tb.shared_bytes);
+            h->path = buf;
+        } else {
+            h->path = std::string("multipass (") + why + ")";
+        }
+    }
     // scratch layout (bytes, 256-aligned pieces)
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
@@ -921,6 +766,9 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     size_t o_accs = take(sizeof(double) * (size_t)blocks * T);
     size_t o_accc = take(sizeof(double) * (size_t)blocks * T);
     size_t o_begin = take(sizeof(uint32_t) * 4);
+    size_t o_db = h->tiled ? take(sizeof(float) * (size_t)e) : 0;
+    size_t o_qb = h->tiled ? take(sizeof(float) * (size_t)sn) : 0;
+    size_t o_rb = h->tiled ? take(sizeof(float) * (size_t)e) : 0;
     CKC(cudaMalloc(&h->scratch, off));
     CKC(cudaMemsetAsync(h->scratch, 0, off, h->s));
     char *base = (char *)h->scratch;
@@ -956,7 +804,12 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     d.gradients = (float *)(base + o_grad);
     d.acc_sum = (double *)(base + o_accs);
     d.acc_comp = (double *)(base + o_accc);
-    d.begin = h->d_begin;
+    if (h->tiled) {
+        d.depth_b = (float *)(base + o_db);
+        d.q_b = (float *)(base + o_qb);
+        d.rain_time_b = (float *)(base + o_rb);
+        d.plan = h->tb.plan;
+    }
     // control block initial values
     Ctl init{};
     init.limit_value[0] = __builtin_inff();
@@ -975,6 +828,7 @@ int nhf_destroy(nhf_handle *h)
     if (h->s) cudaStreamSynchronize(h->s);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     if (h->graph_def) cudaGraphDestroy(h->graph_def);
+    if (h->tb.device_memory) cudaFree(h->tb.device_memory);
     if (h->scratch) cudaFree(h->scratch);
     if (h->h_begin) cudaFreeHost(h->h_begin);
     if (h->h_trace) cudaFreeHost(h->h_trace);
@@ -1091,7 +945,8 @@ int nhf_run_batch_async(nhf_handle *h, const uint32_t target[2], const uint32_t 
     if (!h->graph) { rc = build_graph(h); if (rc) return rc; }
     Dev d = h->dev;
     uint32_t w[4] = {target[0], target[1], origin[0], origin[1]};
-    void *args[5] = {&d, &w[0], &w[1], &w[2], &w[3]};
+    int prepare_first = h->tiled ? 1 : 0;
+    void *args[6] = {&d, &w[0], &w[1], &w[2], &w[3], &prepare_first};
     cudaKernelNodeParams kp = h->begin_params;
     kp.kernelParams = args;
     kp.extra = nullptr;
@@ -1207,6 +1062,7 @@ int nhf_read_eq(nhf_handle *h, float *eq)
 {
     if (!h || !eq) return NHF_EINVAL;
     int rc = enter(h); if (rc) return rc;
+    k_eq<<<grid_for(h->m.e_num - 1, 256), 256, 0, h->s>>>(h->dev);
     CK(h, cudaMemcpyAsync(eq, h->dev.eq, sizeof(float) * 4 * (size_t)h->m.e_num, cudaMemcpyDeviceToDevice, h->s));
     return leave(h);
 }
@@ -1222,6 +1078,8 @@ int nhf_read_gradients(nhf_handle *h, float *gradients)
 }
 
 void *nhf_stream(nhf_handle *h) { return h ? (void *)h->s : nullptr; }
+
+const char *nhf_path(const nhf_handle *h) { return h ? h->path.c_str() : ""; }
 
 int nhf_synchronize(nhf_handle *h)
 {

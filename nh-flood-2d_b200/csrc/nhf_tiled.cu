@@ -1,0 +1,958 @@
+// Fused local-inertial step: one kernel launch per time step.
+//
+// Cells are split into tiles of T consecutive reference indices (T = 1024,
+// 512 or 256; a tile covers T/256 whole budget blocks). A 256-thread block
+// owns one tile and stages in shared memory the tile (ring 0) and three rings
+// of neighbours (graph distance 1..3), because one step of the reference's
+// passes (solver_compact.py:439-613) and its CFL (617-641) reach that far:
+//   ring <= 3  water level and bed           -> momentum q* of faces(ring <= 2)
+//   ring <= 2  donor factor from those q*    -> final q of faces(ring <= 1)
+//   ring <= 1  depth update from final q     -> CFL of the sides the tile owns
+// Every quantity is computed with the reference's operation order, so a cell
+// that several tiles recompute gets the same bits everywhere; each output
+// (depth, side q, extrema, budget block) has exactly one writer, its owner
+// tile. depth, q and rain_time are double-buffered so that halo reads never
+// see a neighbour's update of the same step. The last block to finish commits
+// the clock, writes the trace row and prepares the next step, so a batch is
+// one launch per step in a CUDA graph.
+//
+// The host planner below builds, per tile, the ring lists, the local side
+// list and a local face CSR, all relative to the tile's first cell and side.
+// Tiles whose relative tables coincide (regular grids numbered tile by tile)
+// share one pattern, so the index tables stay in L2.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "nhf_common.cuh"
+#include "nhf_math.cuh"
+
+namespace nhf {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxSharedBytes = 110 * 1024;
+constexpr uint8_t kOwned = 1, kFinal = 2;
+
+// ----------------------------------------------------------------- kernels
+
+template <int CPT>
+struct CellTerms {
+    float removed[CPT], floor_v[CPT], level[CPT][5], discharge[CPT];
+    int bi[CPT], kind[CPT];
+};
+
+struct Tile {
+    int n_ext, n_r0, n_r01, n_r012, n_sides, n_owned, n_qf, r0off;
+    int cbase, sbase;
+    const int32_t *ext;
+    const int32_t *srel;
+    const uint32_t *lohi;
+    const uint32_t *fdesc;
+    const uint16_t *fidx;
+};
+
+// Face flux sums of one local cell (solver_compact.py:548-557) in the
+// reference's CSR order.
+__device__ __forceinline__ void face_sums(const Tile &tl, const float *sh_q, const float *sh_len, int slot,
+                                          float fl[4])
+{
+    uint32_t fd = tl.fdesc[slot];
+    int k = (int)(fd & 0xffffu);
+    uint32_t counts = fd >> 16;
+    for (int dd = 0; dd < 4; ++dd) {
+        int cnt = (int)((counts >> (4 * dd)) & 15u);
+        float face_flux = 0.0f;
+        for (int j = 0; j < cnt; ++j) {
+            int ls = tl.fidx[k++];
+            face_flux += sh_q[ls] * sh_len[ls];
+        }
+        fl[dd] = face_flux;
+    }
+}
+
+template <bool kThetaOne, bool kHanging, int CPT>
+__global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double sh_tree[kThreads];
+    __shared__ unsigned long long sh_min[kThreads / 32];
+    __shared__ uint32_t sh_cnt[3];
+    __shared__ uint32_t sh_minbits;
+    __shared__ int sh_last;
+    Ctl *c = d.ctl;
+    const nhf_mesh &m = d.m;
+    const int tid = threadIdx.x;
+
+    if (tid == 0) { sh_cnt[0] = sh_cnt[1] = sh_cnt[2] = 0u; sh_minbits = __float_as_uint(1.0f); }
+    const int active = c->active;
+    if (!active) {
+        // No physics this slot: the last block advances the slot and prepares the next.
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            unsigned ticket = atomicAdd(&c->done_blocks, 1u);
+            if (ticket == gridDim.x - 1) {
+                c->done_blocks = 0;
+                finish_step(c);
+                if (c->slot < d.batch_size) prepare_step(d, c, cur_depth(d, c->parity), cur_q(d, c->parity));
+            }
+        }
+        return;
+    }
+    const int parity = c->parity;
+    const float dt = c->dt;
+    const int raining = c->raining;
+    const float *depth_in = parity ? d.depth_b : m.depth;
+    float *depth_out = parity ? m.depth : d.depth_b;
+    const float *q_in = parity ? d.q_b : m.q;
+    float *q_out = parity ? m.q : d.q_b;
+    const float *rt_in = parity ? d.rain_time_b : m.rain_time;
+    float *rt_out = parity ? m.rain_time : d.rain_time_b;
+
+    const TilePlan &P = d.plan;
+    Tile tl;
+    {
+        const int t = blockIdx.x;
+        const int pat = P.tile_pattern[t];
+        const int32_t *cnt = P.p_counts + 8 * pat;
+        const int32_t *off = P.p_offsets + 4 * pat;
+        tl.n_ext = cnt[0]; tl.n_r0 = cnt[1]; tl.n_r01 = cnt[2]; tl.n_r012 = cnt[3];
+        tl.n_sides = cnt[4]; tl.n_owned = cnt[5]; tl.n_qf = cnt[6]; tl.r0off = cnt[7];
+        tl.cbase = P.tile_cbase[t];
+        tl.sbase = P.tile_sbase[t];
+        tl.ext = P.ext_rel + off[0];
+        tl.srel = P.side_rel + off[1];
+        tl.lohi = P.side_lohi + off[1];
+        tl.fdesc = P.face_desc + off[2];
+        tl.fidx = P.face_idx + off[3];
+    }
+    float *sh_h = reinterpret_cast<float *>(smem_raw);
+    float *sh_z = sh_h + P.max_ext;
+    float *sh_s = sh_z + P.max_ext;  // donor factor, then the new depth
+    int *sh_g = reinterpret_cast<int *>(sh_s + P.max_ext);
+    float *sh_q = reinterpret_cast<float *>(sh_g + P.max_ext);  // q*, then final q
+    float *sh_len = sh_q + P.max_sides;
+
+    // P0: stage water depth and bed of the tile and its three rings.
+    for (int i = tid; i < tl.n_ext; i += kThreads) {
+        int g = i ? tl.cbase + tl.ext[i] : 0;
+        sh_g[i] = g;
+        sh_h[i] = i ? depth_in[g] : m.depth[0];
+        sh_z[i] = m.bed[g];
+        sh_s[i] = 0.0f;  // donor_scale of the exterior sentinel stays 0
+    }
+    __syncthreads();
+
+    // P1: momentum (solver_compact.py:439-486) for every local side.
+    for (int j = tid; j < tl.n_sides; j += kThreads) {
+        const int gid = tl.sbase + tl.srel[j];
+        const uint32_t lh = tl.lohi[j];
+        const int a = (int)(lh & 0xffffu), b = (int)(lh >> 16);
+        float zl = sh_z[a], zh = sh_z[b];
+        float hl = zl + sh_h[a], hr = zh + sh_h[b];
+        float dx = d.sdc[gid];
+        float xq = q_in[gid];
+        float xwh = maxf(hl, hr) - maxf(maxf(zl, zh), kDh);
+        float difference = hr - hl;
+        if (kHanging) {
+            int index = m.edge_index[gid];
+            if (index >= 0 && sh_h[a] > d.min_h && sh_h[b] > d.min_h) {
+                int axis = m.topology[3 * gid] == 2 ? 1 : 0;
+                float o0 = m.offsets[2 * index], o1 = m.offsets[2 * index + 1];
+                if (o0 != 0.0f) difference -= d.gradients[2 * m.slots[2 * index] + axis] * o0;
+                if (o1 != 0.0f) difference += d.gradients[2 * m.slots[2 * index + 1] + axis] * o1;
+            }
+        }
+        float xdq = (d.neg_g * difference / dx) * maxf(xwh, 0.0f) * dt;
+        float n = m.side_n[gid];
+        float ratio = 0.0f;
+        if (xq != 0.0f) ratio = xq / pow_f32(maxf(xwh, 0.00001f), d.seven_thirds);
+        float xf = 1.0f + d.g * dt * (n * n) * fabsf(ratio);
+        float nb;
+        if (kThetaOne) {
+            nb = 0.0f + 0.0f;
+        } else {
+            int so = m.topology[3 * gid];
+            int dl = so == 2 ? 0 : 2, dr = so == 2 ? 1 : 3;
+            int ga = sh_g[a], gb = sh_g[b];
+            nb = boundary_neighbor_sum(xq, d.face_qn[4 * ga + dl], d.face_qn[4 * gb + dr],
+                                       m.open_face[4 * ga + dl], m.open_face[4 * gb + dr]);
+        }
+        float new_q = (d.sita * xq + d.half_rest * nb + xdq) / xf;
+        new_q = xwh < d.min_h ? 0.0f : new_q;
+        new_q *= m.sbf[gid] == 1 ? 0.0f : 1.0f;
+        sh_q[j] = new_q;
+        sh_len[j] = m.length[gid];
+    }
+    __syncthreads();
+
+    // P2: donor factor (solver_compact.py:491-514) for rings 0..2.
+    {
+        uint32_t my_limited = 0;
+        uint32_t my_min = __float_as_uint(1.0f);
+        for (int i = 1 + tid; i <= tl.n_r012; i += kThreads) {
+            const int g = sh_g[i];
+            int bi = m.boundary_id[g];
+            int kind = bi >= 0 ? m.kind[bi] : -1;
+            float discharge = 0.0f;
+            if (kind == 1) discharge = d.values[bi] * m.weight[g];
+            float rainq = 0.0f;
+            if (raining) rainq = d.rain_rates[m.rain_index[g]];
+            float pipe = 0.0f;
+            float positive = (maxf(pipe, 0.0f) + maxf(discharge, 0.0f)) * dt;
+            float area = m.area[g];
+            float available = sh_h[i] * area + positive + rainq * dt * area;
+            float outgoing = (maxf(-pipe, 0.0f) + maxf(-discharge, 0.0f)) * dt;
+            uint32_t fd = tl.fdesc[i];
+            int k = (int)(fd & 0xffffu);
+            uint32_t counts = fd >> 16;
+            for (int dd = 0; dd < 4; ++dd) {
+                int cntd = (int)((counts >> (4 * dd)) & 15u);
+                for (int jj = 0; jj < cntd; ++jj) {
+                    int ls = tl.fidx[k++];
+                    float signed_q = sh_q[ls] * sh_len[ls];
+                    if (dd == 0 || dd == 2) signed_q = -signed_q;
+                    outgoing += maxf(signed_q, 0.0f) * dt;
+                }
+            }
+            float sc = 1.0f;
+            if (outgoing > available && kind != 0) {
+                sc = available / outgoing;
+                if (i <= tl.n_r0) {
+                    my_limited += 1;
+                    uint32_t bits = __float_as_uint(sc);
+                    my_min = bits < my_min ? bits : my_min;
+                }
+            }
+            sh_s[i] = sc;
+        }
+        if (my_limited) {
+            atomicAdd(&sh_cnt[0], my_limited);
+            atomicMin(&sh_minbits, my_min);
+        }
+    }
+    __syncthreads();
+
+    // P3: final discharge of faces(ring <= 1) (solver_compact.py:516-522).
+    {
+        uint32_t my_faces = 0;
+        for (int j = tid; j < tl.n_qf; j += kThreads) {
+            const uint32_t lh = tl.lohi[j];
+            const int a = (int)(lh & 0xffffu), b = (int)(lh >> 16);
+            float q = sh_q[j];
+            int donor = q >= 0.0f ? a : b;
+            float sc = sh_s[donor];
+            if (j < tl.n_owned && q != 0.0f && sc < 1.0f) my_faces += 1;
+            sh_q[j] = q * sc;
+        }
+        if (my_faces) atomicAdd(&sh_cnt[1], my_faces);
+    }
+    __syncthreads();
+
+    // P4: sources and depth update (solver_compact.py:525-610). Ring 0 cells
+    // are mapped to threads as tile offset o = tid + 256 * k, so the cells of
+    // budget block k of the tile sit in thread order for the budget tree.
+    CellTerms<CPT> terms;
+    uint32_t my_wet = 0;
+    const uint32_t step_hi = c->step_end[0], step_lo = c->step_end[1];
+#pragma unroll
+    for (int kk = 0; kk < CPT; ++kk) {
+        terms.removed[kk] = 0.0f; terms.floor_v[kk] = 0.0f; terms.discharge[kk] = 0.0f;
+        for (int q5 = 0; q5 < 5; ++q5) terms.level[kk][q5] = 0.0f;
+        terms.bi[kk] = -1; terms.kind[kk] = -1;
+        const int o = tid + kThreads * kk;
+        const int slot = o - tl.r0off + 1;
+        if (o < tl.r0off || slot > tl.n_r0) continue;
+        const int g = tl.cbase + o;
+        int bi = m.boundary_id[g];
+        int kind = bi >= 0 ? m.kind[bi] : -1;
+        terms.bi[kk] = bi; terms.kind[kk] = kind;
+        float sc = sh_s[slot];
+        float pq = 0.0f;
+        float pipe = maxf(pq, 0.0f) + minf(pq, 0.0f) * sc;
+        float discharge = 0.0f;
+        if (kind == 1) {
+            float requested = d.values[bi] * m.weight[g];
+            discharge = maxf(requested, 0.0f) + minf(requested, 0.0f) * sc;
+            terms.discharge[kk] = discharge * dt;
+        }
+        float ssq = pipe + discharge;
+        float rainq = 0.0f;
+        if (raining) rainq = d.rain_rates[m.rain_index[g]];
+        float infil;
+        if (rainq > 0.0f) {
+            float rt = rt_in[g] + dt;
+            rt_out[g] = rt;
+            float f0 = m.f0[g], fc = m.fc[g];
+            float diff = f0 - fc;
+            infil = diff == 0.0f ? fc + 0.0f : fc + diff * exp_f32(-m.k[g] * rt / 3600.0f);
+            if (__float_as_uint(infil) != __float_as_uint(m.infiltration[g])) m.infiltration[g] = infil;
+        } else {
+            infil = m.infiltration[g];
+        }
+        float fl[4];
+        face_sums(tl, sh_q, sh_len, slot, fl);
+        float ql = fl[0], qr = fl[1], qb = fl[2], qt = fl[3];
+        float tq = ql - qr + qb - qt + ssq;
+        float ea = m.area[g];
+        float rain_depth = rainq * dt;
+        float increment = tq * dt / ea + rain_depth;
+        float previous = sh_h[slot];
+        float raw_depth = previous + increment;
+        float removed = minf(infil * dt, maxf(raw_depth, 0.0f));
+        raw_depth -= removed;
+        float floor_v = maxf(-raw_depth, 0.0f);
+        terms.removed[kk] = removed * ea;
+        terms.floor_v[kk] = floor_v * ea;
+        float depth;
+        if (kind == 0) {
+            float target = maxf(d.level_values[bi] - sh_z[slot], 0.0f);
+            terms.level[kk][0] = (target - previous) * ea;
+            terms.level[kk][1] = -(ql - qr + qb - qt) * dt;
+            terms.level[kk][2] = -pipe * dt;
+            terms.level[kk][3] = -rain_depth * ea;
+            terms.level[kk][4] = removed * ea;
+            depth = target;
+        } else {
+            depth = maxf(raw_depth, 0.0f);
+        }
+        depth_out[g] = depth;
+        sh_s[slot] = depth;
+        float h = maxf(depth, 0.01f);
+        float u = 0.0f, v = 0.0f;
+        if (depth >= d.min_h) {
+            u = (ql + qr) / m.height[g] / h / 2.0f;
+            v = (qb + qt) / m.width[g] / h / 2.0f;
+        }
+        float speed = sqrtf(u * u + v * v);
+        float ms = m.max_speed[g];
+        if (speed > ms) m.max_speed[g] = speed;
+        if (depth > m.max_depth[g]) {
+            m.max_depth[g] = depth;
+            m.peak_hi[g] = step_hi; m.peak_lo[g] = step_lo;
+        }
+        my_wet += depth >= d.min_h ? 1u : 0u;
+    }
+    // ring 1: the new depth only (for the CFL of owned sides)
+    for (int i = tl.n_r0 + 1 + tid; i <= tl.n_r01; i += kThreads) {
+        const int g = sh_g[i];
+        int bi = m.boundary_id[g];
+        int kind = bi >= 0 ? m.kind[bi] : -1;
+        float sc = sh_s[i];
+        float pq = 0.0f;
+        float pipe = maxf(pq, 0.0f) + minf(pq, 0.0f) * sc;
+        float discharge = 0.0f;
+        if (kind == 1) {
+            float requested = d.values[bi] * m.weight[g];
+            discharge = maxf(requested, 0.0f) + minf(requested, 0.0f) * sc;
+        }
+        float ssq = pipe + discharge;
+        float rainq = 0.0f;
+        if (raining) rainq = d.rain_rates[m.rain_index[g]];
+        float infil;
+        if (rainq > 0.0f) {
+            float rt = rt_in[g] + dt;
+            float f0 = m.f0[g], fc = m.fc[g];
+            float diff = f0 - fc;
+            infil = diff == 0.0f ? fc + 0.0f : fc + diff * exp_f32(-m.k[g] * rt / 3600.0f);
+        } else {
+            infil = m.infiltration[g];
+        }
+        float fl[4];
+        face_sums(tl, sh_q, sh_len, i, fl);
+        float tq = fl[0] - fl[1] + fl[2] - fl[3] + ssq;
+        float ea = m.area[g];
+        float rain_depth = rainq * dt;
+        float increment = tq * dt / ea + rain_depth;
+        float raw_depth = sh_h[i] + increment;
+        float removed = minf(infil * dt, maxf(raw_depth, 0.0f));
+        raw_depth -= removed;
+        float depth = kind == 0 ? maxf(d.level_values[bi] - sh_z[i], 0.0f) : maxf(raw_depth, 0.0f);
+        sh_s[i] = depth;
+    }
+    __syncthreads();
+
+    // Budget partials: one writer per (budget block, term), fixed tree.
+    {
+        const int T = d.terms;
+        const int B = m.b_num;
+#pragma unroll
+        for (int kk = 0; kk < CPT; ++kk) {
+            const int blk = (tl.cbase >> 8) + kk;
+            if (blk >= d.blocks) break;  // uniform across the block
+            double *acc_s = d.acc_sum + (size_t)blk * T;
+            double *acc_c = d.acc_comp + (size_t)blk * T;
+            for (int t = 0; t < T; ++t) {
+                float val = 0.0f;
+                if (t == 0) val = terms.removed[kk];
+                else if (t == 1) val = terms.kind[kk] == 0 ? 0.0f : terms.floor_v[kk];
+                else if (t == 2) val = terms.kind[kk] == 0 ? terms.floor_v[kk] : 0.0f;
+                else if (t == 3) val = 0.0f;  // pipe exchange: no coupling
+                else if (t < 4 + 5 * B) {
+                    int b = (t - 4) / 5;
+                    if (b == terms.bi[kk] && terms.kind[kk] == 0) val = terms.level[kk][(t - 4) % 5];
+                } else {
+                    int b = t - 4 - 5 * B;
+                    if (b == terms.bi[kk]) val = terms.discharge[kk];
+                }
+                if (!__syncthreads_or(val != 0.0f)) continue;
+                double sum = block_tree((double)val, sh_tree);
+                if (tid == 0) acc_add(acc_s + t, acc_c + t, sum);
+            }
+        }
+    }
+
+    // P5: owned sides: final q out, CFL with the new depths.
+    unsigned long long best = kCflEmpty;
+    for (int j = tid; j < tl.n_owned; j += kThreads) {
+        const int gid = tl.sbase + tl.srel[j];
+        const uint32_t lh = tl.lohi[j];
+        const int a = (int)(lh & 0xffffu), b = (int)(lh >> 16);
+        float qv = sh_q[j];
+        q_out[gid] = qv;
+        if (a != 0 && b != 0) {
+            float zl = sh_z[a], zh = sh_z[b];
+            float head = maxf(zl + sh_s[a], zh + sh_s[b]);
+            float h = maxf(head - maxf(maxf(zl, zh), kDh), 0.01f);
+            float cfl = d.afa * sh_len[j] / (sqrtf(d.g * h) + fabsf(qv) / h);
+            unsigned long long key = ((unsigned long long)__float_as_uint(cfl) << 32) | (unsigned)gid;
+            best = key < best ? key : best;
+        }
+    }
+    best = warp_min_u64(best);
+    const int lane = tid & 31, warp = tid >> 5;
+    if (lane == 0) sh_min[warp] = best;
+    if (my_wet) atomicAdd(&sh_cnt[2], my_wet);
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long bmin = kCflEmpty;
+        for (int w = 0; w < kThreads / 32; ++w) bmin = sh_min[w] < bmin ? sh_min[w] : bmin;
+        if (bmin != kCflEmpty) atomicMin(&c->cfl_packed, bmin);
+        if (sh_cnt[0]) {
+            atomicAdd(&c->limited_cells, sh_cnt[0]);
+            atomicMin(&c->min_scale_bits, sh_minbits);
+        }
+        if (sh_cnt[1]) atomicAdd(&c->limited_faces, sh_cnt[1]);
+        if (sh_cnt[2]) atomicAdd(&c->wet, sh_cnt[2]);
+        __threadfence();
+        unsigned ticket = atomicAdd(&c->done_blocks, 1u);
+        sh_last = ticket == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!sh_last || tid != 0) return;
+    // Last block: CFL result, trace row, clock commit, next step's preparation.
+    __threadfence();
+    unsigned long long packed = atomicExch(&c->cfl_packed, kCflEmpty);
+    c->done_blocks = 0;
+    if (packed == kCflEmpty) {
+        c->ndt = __uint_as_float(0x7f800000u);
+        c->cfl_arg = 0;
+    } else {
+        c->ndt = __uint_as_float((uint32_t)(packed >> 32));
+        c->cfl_arg = (int32_t)(packed & 0xffffffffu);
+    }
+    finish_step(c);
+    c->parity = parity ^ 1;
+    if (c->slot < d.batch_size) prepare_step(d, c, depth_out, q_out);
+}
+
+// Batch start: the rain-time second buffer equals the caller's buffer (cells
+// that do not rain during the batch are never rewritten).
+__global__ void k_batch_start(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.e_num; i += gridDim.x * blockDim.x)
+        d.rain_time_b[i] = m.rain_time[i];
+}
+
+// Batch end: bring the current state back into the caller's buffers.
+__global__ void k_batch_end(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    Ctl *c = d.ctl;
+    __shared__ int last;
+    if (c->parity) {
+        const int stride = gridDim.x * blockDim.x;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.e_num; i += stride) {
+            m.depth[i] = d.depth_b[i];
+            m.rain_time[i] = d.rain_time_b[i];
+        }
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.s_num; i += stride) m.q[i] = d.q_b[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned ticket = atomicAdd(&c->done_blocks, 1u);
+        last = ticket == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        c->done_blocks = 0;
+        c->parity = 0;
+    }
+}
+
+// u, v of the current state (the velocity function, solver_compact.py:355-362).
+__global__ void k_velocity(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    for (int ei = 1 + blockIdx.x * blockDim.x + threadIdx.x; ei < m.e_num; ei += gridDim.x * blockDim.x) {
+        float fl[4];
+        for (int dd = 0; dd < 4; ++dd) {
+            float total = 0.0f;
+            int p = m.face_ptr[4 * ei + dd], cnt = m.face_count[4 * ei + dd];
+            for (int j = 0; j < cnt; ++j) {
+                int si = m.isl_data[p + j];
+                total += m.q[si] * m.length[si];
+            }
+            fl[dd] = total;
+        }
+        float depth = m.depth[ei];
+        float h = maxf(depth, 0.01f);
+        float u = 0.0f, v = 0.0f;
+        if (depth >= d.min_h) {
+            u = (fl[0] + fl[1]) / m.height[ei] / h / 2.0f;
+            v = (fl[2] + fl[3]) / m.width[ei] / h / 2.0f;
+        }
+        m.u[ei] = u;
+        m.v[ei] = v;
+    }
+}
+
+// --------------------------------------------------------------- planner
+
+struct Pattern {
+    std::vector<int32_t> counts;  // 8
+    std::vector<int32_t> ext;
+    std::vector<int32_t> srel;
+    std::vector<uint32_t> lohi;
+    std::vector<uint32_t> fdesc;
+    std::vector<uint16_t> fidx;
+};
+
+uint64_t fnv(uint64_t h, const void *p, size_t n)
+{
+    const unsigned char *b = (const unsigned char *)p;
+    for (size_t i = 0; i < n; ++i) { h ^= b[i]; h *= 1099511628211ULL; }
+    return h;
+}
+
+uint64_t pattern_hash(const Pattern &p)
+{
+    uint64_t h = 1469598103934665603ULL;
+    h = fnv(h, p.counts.data(), p.counts.size() * 4);
+    h = fnv(h, p.ext.data(), p.ext.size() * 4);
+    h = fnv(h, p.srel.data(), p.srel.size() * 4);
+    h = fnv(h, p.lohi.data(), p.lohi.size() * 4);
+    h = fnv(h, p.fdesc.data(), p.fdesc.size() * 4);
+    h = fnv(h, p.fidx.data(), p.fidx.size() * 2);
+    return h;
+}
+
+bool same(const Pattern &a, const Pattern &b)
+{
+    return a.counts == b.counts && a.ext == b.ext && a.srel == b.srel && a.lohi == b.lohi && a.fdesc == b.fdesc &&
+           a.fidx == b.fidx;
+}
+
+struct HostMesh {
+    int e, s;
+    std::vector<int32_t> topo, fptr, fcnt, isl;
+};
+
+int copy_back(const nhf_mesh &m, cudaStream_t st, HostMesh &hm)
+{
+    hm.e = m.e_num; hm.s = m.s_num;
+    hm.topo.resize((size_t)m.s_num * 3);
+    hm.fptr.resize((size_t)m.e_num * 4);
+    hm.fcnt.resize((size_t)m.e_num * 4);
+    hm.isl.resize((size_t)(m.isl_len > 0 ? m.isl_len : 1));
+    if (cudaMemcpyAsync(hm.topo.data(), m.topology, hm.topo.size() * 4, cudaMemcpyDeviceToHost, st) ||
+        cudaMemcpyAsync(hm.fptr.data(), m.face_ptr, hm.fptr.size() * 4, cudaMemcpyDeviceToHost, st) ||
+        cudaMemcpyAsync(hm.fcnt.data(), m.face_count, hm.fcnt.size() * 4, cudaMemcpyDeviceToHost, st) ||
+        (m.isl_len > 0 && cudaMemcpyAsync(hm.isl.data(), m.isl_data, (size_t)m.isl_len * 4, cudaMemcpyDeviceToHost, st)) ||
+        cudaStreamSynchronize(st))
+        return 1;
+    return 0;
+}
+
+// Sides listed by each cell must be exactly the sides naming that cell as a
+// neighbour; every side must be listed by its owner (lower, else higher).
+bool consistent(const HostMesh &hm, std::string &why)
+{
+    std::vector<int> listed(hm.s, 0);
+    for (int c = 1; c < hm.e; ++c)
+        for (int dd = 0; dd < 4; ++dd) {
+            int p = hm.fptr[4 * c + dd], n = hm.fcnt[4 * c + dd];
+            if (n < 0 || n > 15) { why = "a face has more than 15 sides"; return false; }
+            for (int j = 0; j < n; ++j) {
+                int sid = hm.isl[p + j];
+                if (sid < 1 || sid >= hm.s) { why = "face lists an invalid side"; return false; }
+                int lo = hm.topo[3 * sid + 1], hi = hm.topo[3 * sid + 2];
+                if (lo != c && hi != c) { why = "face lists a side that does not touch the cell"; return false; }
+                listed[sid] += 1;
+            }
+        }
+    for (int sid = 1; sid < hm.s; ++sid) {
+        int lo = hm.topo[3 * sid + 1], hi = hm.topo[3 * sid + 2];
+        int expect = (lo != 0) + (hi != 0);
+        if (expect == 0 || listed[sid] != expect || lo == hi) { why = "a side is not listed by exactly its cells"; return false; }
+    }
+    return true;
+}
+
+int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::vector<int32_t> &tile_pattern,
+               std::vector<int32_t> &tile_cbase, std::vector<int32_t> &tile_sbase, int &max_ext, int &max_sides,
+               std::string &why)
+{
+    const int e = hm.e, s = hm.s;
+    // cell adjacency through interior sides
+    std::vector<int> deg(e + 1, 0);
+    for (int sid = 1; sid < s; ++sid) {
+        int lo = hm.topo[3 * sid + 1], hi = hm.topo[3 * sid + 2];
+        if (lo && hi) { deg[lo]++; deg[hi]++; }
+    }
+    std::vector<int> aptr(e + 1, 0);
+    for (int c = 0; c < e; ++c) aptr[c + 1] = aptr[c] + deg[c];
+    std::vector<int> adj(aptr[e]);
+    std::vector<int> fill(aptr.begin(), aptr.end() - 1);
+    for (int sid = 1; sid < s; ++sid) {
+        int lo = hm.topo[3 * sid + 1], hi = hm.topo[3 * sid + 2];
+        if (lo && hi) { adj[fill[lo]++] = hi; adj[fill[hi]++] = lo; }
+    }
+    const int n_tiles = (e + T - 1) / T;
+    std::vector<int> stamp(e, -1), ring(e, 0), slot(e, 0);
+    std::vector<int> sstamp(s, -1), sloc(s, 0);
+    std::vector<uint8_t> sflag(s, 0);
+    std::unordered_map<uint64_t, std::vector<int>> index;
+    patterns.clear();
+    tile_pattern.assign(n_tiles, 0);
+    tile_cbase.assign(n_tiles, 0);
+    tile_sbase.assign(n_tiles, 0);
+    max_ext = max_sides = 0;
+    std::vector<int> ext, sides;
+    for (int t = 0; t < n_tiles; ++t) {
+        const int cbase = t * T;
+        const int r0_first = std::max(cbase, 1), r0_end = std::min(cbase + T, e);
+        ext.clear();
+        ext.push_back(0);
+        stamp[0] = t; ring[0] = -1; slot[0] = 0;
+        for (int g = r0_first; g < r0_end; ++g) { stamp[g] = t; ring[g] = 0; slot[g] = (int)ext.size(); ext.push_back(g); }
+        int ring_begin[5];
+        ring_begin[0] = 1;
+        for (int r = 1; r <= 3; ++r) {
+            ring_begin[r] = (int)ext.size();
+            for (int i = ring_begin[r - 1]; i < ring_begin[r]; ++i) {
+                int cc = ext[i];
+                for (int k = aptr[cc]; k < aptr[cc + 1]; ++k) {
+                    int nb = adj[k];
+                    if (stamp[nb] != t) { stamp[nb] = t; ring[nb] = r; ext.push_back(nb); }
+                }
+            }
+            std::sort(ext.begin() + ring_begin[r], ext.end());
+            for (int i = ring_begin[r]; i < (int)ext.size(); ++i) slot[ext[i]] = i;
+        }
+        ring_begin[4] = (int)ext.size();
+        const int n_r0 = ring_begin[1] - 1, n_r01 = ring_begin[2] - 1, n_r012 = ring_begin[3] - 1;
+        // local sides: faces of rings 0..2
+        sides.clear();
+        for (int i = 1; i <= n_r012; ++i) {
+            int cc = ext[i];
+            for (int dd = 0; dd < 4; ++dd) {
+                int p = hm.fptr[4 * cc + dd], n = hm.fcnt[4 * cc + dd];
+                for (int j = 0; j < n; ++j) {
+                    int sid = hm.isl[p + j];
+                    if (sstamp[sid] != t) { sstamp[sid] = t; sflag[sid] = 0; sides.push_back(sid); }
+                    if (ring[cc] <= 1) sflag[sid] |= kFinal;
+                }
+            }
+        }
+        for (int sid : sides) {
+            int lo = hm.topo[3 * sid + 1], hi = hm.topo[3 * sid + 2];
+            if ((lo && stamp[lo] != t) || (hi && stamp[hi] != t)) { why = "side endpoint outside the staged rings"; return 1; }
+            int owner = lo ? lo : hi;
+            if (owner && ring[owner] == 0 && stamp[owner] == t) sflag[sid] |= kOwned;
+        }
+        auto rank = [&](int sid) { return (sflag[sid] & kOwned) ? 0 : ((sflag[sid] & kFinal) ? 1 : 2); };
+        std::sort(sides.begin(), sides.end(), [&](int x, int y) {
+            int rx = rank(x), ry = rank(y);
+            return rx != ry ? rx < ry : x < y;
+        });
+        int n_owned = 0, n_qf = 0;
+        for (int i = 0; i < (int)sides.size(); ++i) {
+            sloc[sides[i]] = i;
+            n_owned += (sflag[sides[i]] & kOwned) ? 1 : 0;
+            n_qf += (sflag[sides[i]] & (kOwned | kFinal)) ? 1 : 0;
+        }
+        if ((int)ext.size() > 65535 || (int)sides.size() > 65535) { why = "tile halo too large"; return 1; }
+        int sbase = sides.empty() ? 0 : *std::min_element(sides.begin(), sides.end());
+        Pattern p;
+        p.counts = {(int)ext.size(), n_r0, n_r01, n_r012, (int)sides.size(), n_owned, n_qf, r0_first - cbase};
+        p.ext.resize(ext.size());
+        p.ext[0] = 0;
+        for (size_t i = 1; i < ext.size(); ++i) p.ext[i] = ext[i] - cbase;
+        p.srel.resize(sides.size());
+        p.lohi.resize(sides.size());
+        for (size_t i = 0; i < sides.size(); ++i) {
+            int sid = sides[i];
+            p.srel[i] = sid - sbase;
+            int lo = hm.topo[3 * sid + 1], hi = hm.topo[3 * sid + 2];
+            p.lohi[i] = (uint32_t)slot[lo] | ((uint32_t)slot[hi] << 16);
+        }
+        p.fdesc.assign(n_r012 + 1, 0u);
+        for (int i = 1; i <= n_r012; ++i) {
+            int cc = ext[i];
+            if (p.fidx.size() > 65535) { why = "tile face table too large"; return 1; }
+            uint32_t counts = 0;
+            uint32_t start = (uint32_t)p.fidx.size();
+            for (int dd = 0; dd < 4; ++dd) {
+                int pp = hm.fptr[4 * cc + dd], n = hm.fcnt[4 * cc + dd];
+                counts |= (uint32_t)n << (4 * dd);
+                for (int j = 0; j < n; ++j) p.fidx.push_back((uint16_t)sloc[hm.isl[pp + j]]);
+            }
+            p.fdesc[i] = start | (counts << 16);
+        }
+        if (p.fidx.size() > 65535) { why = "tile face table too large"; return 1; }
+        max_ext = std::max(max_ext, (int)ext.size());
+        max_sides = std::max(max_sides, (int)sides.size());
+        uint64_t hsh = pattern_hash(p);
+        int found = -1;
+        auto it = index.find(hsh);
+        if (it != index.end())
+            for (int cand : it->second)
+                if (same(patterns[cand], p)) { found = cand; break; }
+        if (found < 0) {
+            found = (int)patterns.size();
+            patterns.push_back(std::move(p));
+            index[hsh].push_back(found);
+        }
+        tile_pattern[t] = found;
+        tile_cbase[t] = cbase;
+        tile_sbase[t] = sbase;
+    }
+    return 0;
+}
+
+template <typename K>
+void set_smem(K kernel, size_t bytes)
+{
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int CPT>
+void set_smem_all(size_t bytes)
+{
+    set_smem(k_step_tiled<true, false, CPT>, bytes);
+    set_smem(k_step_tiled<false, false, CPT>, bytes);
+    set_smem(k_step_tiled<true, true, CPT>, bytes);
+    set_smem(k_step_tiled<false, true, CPT>, bytes);
+}
+
+template <int CPT>
+void launch_step(const Dev &d, size_t smem, cudaStream_t s)
+{
+    const int grid = d.plan.n_tiles;
+    const bool hanging = d.m.hang_cells > 0;
+    if (d.theta_one) {
+        if (hanging) k_step_tiled<true, true, CPT><<<grid, kThreads, smem, s>>>(d);
+        else k_step_tiled<true, false, CPT><<<grid, kThreads, smem, s>>>(d);
+    } else {
+        if (hanging) k_step_tiled<false, true, CPT><<<grid, kThreads, smem, s>>>(d);
+        else k_step_tiled<false, false, CPT><<<grid, kThreads, smem, s>>>(d);
+    }
+}
+
+}  // namespace
+
+// Tangential gradients for the tiled form (reads the current-parity depth).
+namespace {
+__global__ void k_pressure_tiled(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    if (!d.ctl->active) return;
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= m.hang_cells) return;
+    const float *depth = cur_depth(d, d.ctl->parity);
+    int cell = m.hcells[slot];
+    for (int axis = 0; axis < 2; ++axis) {
+        if (m.axes[2 * slot + axis] != 1) continue;
+        float value = 0.0f;
+        if (depth[cell] > d.min_h) {
+            float dv[2], xv[2];
+            int ok[2];
+            for (int side_of = 0; side_of < 2; ++side_of) {
+                int direction = axis == 1 ? 2 + side_of : side_of;
+                float val = 0.0f, distance = 0.0f, total = 0.0f;
+                int usable = 1;
+                float eta = m.bed[cell] + depth[cell];
+                int start = m.face_ptr[4 * cell + direction], count = m.face_count[4 * cell + direction];
+                for (int j = 0; j < count; ++j) {
+                    int side = m.isl_data[start + j];
+                    int other = m.topology[3 * side + 1] + m.topology[3 * side + 2] - cell;
+                    if (other == 0 || depth[other] <= d.min_h) {
+                        usable = 0;
+                    } else {
+                        float weight = m.length[side];
+                        val += weight * ((m.bed[other] + depth[other]) - eta);
+                        float delta = axis == 1 ? m.y[other] - m.y[cell] : m.x[other] - m.x[cell];
+                        distance += weight * delta;
+                        total += weight;
+                    }
+                }
+                if (total > 0.0f) { val /= total; distance /= total; }
+                else usable = 0;
+                dv[side_of] = val; xv[side_of] = distance; ok[side_of] = usable;
+            }
+            if (ok[0] && ok[1]) value = (dv[1] - dv[0]) / (xv[1] - xv[0]);
+            else if (ok[0]) value = dv[0] / xv[0];
+            else if (ok[1]) value = dv[1] / xv[1];
+        }
+        d.gradients[2 * slot + axis] = value;
+    }
+}
+
+// length-weighted face discharge for theta < 1 (solver_compact.py:118-132)
+__global__ void k_face_qn_tiled(Dev d)
+{
+    const nhf_mesh &m = d.m;
+    if (!d.ctl->active) return;
+    int ei = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ei >= m.e_num) return;
+    const float *q = cur_q(d, d.ctl->parity);
+    for (int dd = 0; dd < 4; ++dd) {
+        int start = m.face_ptr[4 * ei + dd], count = m.face_count[4 * ei + dd];
+        float result = 0.0f;
+        if (count == 1) {
+            result = q[m.isl_data[start]];
+        } else if (count > 1) {
+            float total = 0.0f, width = 0.0f;
+            for (int o = 0; o < count; ++o) {
+                int side = m.isl_data[start + o];
+                total += q[side] * m.length[side];
+                width += m.length[side];
+            }
+            result = total / width;
+        }
+        d.face_qn[4 * ei + dd] = result;
+    }
+}
+}  // namespace
+
+int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, size_t why_len)
+{
+    std::string reason;
+    auto bad = [&](const std::string &r) {
+        snprintf(why, why_len, "%s", r.c_str());
+        return 1;
+    };
+    if (m.e_num < 2) return bad("mesh has no cells");
+    HostMesh hm;
+    if (copy_back(m, s, hm)) return bad("copying the mesh tables to the host failed");
+    if (!consistent(hm, reason)) return bad(reason);
+    std::vector<Pattern> patterns;
+    std::vector<int32_t> tp, tc, ts;
+    int max_ext = 0, max_sides = 0, tile = 0;
+    size_t smem = 0;
+    for (int T : {1024, 512, 256}) {
+        if (plan_tiles(hm, T, patterns, tp, tc, ts, max_ext, max_sides, reason)) return bad(reason);
+        smem = (size_t)max_ext * 16 + (size_t)max_sides * 8;
+        if (smem <= (size_t)kMaxSharedBytes) { tile = T; break; }
+    }
+    if (!tile) return bad("tile halos exceed shared memory (cell numbering is not spatially coherent)");
+    // flatten patterns
+    std::vector<int32_t> counts, offsets, ext, srel;
+    std::vector<uint32_t> lohi, fdesc;
+    std::vector<uint16_t> fidx;
+    for (const Pattern &p : patterns) {
+        counts.insert(counts.end(), p.counts.begin(), p.counts.end());
+        offsets.push_back((int32_t)ext.size());
+        offsets.push_back((int32_t)srel.size());
+        offsets.push_back((int32_t)fdesc.size());
+        offsets.push_back((int32_t)fidx.size());
+        ext.insert(ext.end(), p.ext.begin(), p.ext.end());
+        srel.insert(srel.end(), p.srel.begin(), p.srel.end());
+        lohi.insert(lohi.end(), p.lohi.begin(), p.lohi.end());
+        fdesc.insert(fdesc.end(), p.fdesc.begin(), p.fdesc.end());
+        fidx.insert(fidx.end(), p.fidx.begin(), p.fidx.end());
+    }
+    if (fidx.empty()) fidx.push_back(0);
+    if (srel.empty()) { srel.push_back(0); lohi.push_back(0); }
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
+    size_t o_tp = take(tp.size() * 4), o_tc = take(tc.size() * 4), o_ts = take(ts.size() * 4);
+    size_t o_cnt = take(counts.size() * 4), o_off = take(offsets.size() * 4), o_ext = take(ext.size() * 4);
+    size_t o_srel = take(srel.size() * 4), o_lohi = take(lohi.size() * 4), o_fd = take(fdesc.size() * 4);
+    size_t o_fi = take(fidx.size() * 2);
+    void *mem = nullptr;
+    if (cudaMalloc(&mem, off) != cudaSuccess) return bad("allocating the tile plan failed");
+    char *b = (char *)mem;
+    auto up = [&](size_t o, const void *src, size_t n) {
+        return cudaMemcpyAsync(b + o, src, n, cudaMemcpyHostToDevice, s) == cudaSuccess;
+    };
+    bool ok = up(o_tp, tp.data(), tp.size() * 4) && up(o_tc, tc.data(), tc.size() * 4) &&
+              up(o_ts, ts.data(), ts.size() * 4) && up(o_cnt, counts.data(), counts.size() * 4) &&
+              up(o_off, offsets.data(), offsets.size() * 4) && up(o_ext, ext.data(), ext.size() * 4) &&
+              up(o_srel, srel.data(), srel.size() * 4) && up(o_lohi, lohi.data(), lohi.size() * 4) &&
+              up(o_fd, fdesc.data(), fdesc.size() * 4) && up(o_fi, fidx.data(), fidx.size() * 2) &&
+              cudaStreamSynchronize(s) == cudaSuccess;
+    if (!ok) { cudaFree(mem); return bad("uploading the tile plan failed"); }
+    TilePlan &P = out->plan;
+    P.n_tiles = (int32_t)tp.size();
+    P.tile = tile;
+    P.max_ext = max_ext;
+    P.max_sides = max_sides;
+    P.cells_per_thread = tile / kThreads;
+    P.tile_pattern = (const int32_t *)(b + o_tp);
+    P.tile_cbase = (const int32_t *)(b + o_tc);
+    P.tile_sbase = (const int32_t *)(b + o_ts);
+    P.p_counts = (const int32_t *)(b + o_cnt);
+    P.p_offsets = (const int32_t *)(b + o_off);
+    P.ext_rel = (const int32_t *)(b + o_ext);
+    P.side_rel = (const int32_t *)(b + o_srel);
+    P.side_lohi = (const uint32_t *)(b + o_lohi);
+    P.face_desc = (const uint32_t *)(b + o_fd);
+    P.face_idx = (const uint16_t *)(b + o_fi);
+    out->device_memory = mem;
+    out->shared_bytes = smem;
+    out->patterns = (int)patterns.size();
+    if (P.cells_per_thread == 4) set_smem_all<4>(smem);
+    else if (P.cells_per_thread == 2) set_smem_all<2>(smem);
+    else set_smem_all<1>(smem);
+    return 0;
+}
+
+void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s)
+{
+    const nhf_mesh &m = d.m;
+    if (m.hang_cells > 0) k_pressure_tiled<<<(m.hang_cells + 255) / 256, 256, 0, s>>>(d);
+    if (!d.theta_one) k_face_qn_tiled<<<(m.e_num + 255) / 256, 256, 0, s>>>(d);
+    switch (d.plan.cells_per_thread) {
+    case 4: launch_step<4>(d, b.shared_bytes, s); break;
+    case 2: launch_step<2>(d, b.shared_bytes, s); break;
+    default: launch_step<1>(d, b.shared_bytes, s); break;
+    }
+}
+
+void tiled_enqueue_batch_start(const Dev &d, cudaStream_t s)
+{
+    int grid = (d.m.e_num + 255) / 256;
+    if (grid > 148 * 16) grid = 148 * 16;
+    k_batch_start<<<grid, 256, 0, s>>>(d);
+}
+
+void tiled_enqueue_batch_end(const Dev &d, cudaStream_t s)
+{
+    int n = d.m.e_num > d.m.s_num ? d.m.e_num : d.m.s_num;
+    int grid = (n + 255) / 256;
+    if (grid > 148 * 16) grid = 148 * 16;
+    k_batch_end<<<grid, 256, 0, s>>>(d);
+    k_velocity<<<grid, 256, 0, s>>>(d);
+}
+
+}  // namespace nhf

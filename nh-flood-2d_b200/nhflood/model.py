@@ -28,6 +28,7 @@ class StepParams:
     batch_size: int = 32
     g: float = float(G)
     min_dt: float = float(np.float32(MIN_DT))
+    path: str = 'auto'  # 'auto': fused tiled step when the mesh allows it; 'multipass'
 
 
 @dataclass

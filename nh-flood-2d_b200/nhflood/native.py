@@ -30,7 +30,7 @@ class NhfMesh(ctypes.Structure):
 
 class NhfParams(ctypes.Structure):
     _fields_ = [('g', c_float), ('afa', c_float), ('sita', c_float), ('min_h', c_float),
-                ('min_dt', c_float), ('batch_size', c_int32)]
+                ('min_dt', c_float), ('batch_size', c_int32), ('path', c_int32)]
 
 
 _LIB = None
@@ -75,6 +75,7 @@ def library(path=None):
         'nhf_read_gradients': (c_int32, [H, c_void_p]),
         'nhf_synchronize': (c_int32, [H]),
         'nhf_stream': (c_void_p, [H]),
+        'nhf_path': (ctypes.c_char_p, [H]),
         'nhf_cfl_noalloc': (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_float, c_float,
                                       c_void_p, c_void_p, c_void_p]),
         'nhf_cfl_noalloc_error': (ctypes.c_char_p, []),
@@ -94,7 +95,7 @@ def exported_symbols() -> list[str]:
             'nhf_compute_cfl', 'nhf_initial_diagnostics', 'nhf_reset_extrema', 'nhf_run_batch',
             'nhf_run_batch_async', 'nhf_read_trace', 'nhf_budget_flush', 'nhf_budget_terms', 'nhf_get_cfl',
             'nhf_limits', 'nhf_reset_limits', 'nhf_sample_stations', 'nhf_read_eq', 'nhf_read_gradients',
-            'nhf_synchronize', 'nhf_stream', 'nhf_cfl_noalloc', 'nhf_cfl_noalloc_error']
+            'nhf_synchronize', 'nhf_stream', 'nhf_path', 'nhf_cfl_noalloc', 'nhf_cfl_noalloc_error']
 
 
 def _u32(a):
@@ -154,7 +155,8 @@ class CudaEngine(Engine):
             tensor = self.t.get(name)
             setattr(mesh, name, tensor.data_ptr() if tensor is not None else None)
         self._mesh = mesh
-        p = NhfParams(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size)
+        p = NhfParams(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size,
+                      1 if params.path == 'multipass' else 0)
         handle = c_void_p()
         with torch.cuda.device(dev):
             stream = torch.cuda.current_stream(dev).cuda_stream
@@ -163,6 +165,7 @@ class CudaEngine(Engine):
             raise RuntimeError(f'nhf_create failed ({rc}): {self.lib.nhf_last_error(None).decode()}')
         self.h = handle
         self.terms = self.lib.nhf_budget_terms(self.h)
+        self.path = self.lib.nhf_path(self.h).decode()
         self._trace = np.zeros((self.batch_size, NHF_TRACE_COLS), dtype=np.uint32)
 
     # -- helpers ----------------------------------------------------------

@@ -131,48 +131,66 @@ def _iso(seconds: float) -> str:
 
 # ------------------------------------------------------------ mesh builders
 
-def uniform_grid(nx: int, ny: int, dx: float, bed: np.ndarray, land: np.ndarray) -> MeshData:
-    """Row-major nx x ny grid of square cells; vertical sides first (row by
-    row, west to east), then horizontal sides (south to north)."""
+def uniform_grid(nx: int, ny: int, dx: float, bed: np.ndarray, land: np.ndarray, tile: int = 32) -> MeshData:
+    """nx x ny grid of square cells numbered tile by tile (tile x tile blocks in
+    row-major block order, row-major inside a block), so that consecutive cell
+    indices form compact tiles. Each cell owns its east and north sides (and
+    its exterior west/south sides on the domain edge); sides are numbered in
+    owner order, so tiles away from the edges have identical relative
+    numbering."""
     n = nx * ny
     e = n + 1
-    j, i = np.divmod(np.arange(n, dtype=np.int64), nx)
-    cell = np.arange(1, e, dtype=np.int64)
-    nv = ny * (nx + 1)
-    vid = 1 + j * (nx + 1) + i          # west side of each cell
-    hid = 1 + nv + j * nx + i           # south side of each cell
+    jj, ii = np.divmod(np.arange(n, dtype=np.int64), nx)          # row-major grid positions
+    ntx = (nx + tile - 1) // tile
+    key = ((jj // tile) * ntx + ii // tile) * (tile * tile) + (jj % tile) * tile + (ii % tile)
+    order = np.argsort(key, kind='stable')                         # grid position of each cell id - 1
+    cid = np.empty(n, np.int64)
+    cid[order] = np.arange(1, e)                                   # cell id of each grid position
+    grid_id = cid.reshape(ny, nx)
+    i, j = ii[order], jj[order]                                    # grid position by cell id - 1
     x = np.zeros(e, np.float32)
     y = np.zeros(e, np.float32)
     x[1:] = (i + 0.5) * dx
     y[1:] = (j + 0.5) * dx
     z = np.zeros(e, np.float32)
-    z[1:] = bed.reshape(-1)
+    z[1:] = np.asarray(bed, np.float32).reshape(-1)[order]
     land_type = np.zeros(e, np.uint8)
-    land_type[1:] = land.reshape(-1)
-    counts = np.zeros((e, 4), np.int32)
-    counts[1:] = 1
-    face_ptr = np.zeros((e, 4), np.int32)
-    face_ptr[1:] = 4 * (cell[:, None] - 1) + np.arange(4)
-    isl = np.stack([vid, vid + 1, hid, hid + nx], axis=1).reshape(-1).astype(np.int32)
-    s = 1 + nv + (ny + 1) * nx
+    land_type[1:] = np.asarray(land).reshape(-1)[order]
+    # owned sides per cell: slot 0 east, 1 north, 2 west (edge), 3 south (edge)
+    owner = np.arange(1, e, dtype=np.int64)
+    has = np.stack([np.ones(n, bool), np.ones(n, bool), i == 0, j == 0], axis=1)
+    count = has.sum(axis=1)
+    first = np.zeros(n + 1, np.int64)
+    first[1:] = np.cumsum(count)
+    slot_rank = np.cumsum(has, axis=1) - 1                         # rank among the cell's owned sides
+    sid = np.where(has, 1 + first[:-1, None] + slot_rank, 0)       # side id per (cell, slot)
+    s = 1 + int(first[-1])
     topo = np.zeros((s, 3), np.int32)
     sx = np.zeros(s, np.float32)
     sy = np.zeros(s, np.float32)
-    # vertical sides
-    vj, vi = np.divmod(np.arange(nv, dtype=np.int64), nx + 1)
-    topo[1:1 + nv, 0] = 2
-    topo[1:1 + nv, 1] = np.where(vi > 0, vj * nx + vi, 0)          # cell (vi-1, vj) = vj*nx + vi
-    topo[1:1 + nv, 2] = np.where(vi < nx, vj * nx + vi + 1, 0)
-    sx[1:1 + nv] = vi * dx
-    sy[1:1 + nv] = (vj + 0.5) * dx
-    # horizontal sides
-    nh = (ny + 1) * nx
-    hj, hi = np.divmod(np.arange(nh, dtype=np.int64), nx)
-    topo[1 + nv:, 0] = 1
-    topo[1 + nv:, 1] = np.where(hj > 0, (hj - 1) * nx + hi + 1, 0)
-    topo[1 + nv:, 2] = np.where(hj < ny, hj * nx + hi + 1, 0)
-    sx[1 + nv:] = (hi + 0.5) * dx
-    sy[1 + nv:] = hj * dx
+    east_nb = np.where(i < nx - 1, grid_id[j, np.minimum(i + 1, nx - 1)], 0)
+    north_nb = np.where(j < ny - 1, grid_id[np.minimum(j + 1, ny - 1), i], 0)
+    e_ids, n_ids = sid[:, 0], sid[:, 1]
+    topo[e_ids] = np.stack([np.full(n, 2), owner, east_nb], axis=1)
+    sx[e_ids], sy[e_ids] = (i + 1) * dx, (j + 0.5) * dx
+    topo[n_ids] = np.stack([np.full(n, 1), owner, north_nb], axis=1)
+    sx[n_ids], sy[n_ids] = (i + 0.5) * dx, (j + 1) * dx
+    w = has[:, 2]
+    topo[sid[w, 2]] = np.stack([np.full(w.sum(), 2), np.zeros(w.sum(), np.int64), owner[w]], axis=1)
+    sx[sid[w, 2]], sy[sid[w, 2]] = 0.0, (j[w] + 0.5) * dx
+    so = has[:, 3]
+    topo[sid[so, 3]] = np.stack([np.full(so.sum(), 1), np.zeros(so.sum(), np.int64), owner[so]], axis=1)
+    sx[sid[so, 3]], sy[sid[so, 3]] = (i[so] + 0.5) * dx, 0.0
+    # faces: west side = east side of the west neighbour (or own edge side), etc.
+    west_cell = np.where(i > 0, grid_id[j, np.maximum(i - 1, 0)], 0)
+    south_cell = np.where(j > 0, grid_id[np.maximum(j - 1, 0), i], 0)
+    west_side = np.where(i > 0, sid[np.maximum(west_cell - 1, 0), 0], sid[:, 2])
+    south_side = np.where(j > 0, sid[np.maximum(south_cell - 1, 0), 1], sid[:, 3])
+    counts = np.zeros((e, 4), np.int32)
+    counts[1:] = 1
+    face_ptr = np.zeros((e, 4), np.int32)
+    face_ptr[1:] = 4 * (owner[:, None] - 1) + np.arange(4)
+    isl = np.stack([west_side, e_ids, south_side, n_ids], axis=1).reshape(-1).astype(np.int32)
     length = np.full(s, dx, np.float32)
     length[0] = 0
     return MeshData(x=x, y=y, z=z, land_type=land_type, counts=counts, face_ptr=face_ptr, isl_data=isl,

@@ -46,37 +46,53 @@ CASES = {
 }
 
 
+def cuda_engine(path):
+    def factory(arrays, params):
+        from nhflood.native import CudaEngine
+        params.path = path
+        engine = CudaEngine(arrays, params)
+        assert engine.path.startswith('tiled' if path == 'auto' else 'multipass'), engine.path
+        return engine
+    return factory
+
+
+PATHS = ['auto', 'multipass']
+
+
+@pytest.mark.parametrize('path', PATHS)
 @pytest.mark.parametrize('name', sorted(CASES))
-def test_two_cell_cases_bit_exact(tmp_path, cuda_available, name):
+def test_two_cell_cases_bit_exact(tmp_path, cuda_available, name, path):
     kw = dict(CASES[name])
     bands, duration = kw.pop('bands'), kw.pop('duration')
     dc, fc = two_cell_case(tmp_path / 'oracle', bands, duration, **kw)
     a = run(dc, fc, 'oracle')
     dc, fc = two_cell_case(tmp_path / 'cuda', bands, duration, **kw)
-    b = run(dc, fc, 'cuda')
+    b = run(dc, fc, cuda_engine(path))
     assert b.manifest['backend'] == 'cuda'
     assert_runs_identical(a, b)
 
 
+@pytest.mark.parametrize('path', PATHS)
 @pytest.mark.parametrize('sita', [1.0, 0.7])
-def test_grid_with_limiter_and_theta_bit_exact(tmp_path, cuda_available, sita):
+def test_grid_with_limiter_and_theta_bit_exact(tmp_path, cuda_available, sita, path):
     results = []
-    for engine in ('oracle', 'cuda'):
-        path = tmp_path / engine
-        path.mkdir()
-        grid3_mesh(path)
+    for engine in ('oracle', cuda_engine(path)):
+        name = 'oracle' if engine == 'oracle' else 'cuda'
+        path_dir = tmp_path / name
+        path_dir.mkdir()
+        grid3_mesh(path_dir)
         from scenarios import write_rain
         from nhflood.raster import from_origin
         from nhflood.input import ForceConfig
-        rain = write_rain(path, [[[0]]], from_origin(0, 30, 30, 30), [(0, 20)])
+        rain = write_rain(path_dir, [[[0]]], from_origin(0, 30, 30, 30), [(0, 20)])
         q = np.zeros(25, np.float32)
         for side, value in {grid_vertical(1, 1): -1, grid_vertical(1, 2): 1,
                             grid_horizontal(1, 1): -1, grid_horizontal(2, 1): 1}.items():
             q[side] = value
         depth = np.zeros(10, np.float32)
         depth[grid_cell(1, 1)] = .1
-        seed = seed_checkpoint(path / 'seed.fdb', path / 'ne.txt', path / 'ns.txt', depth=depth, q=q)
-        dc = domain(path, duration=20, yield_step=5, restart=seed, sita=sita,
+        seed = seed_checkpoint(path_dir / 'seed.fdb', path_dir / 'ne.txt', path_dir / 'ns.txt', depth=depth, q=q)
+        dc = domain(path_dir, duration=20, yield_step=5, restart=seed, sita=sita,
                     land={10: dict(manning_n=1e-3, infiltration='none')})
         fc = ForceConfig(boundaries=[], rainfall=rain)
         results.append(run(dc, fc, engine))
@@ -84,15 +100,16 @@ def test_grid_with_limiter_and_theta_bit_exact(tmp_path, cuda_available, sita):
     assert results[1].manifest['limiter_activity']['limited_cell_steps'] > 0
 
 
-def test_plain_uniform_256_full_run_bit_exact(tmp_path, cuda_available):
+@pytest.mark.parametrize('path', PATHS)
+def test_plain_uniform_256_full_run_bit_exact(tmp_path, cuda_available, path):
     """The 65,536-cell plain configuration for its whole 3600 s: identical
     dt sequences and per-step wet counts; every 300 s frame identical."""
     from nhflood.output import list_depth_frames, read_depth_frame
     from nhflood.workloads import plain_uniform_256, simulate
-    from runner import cuda_factory, oracle_factory
+    from runner import oracle_factory
     w = plain_uniform_256()
     row_a, rec_a = simulate(w, tmp_path / 'oracle', engine_factory=oracle_factory)
-    row_b, rec_b = simulate(w, tmp_path / 'cuda', engine_factory=cuda_factory)
+    row_b, rec_b = simulate(w, tmp_path / 'cuda', engine_factory=cuda_engine(path))
     assert rec_b.data['backend'] == 'cuda'
     np.testing.assert_array_equal(rec_a.trace, rec_b.trace)
     assert rec_a.trace[:, 9].max() > 1000  # the run does flood
