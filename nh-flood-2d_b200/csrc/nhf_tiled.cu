@@ -35,7 +35,6 @@
 namespace nhf {
 namespace {
 
-constexpr int kThreads = 256;
 constexpr int kMaxSharedBytes = 110 * 1024;
 constexpr uint8_t kOwned = 1, kFinal = 2;
 
@@ -76,20 +75,58 @@ __device__ __forceinline__ void face_sums(const Tile &tl, const float *sh_q, con
     }
 }
 
-template <bool kThetaOne, bool kHanging, int CPT>
-__global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
+// The canonical 256-slot pairwise tree (stride 128 .. 1) run on every
+// 256-thread half of the block at once; the sums land in threads 0, 256, ...
+template <int NT>
+__device__ __forceinline__ double tree_halves(double v, double *sh)
+{
+    const int tid = threadIdx.x;
+    const int lane256 = tid & 255;
+    sh[tid] = v;
+    __syncthreads();
+    for (int stride = 128; stride >= 32; stride >>= 1) {
+        if (lane256 < stride) sh[tid] += sh[tid + stride];
+        __syncthreads();
+    }
+    double r = 0.0;
+    if (lane256 < 32) {
+        r = sh[tid];
+        for (int stride = 16; stride >= 1; stride >>= 1) r += __shfl_down_sync(0xffffffffu, r, stride);
+    }
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ float term_value(int t, int B, float removed, float floor_v, const float *level,
+                                            float discharge, int bi, int kind)
+{
+    if (t == 0) return removed;
+    if (t == 1) return kind == 0 ? 0.0f : floor_v;
+    if (t == 2) return kind == 0 ? floor_v : 0.0f;
+    if (t == 3) return 0.0f;  // pipe exchange: no coupling
+    if (t < 4 + 5 * B) {
+        int b = (t - 4) / 5;
+        return (b == bi && kind == 0) ? level[(t - 4) % 5] : 0.0f;
+    }
+    return (t - 4 - 5 * B == bi) ? discharge : 0.0f;
+}
+
+template <bool kThetaOne, bool kHanging, int NT, int CPT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double sh_tree[kThreads];
-    __shared__ unsigned long long sh_min[kThreads / 32];
+    __shared__ double sh_tree[NT];
+    __shared__ unsigned long long sh_min[NT / 32];
     __shared__ uint32_t sh_cnt[3];
     __shared__ uint32_t sh_minbits;
+    __shared__ uint32_t sh_mask[CPT][NT / 256];
     __shared__ int sh_last;
     Ctl *c = d.ctl;
     const nhf_mesh &m = d.m;
     const int tid = threadIdx.x;
 
     if (tid == 0) { sh_cnt[0] = sh_cnt[1] = sh_cnt[2] = 0u; sh_minbits = __float_as_uint(1.0f); }
+    if (tid < CPT * (NT / 256)) (&sh_mask[0][0])[tid] = 0u;
     const int active = c->active;
     if (!active) {
         // No physics this slot: the last block advances the slot and prepares the next.
@@ -132,32 +169,45 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
         tl.fdesc = P.face_desc + off[2];
         tl.fidx = P.face_idx + off[3];
     }
+    const int E = P.max_ext;
     float *sh_h = reinterpret_cast<float *>(smem_raw);
-    float *sh_z = sh_h + P.max_ext;
-    float *sh_s = sh_z + P.max_ext;  // donor factor, then the new depth
-    int *sh_g = reinterpret_cast<int *>(sh_s + P.max_ext);
-    float *sh_q = reinterpret_cast<float *>(sh_g + P.max_ext);  // q*, then final q
+    float *sh_z = sh_h + E;
+    float *sh_s = sh_z + E;      // donor factor, then the new depth
+    float *sh_rq = sh_s + E;     // rain rate of the cell (0 when not raining)
+    float *sh_area = sh_rq + E;
+    int *sh_g = reinterpret_cast<int *>(sh_area + E);
+    int *sh_bi = sh_g + E;       // boundary id, -1 for none
+    float *sh_q = reinterpret_cast<float *>(sh_bi + E);  // q*, then final q
     float *sh_len = sh_q + P.max_sides;
 
-    // P0: stage water depth and bed of the tile and its three rings.
-    for (int i = tid; i < tl.n_ext; i += kThreads) {
+    // P0: stage the tile and its rings; cells of rings 0..2 also bring the
+    // per-cell inputs of the donor factor and the depth update.
+    for (int i = tid; i < tl.n_ext; i += NT) {
         int g = i ? tl.cbase + tl.ext[i] : 0;
         sh_g[i] = g;
         sh_h[i] = i ? depth_in[g] : m.depth[0];
         sh_z[i] = m.bed[g];
         sh_s[i] = 0.0f;  // donor_scale of the exterior sentinel stays 0
+        if (i >= 1 && i <= tl.n_r012) {
+            sh_area[i] = m.area[g];
+            sh_bi[i] = m.boundary_id[g];
+            sh_rq[i] = raining ? d.rain_rates[m.rain_index[g]] : 0.0f;
+        }
     }
     __syncthreads();
 
     // P1: momentum (solver_compact.py:439-486) for every local side.
-    for (int j = tid; j < tl.n_sides; j += kThreads) {
+    for (int j = tid; j < tl.n_sides; j += NT) {
         const int gid = tl.sbase + tl.srel[j];
         const uint32_t lh = tl.lohi[j];
         const int a = (int)(lh & 0xffffu), b = (int)(lh >> 16);
+        float xq = q_in[gid];
+        float dx = d.sdc[gid];
+        float n = m.side_n[gid];
+        float len = m.length[gid];
+        float bf = m.sbf[gid] == 1 ? 0.0f : 1.0f;
         float zl = sh_z[a], zh = sh_z[b];
         float hl = zl + sh_h[a], hr = zh + sh_h[b];
-        float dx = d.sdc[gid];
-        float xq = q_in[gid];
         float xwh = maxf(hl, hr) - maxf(maxf(zl, zh), kDh);
         float difference = hr - hl;
         if (kHanging) {
@@ -170,7 +220,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
             }
         }
         float xdq = (d.neg_g * difference / dx) * maxf(xwh, 0.0f) * dt;
-        float n = m.side_n[gid];
         float ratio = 0.0f;
         if (xq != 0.0f) ratio = xq / pow_f32(maxf(xwh, 0.00001f), d.seven_thirds);
         float xf = 1.0f + d.g * dt * (n * n) * fabsf(ratio);
@@ -186,9 +235,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
         }
         float new_q = (d.sita * xq + d.half_rest * nb + xdq) / xf;
         new_q = xwh < d.min_h ? 0.0f : new_q;
-        new_q *= m.sbf[gid] == 1 ? 0.0f : 1.0f;
+        new_q *= bf;
         sh_q[j] = new_q;
-        sh_len[j] = m.length[gid];
+        sh_len[j] = len;
     }
     __syncthreads();
 
@@ -196,17 +245,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
     {
         uint32_t my_limited = 0;
         uint32_t my_min = __float_as_uint(1.0f);
-        for (int i = 1 + tid; i <= tl.n_r012; i += kThreads) {
-            const int g = sh_g[i];
-            int bi = m.boundary_id[g];
-            int kind = bi >= 0 ? m.kind[bi] : -1;
+        for (int i = 1 + tid; i <= tl.n_r012; i += NT) {
+            const int bi = sh_bi[i];
+            int kind = -1;
             float discharge = 0.0f;
-            if (kind == 1) discharge = d.values[bi] * m.weight[g];
-            float rainq = 0.0f;
-            if (raining) rainq = d.rain_rates[m.rain_index[g]];
+            if (bi >= 0) {
+                kind = m.kind[bi];
+                if (kind == 1) discharge = d.values[bi] * m.weight[sh_g[i]];
+            }
+            float rainq = sh_rq[i];
             float pipe = 0.0f;
             float positive = (maxf(pipe, 0.0f) + maxf(discharge, 0.0f)) * dt;
-            float area = m.area[g];
+            float area = sh_area[i];
             float available = sh_h[i] * area + positive + rainq * dt * area;
             float outgoing = (maxf(-pipe, 0.0f) + maxf(-discharge, 0.0f)) * dt;
             uint32_t fd = tl.fdesc[i];
@@ -242,7 +292,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
     // P3: final discharge of faces(ring <= 1) (solver_compact.py:516-522).
     {
         uint32_t my_faces = 0;
-        for (int j = tid; j < tl.n_qf; j += kThreads) {
+        for (int j = tid; j < tl.n_qf; j += NT) {
             const uint32_t lh = tl.lohi[j];
             const int a = (int)(lh & 0xffffu), b = (int)(lh >> 16);
             float q = sh_q[j];
@@ -256,22 +306,24 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
     __syncthreads();
 
     // P4: sources and depth update (solver_compact.py:525-610). Ring 0 cells
-    // are mapped to threads as tile offset o = tid + 256 * k, so the cells of
-    // budget block k of the tile sit in thread order for the budget tree.
+    // are mapped to threads as tile offset o = tid + NT * k, so each budget
+    // block of the tile sits on one 256-thread half in thread order.
     CellTerms<CPT> terms;
     uint32_t my_wet = 0;
+    const int T = d.terms;
+    const int B = m.b_num;
     const uint32_t step_hi = c->step_end[0], step_lo = c->step_end[1];
 #pragma unroll
     for (int kk = 0; kk < CPT; ++kk) {
         terms.removed[kk] = 0.0f; terms.floor_v[kk] = 0.0f; terms.discharge[kk] = 0.0f;
         for (int q5 = 0; q5 < 5; ++q5) terms.level[kk][q5] = 0.0f;
         terms.bi[kk] = -1; terms.kind[kk] = -1;
-        const int o = tid + kThreads * kk;
+        const int o = tid + NT * kk;
         const int slot = o - tl.r0off + 1;
         if (o < tl.r0off || slot > tl.n_r0) continue;
         const int g = tl.cbase + o;
-        int bi = m.boundary_id[g];
-        int kind = bi >= 0 ? m.kind[bi] : -1;
+        const int bi = sh_bi[slot];
+        const int kind = bi >= 0 ? m.kind[bi] : -1;
         terms.bi[kk] = bi; terms.kind[kk] = kind;
         float sc = sh_s[slot];
         float pq = 0.0f;
@@ -283,8 +335,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
             terms.discharge[kk] = discharge * dt;
         }
         float ssq = pipe + discharge;
-        float rainq = 0.0f;
-        if (raining) rainq = d.rain_rates[m.rain_index[g]];
+        float rainq = sh_rq[slot];
         float infil;
         if (rainq > 0.0f) {
             float rt = rt_in[g] + dt;
@@ -300,7 +351,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
         face_sums(tl, sh_q, sh_len, slot, fl);
         float ql = fl[0], qr = fl[1], qb = fl[2], qt = fl[3];
         float tq = ql - qr + qb - qt + ssq;
-        float ea = m.area[g];
+        float ea = sh_area[slot];
         float rain_depth = rainq * dt;
         float increment = tq * dt / ea + rain_depth;
         float previous = sh_h[slot];
@@ -331,19 +382,26 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
             v = (qb + qt) / m.width[g] / h / 2.0f;
         }
         float speed = sqrtf(u * u + v * v);
-        float ms = m.max_speed[g];
-        if (speed > ms) m.max_speed[g] = speed;
+        if (speed > m.max_speed[g]) m.max_speed[g] = speed;
         if (depth > m.max_depth[g]) {
             m.max_depth[g] = depth;
             m.peak_hi[g] = step_hi; m.peak_lo[g] = step_lo;
         }
         my_wet += depth >= d.min_h ? 1u : 0u;
+        if (T <= 32) {
+            uint32_t mask = 0;
+            for (int t = 0; t < T; ++t)
+                if (term_value(t, B, terms.removed[kk], terms.floor_v[kk], terms.level[kk], terms.discharge[kk],
+                               bi, kind) != 0.0f)
+                    mask |= 1u << t;
+            if (mask) atomicOr(&sh_mask[kk][tid >> 8], mask);
+        }
     }
     // ring 1: the new depth only (for the CFL of owned sides)
-    for (int i = tl.n_r0 + 1 + tid; i <= tl.n_r01; i += kThreads) {
+    for (int i = tl.n_r0 + 1 + tid; i <= tl.n_r01; i += NT) {
         const int g = sh_g[i];
-        int bi = m.boundary_id[g];
-        int kind = bi >= 0 ? m.kind[bi] : -1;
+        const int bi = sh_bi[i];
+        const int kind = bi >= 0 ? m.kind[bi] : -1;
         float sc = sh_s[i];
         float pq = 0.0f;
         float pipe = maxf(pq, 0.0f) + minf(pq, 0.0f) * sc;
@@ -353,8 +411,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
             discharge = maxf(requested, 0.0f) + minf(requested, 0.0f) * sc;
         }
         float ssq = pipe + discharge;
-        float rainq = 0.0f;
-        if (raining) rainq = d.rain_rates[m.rain_index[g]];
+        float rainq = sh_rq[i];
         float infil;
         if (rainq > 0.0f) {
             float rt = rt_in[g] + dt;
@@ -367,7 +424,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
         float fl[4];
         face_sums(tl, sh_q, sh_len, i, fl);
         float tq = fl[0] - fl[1] + fl[2] - fl[3] + ssq;
-        float ea = m.area[g];
+        float ea = sh_area[i];
         float rain_depth = rainq * dt;
         float increment = tq * dt / ea + rain_depth;
         float raw_depth = sh_h[i] + increment;
@@ -379,38 +436,30 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
     __syncthreads();
 
     // Budget partials: one writer per (budget block, term), fixed tree.
-    {
-        const int T = d.terms;
-        const int B = m.b_num;
 #pragma unroll
-        for (int kk = 0; kk < CPT; ++kk) {
-            const int blk = (tl.cbase >> 8) + kk;
-            if (blk >= d.blocks) break;  // uniform across the block
-            double *acc_s = d.acc_sum + (size_t)blk * T;
-            double *acc_c = d.acc_comp + (size_t)blk * T;
-            for (int t = 0; t < T; ++t) {
-                float val = 0.0f;
-                if (t == 0) val = terms.removed[kk];
-                else if (t == 1) val = terms.kind[kk] == 0 ? 0.0f : terms.floor_v[kk];
-                else if (t == 2) val = terms.kind[kk] == 0 ? terms.floor_v[kk] : 0.0f;
-                else if (t == 3) val = 0.0f;  // pipe exchange: no coupling
-                else if (t < 4 + 5 * B) {
-                    int b = (t - 4) / 5;
-                    if (b == terms.bi[kk] && terms.kind[kk] == 0) val = terms.level[kk][(t - 4) % 5];
-                } else {
-                    int b = t - 4 - 5 * B;
-                    if (b == terms.bi[kk]) val = terms.discharge[kk];
-                }
-                if (!__syncthreads_or(val != 0.0f)) continue;
-                double sum = block_tree((double)val, sh_tree);
-                if (tid == 0) acc_add(acc_s + t, acc_c + t, sum);
+    for (int kk = 0; kk < CPT; ++kk) {
+        const int blk0 = (tl.cbase >> 8) + kk * (NT / 256);
+        uint32_t any = 0;
+        for (int hh = 0; hh < NT / 256; ++hh) any |= sh_mask[kk][hh];
+        if (T > 32) any = 0xffffffffu;
+        for (int t = 0; t < T; ++t) {
+            if (t < 32 && !((any >> t) & 1u)) continue;
+            float val = term_value(t, B, terms.removed[kk], terms.floor_v[kk], terms.level[kk], terms.discharge[kk],
+                                   terms.bi[kk], terms.kind[kk]);
+            if (T > 32 && !__syncthreads_or(val != 0.0f)) continue;
+            double sum = tree_halves<NT>((double)val, sh_tree);
+            const int blk = blk0 + (tid >> 8);
+            const bool has = T > 32 ? true : ((sh_mask[kk][tid >> 8] >> t) & 1u) != 0;
+            if ((tid & 255) == 0 && blk < d.blocks && has) {
+                if (T > 32 && sum == 0.0) continue;
+                acc_add(d.acc_sum + (size_t)blk * T + t, d.acc_comp + (size_t)blk * T + t, sum);
             }
         }
     }
 
     // P5: owned sides: final q out, CFL with the new depths.
     unsigned long long best = kCflEmpty;
-    for (int j = tid; j < tl.n_owned; j += kThreads) {
+    for (int j = tid; j < tl.n_owned; j += NT) {
         const int gid = tl.sbase + tl.srel[j];
         const uint32_t lh = tl.lohi[j];
         const int a = (int)(lh & 0xffffu), b = (int)(lh >> 16);
@@ -432,7 +481,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_tiled(Dev d)
     __syncthreads();
     if (tid == 0) {
         unsigned long long bmin = kCflEmpty;
-        for (int w = 0; w < kThreads / 32; ++w) bmin = sh_min[w] < bmin ? sh_min[w] : bmin;
+        for (int w = 0; w < NT / 32; ++w) bmin = sh_min[w] < bmin ? sh_min[w] : bmin;
         if (bmin != kCflEmpty) atomicMin(&c->cfl_packed, bmin);
         if (sh_cnt[0]) {
             atomicAdd(&c->limited_cells, sh_cnt[0]);
@@ -745,26 +794,26 @@ void set_smem(K kernel, size_t bytes)
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-template <int CPT>
+template <int NT, int CPT>
 void set_smem_all(size_t bytes)
 {
-    set_smem(k_step_tiled<true, false, CPT>, bytes);
-    set_smem(k_step_tiled<false, false, CPT>, bytes);
-    set_smem(k_step_tiled<true, true, CPT>, bytes);
-    set_smem(k_step_tiled<false, true, CPT>, bytes);
+    set_smem(k_step_tiled<true, false, NT, CPT>, bytes);
+    set_smem(k_step_tiled<false, false, NT, CPT>, bytes);
+    set_smem(k_step_tiled<true, true, NT, CPT>, bytes);
+    set_smem(k_step_tiled<false, true, NT, CPT>, bytes);
 }
 
-template <int CPT>
+template <int NT, int CPT>
 void launch_step(const Dev &d, size_t smem, cudaStream_t s)
 {
     const int grid = d.plan.n_tiles;
     const bool hanging = d.m.hang_cells > 0;
     if (d.theta_one) {
-        if (hanging) k_step_tiled<true, true, CPT><<<grid, kThreads, smem, s>>>(d);
-        else k_step_tiled<true, false, CPT><<<grid, kThreads, smem, s>>>(d);
+        if (hanging) k_step_tiled<true, true, NT, CPT><<<grid, NT, smem, s>>>(d);
+        else k_step_tiled<true, false, NT, CPT><<<grid, NT, smem, s>>>(d);
     } else {
-        if (hanging) k_step_tiled<false, true, CPT><<<grid, kThreads, smem, s>>>(d);
-        else k_step_tiled<false, false, CPT><<<grid, kThreads, smem, s>>>(d);
+        if (hanging) k_step_tiled<false, true, NT, CPT><<<grid, NT, smem, s>>>(d);
+        else k_step_tiled<false, false, NT, CPT><<<grid, NT, smem, s>>>(d);
     }
 }
 
@@ -859,9 +908,13 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     std::vector<int32_t> tp, tc, ts;
     int max_ext = 0, max_sides = 0, tile = 0;
     size_t smem = 0;
-    for (int T : {1024, 512, 256}) {
+    // Small meshes take small tiles so that every SM gets work.
+    std::vector<int> sizes = {1024, 512, 256};
+    if (m.e_num < 148 * 2 * 1024) sizes = {256};
+    else if (m.e_num < 148 * 4 * 1024) sizes = {512, 256};
+    for (int T : sizes) {
         if (plan_tiles(hm, T, patterns, tp, tc, ts, max_ext, max_sides, reason)) return bad(reason);
-        smem = (size_t)max_ext * 16 + (size_t)max_sides * 8;
+        smem = (size_t)max_ext * 28 + (size_t)max_sides * 8;
         if (smem <= (size_t)kMaxSharedBytes) { tile = T; break; }
     }
     if (!tile) return bad("tile halos exceed shared memory (cell numbering is not spatially coherent)");
@@ -907,7 +960,7 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     P.tile = tile;
     P.max_ext = max_ext;
     P.max_sides = max_sides;
-    P.cells_per_thread = tile / kThreads;
+    P.cells_per_thread = tile == 1024 ? 2 : 1;
     P.tile_pattern = (const int32_t *)(b + o_tp);
     P.tile_cbase = (const int32_t *)(b + o_tc);
     P.tile_sbase = (const int32_t *)(b + o_ts);
@@ -921,9 +974,9 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     out->device_memory = mem;
     out->shared_bytes = smem;
     out->patterns = (int)patterns.size();
-    if (P.cells_per_thread == 4) set_smem_all<4>(smem);
-    else if (P.cells_per_thread == 2) set_smem_all<2>(smem);
-    else set_smem_all<1>(smem);
+    if (tile == 1024) set_smem_all<512, 2>(smem);
+    else if (tile == 512) set_smem_all<512, 1>(smem);
+    else set_smem_all<256, 1>(smem);
     return 0;
 }
 
@@ -932,10 +985,10 @@ void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s)
     const nhf_mesh &m = d.m;
     if (m.hang_cells > 0) k_pressure_tiled<<<(m.hang_cells + 255) / 256, 256, 0, s>>>(d);
     if (!d.theta_one) k_face_qn_tiled<<<(m.e_num + 255) / 256, 256, 0, s>>>(d);
-    switch (d.plan.cells_per_thread) {
-    case 4: launch_step<4>(d, b.shared_bytes, s); break;
-    case 2: launch_step<2>(d, b.shared_bytes, s); break;
-    default: launch_step<1>(d, b.shared_bytes, s); break;
+    switch (d.plan.tile) {
+    case 1024: launch_step<512, 2>(d, b.shared_bytes, s); break;
+    case 512: launch_step<512, 1>(d, b.shared_bytes, s); break;
+    default: launch_step<256, 1>(d, b.shared_bytes, s); break;
     }
 }
 
