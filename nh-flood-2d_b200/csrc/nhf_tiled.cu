@@ -35,7 +35,7 @@
 namespace nhf {
 namespace {
 
-constexpr int kMaxSharedBytes = 110 * 1024;
+constexpr int kMaxSharedBytes = 108 * 1024;
 constexpr uint8_t kOwned = 1, kFinal = 2;
 
 // ----------------------------------------------------------------- kernels
@@ -47,7 +47,7 @@ struct CellTerms {
 };
 
 struct Tile {
-    int n_ext, n_r0, n_r01, n_r012, n_sides, n_owned, n_qf, r0off;
+    int n_ext, n_r0, n_r01, n_r012, n_sides, n_owned, n_qf, r0off, n_faces;
     int cbase, sbase;
     const int32_t *ext;
     const int32_t *srel;
@@ -157,10 +157,11 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
     {
         const int t = blockIdx.x;
         const int pat = P.tile_pattern[t];
-        const int32_t *cnt = P.p_counts + 8 * pat;
+        const int32_t *cnt = P.p_counts + 12 * pat;
         const int32_t *off = P.p_offsets + 4 * pat;
         tl.n_ext = cnt[0]; tl.n_r0 = cnt[1]; tl.n_r01 = cnt[2]; tl.n_r012 = cnt[3];
         tl.n_sides = cnt[4]; tl.n_owned = cnt[5]; tl.n_qf = cnt[6]; tl.r0off = cnt[7];
+        tl.n_faces = cnt[8];
         tl.cbase = P.tile_cbase[t];
         tl.sbase = P.tile_sbase[t];
         tl.ext = P.ext_rel + off[0];
@@ -177,11 +178,19 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
     float *sh_area = sh_rq + E;
     int *sh_g = reinterpret_cast<int *>(sh_area + E);
     int *sh_bi = sh_g + E;       // boundary id, -1 for none
-    float *sh_q = reinterpret_cast<float *>(sh_bi + E);  // q*, then final q
+    uint32_t *sh_fdesc = reinterpret_cast<uint32_t *>(sh_bi + E);
+    float *sh_q = reinterpret_cast<float *>(sh_fdesc + E);  // q*, then final q
     float *sh_len = sh_q + P.max_sides;
+    int32_t *sh_srel = reinterpret_cast<int32_t *>(sh_len + P.max_sides);
+    uint32_t *sh_lohi = reinterpret_cast<uint32_t *>(sh_srel + P.max_sides);
+    uint16_t *sh_fidx = reinterpret_cast<uint16_t *>(sh_lohi + P.max_sides);
 
-    // P0: stage the tile and its rings; cells of rings 0..2 also bring the
+    // P0: stage the tile's index tables (contiguous per pattern) and, for the
+    // tile and its rings, depth and bed; cells of rings 0..2 also bring the
     // per-cell inputs of the donor factor and the depth update.
+    for (int i = tid; i < tl.n_sides; i += NT) { sh_srel[i] = tl.srel[i]; sh_lohi[i] = tl.lohi[i]; }
+    for (int i = tid; i <= tl.n_r012; i += NT) sh_fdesc[i] = tl.fdesc[i];
+    for (int i = tid; i < tl.n_faces; i += NT) sh_fidx[i] = tl.fidx[i];
     for (int i = tid; i < tl.n_ext; i += NT) {
         int g = i ? tl.cbase + tl.ext[i] : 0;
         sh_g[i] = g;
@@ -194,48 +203,56 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
             sh_rq[i] = raining ? d.rain_rates[m.rain_index[g]] : 0.0f;
         }
     }
+    tl.srel = sh_srel;
+    tl.lohi = sh_lohi;
+    tl.fdesc = sh_fdesc;
+    tl.fidx = sh_fidx;
     __syncthreads();
 
-    // P1: momentum (solver_compact.py:439-486) for every local side.
+    // P1: momentum (solver_compact.py:439-486) for every local side. A side
+    // whose flow height is below min_h gets q = +0 whatever its other inputs
+    // (select then * bf), so their loads and arithmetic are skipped.
     for (int j = tid; j < tl.n_sides; j += NT) {
         const int gid = tl.sbase + tl.srel[j];
         const uint32_t lh = tl.lohi[j];
         const int a = (int)(lh & 0xffffu), b = (int)(lh >> 16);
-        float xq = q_in[gid];
-        float dx = d.sdc[gid];
-        float n = m.side_n[gid];
         float len = m.length[gid];
-        float bf = m.sbf[gid] == 1 ? 0.0f : 1.0f;
         float zl = sh_z[a], zh = sh_z[b];
         float hl = zl + sh_h[a], hr = zh + sh_h[b];
         float xwh = maxf(hl, hr) - maxf(maxf(zl, zh), kDh);
-        float difference = hr - hl;
-        if (kHanging) {
-            int index = m.edge_index[gid];
-            if (index >= 0 && sh_h[a] > d.min_h && sh_h[b] > d.min_h) {
-                int axis = m.topology[3 * gid] == 2 ? 1 : 0;
-                float o0 = m.offsets[2 * index], o1 = m.offsets[2 * index + 1];
-                if (o0 != 0.0f) difference -= d.gradients[2 * m.slots[2 * index] + axis] * o0;
-                if (o1 != 0.0f) difference += d.gradients[2 * m.slots[2 * index + 1] + axis] * o1;
+        float new_q = 0.0f;
+        if (!(xwh < d.min_h)) {
+            float xq = q_in[gid];
+            float dx = d.sdc[gid];
+            float n = m.side_n[gid];
+            float bf = m.sbf[gid] == 1 ? 0.0f : 1.0f;
+            float difference = hr - hl;
+            if (kHanging) {
+                int index = m.edge_index[gid];
+                if (index >= 0 && sh_h[a] > d.min_h && sh_h[b] > d.min_h) {
+                    int axis = m.topology[3 * gid] == 2 ? 1 : 0;
+                    float o0 = m.offsets[2 * index], o1 = m.offsets[2 * index + 1];
+                    if (o0 != 0.0f) difference -= d.gradients[2 * m.slots[2 * index] + axis] * o0;
+                    if (o1 != 0.0f) difference += d.gradients[2 * m.slots[2 * index + 1] + axis] * o1;
+                }
             }
+            float xdq = (d.neg_g * difference / dx) * maxf(xwh, 0.0f) * dt;
+            float ratio = 0.0f;
+            if (xq != 0.0f) ratio = xq / pow_f32(maxf(xwh, 0.00001f), d.seven_thirds);
+            float xf = 1.0f + d.g * dt * (n * n) * fabsf(ratio);
+            float nb;
+            if (kThetaOne) {
+                nb = 0.0f + 0.0f;
+            } else {
+                int so = m.topology[3 * gid];
+                int dl = so == 2 ? 0 : 2, dr = so == 2 ? 1 : 3;
+                int ga = sh_g[a], gb = sh_g[b];
+                nb = boundary_neighbor_sum(xq, d.face_qn[4 * ga + dl], d.face_qn[4 * gb + dr],
+                                           m.open_face[4 * ga + dl], m.open_face[4 * gb + dr]);
+            }
+            new_q = (d.sita * xq + d.half_rest * nb + xdq) / xf;
+            new_q *= bf;
         }
-        float xdq = (d.neg_g * difference / dx) * maxf(xwh, 0.0f) * dt;
-        float ratio = 0.0f;
-        if (xq != 0.0f) ratio = xq / pow_f32(maxf(xwh, 0.00001f), d.seven_thirds);
-        float xf = 1.0f + d.g * dt * (n * n) * fabsf(ratio);
-        float nb;
-        if (kThetaOne) {
-            nb = 0.0f + 0.0f;
-        } else {
-            int so = m.topology[3 * gid];
-            int dl = so == 2 ? 0 : 2, dr = so == 2 ? 1 : 3;
-            int ga = sh_g[a], gb = sh_g[b];
-            nb = boundary_neighbor_sum(xq, d.face_qn[4 * ga + dl], d.face_qn[4 * gb + dr],
-                                       m.open_face[4 * ga + dl], m.open_face[4 * gb + dr]);
-        }
-        float new_q = (d.sita * xq + d.half_rest * nb + xdq) / xf;
-        new_q = xwh < d.min_h ? 0.0f : new_q;
-        new_q *= bf;
         sh_q[j] = new_q;
         sh_len[j] = len;
     }
@@ -313,24 +330,49 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
     const int T = d.terms;
     const int B = m.b_num;
     const uint32_t step_hi = c->step_end[0], step_lo = c->step_end[1];
+    // P4a: issue every per-cell load of this thread's ring-0 cells before any
+    // store, so the loads overlap.
+    int in_g[CPT], in_slot[CPT], in_kind[CPT];
+    float in_w[CPT], in_rt[CPT], in_f0[CPT], in_fc[CPT], in_k[CPT], in_inf[CPT], in_hgt[CPT], in_wid[CPT],
+        in_ms[CPT], in_md[CPT];
+#pragma unroll
+    for (int kk = 0; kk < CPT; ++kk) {
+        const int o = tid + NT * kk;
+        const int slot = o - tl.r0off + 1;
+        in_slot[kk] = (o < tl.r0off || slot > tl.n_r0) ? -1 : slot;
+        in_g[kk] = tl.cbase + o;
+        in_kind[kk] = -1;
+        in_w[kk] = in_rt[kk] = in_f0[kk] = in_fc[kk] = in_k[kk] = 0.0f;
+        in_inf[kk] = in_hgt[kk] = in_wid[kk] = in_ms[kk] = in_md[kk] = 0.0f;
+        if (in_slot[kk] < 0) continue;
+        const int g = in_g[kk];
+        const int bi = sh_bi[slot];
+        if (bi >= 0) { in_kind[kk] = m.kind[bi]; in_w[kk] = m.weight[g]; }
+        if (sh_rq[slot] > 0.0f) { in_rt[kk] = rt_in[g]; in_f0[kk] = m.f0[g]; in_fc[kk] = m.fc[g]; in_k[kk] = m.k[g]; }
+        in_inf[kk] = m.infiltration[g];
+        in_hgt[kk] = m.height[g];
+        in_wid[kk] = m.width[g];
+        in_ms[kk] = m.max_speed[g];
+        in_md[kk] = m.max_depth[g];
+    }
+    // P4b: the update itself.
 #pragma unroll
     for (int kk = 0; kk < CPT; ++kk) {
         terms.removed[kk] = 0.0f; terms.floor_v[kk] = 0.0f; terms.discharge[kk] = 0.0f;
         for (int q5 = 0; q5 < 5; ++q5) terms.level[kk][q5] = 0.0f;
         terms.bi[kk] = -1; terms.kind[kk] = -1;
-        const int o = tid + NT * kk;
-        const int slot = o - tl.r0off + 1;
-        if (o < tl.r0off || slot > tl.n_r0) continue;
-        const int g = tl.cbase + o;
+        const int slot = in_slot[kk];
+        if (slot < 0) continue;
+        const int g = in_g[kk];
         const int bi = sh_bi[slot];
-        const int kind = bi >= 0 ? m.kind[bi] : -1;
+        const int kind = in_kind[kk];
         terms.bi[kk] = bi; terms.kind[kk] = kind;
         float sc = sh_s[slot];
         float pq = 0.0f;
         float pipe = maxf(pq, 0.0f) + minf(pq, 0.0f) * sc;
         float discharge = 0.0f;
         if (kind == 1) {
-            float requested = d.values[bi] * m.weight[g];
+            float requested = d.values[bi] * in_w[kk];
             discharge = maxf(requested, 0.0f) + minf(requested, 0.0f) * sc;
             terms.discharge[kk] = discharge * dt;
         }
@@ -338,14 +380,14 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
         float rainq = sh_rq[slot];
         float infil;
         if (rainq > 0.0f) {
-            float rt = rt_in[g] + dt;
+            float rt = in_rt[kk] + dt;
             rt_out[g] = rt;
-            float f0 = m.f0[g], fc = m.fc[g];
+            float f0 = in_f0[kk], fc = in_fc[kk];
             float diff = f0 - fc;
-            infil = diff == 0.0f ? fc + 0.0f : fc + diff * exp_f32(-m.k[g] * rt / 3600.0f);
-            if (__float_as_uint(infil) != __float_as_uint(m.infiltration[g])) m.infiltration[g] = infil;
+            infil = diff == 0.0f ? fc + 0.0f : fc + diff * exp_f32(-in_k[kk] * rt / 3600.0f);
+            if (__float_as_uint(infil) != __float_as_uint(in_inf[kk])) m.infiltration[g] = infil;
         } else {
-            infil = m.infiltration[g];
+            infil = in_inf[kk];
         }
         float fl[4];
         face_sums(tl, sh_q, sh_len, slot, fl);
@@ -353,7 +395,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
         float tq = ql - qr + qb - qt + ssq;
         float ea = sh_area[slot];
         float rain_depth = rainq * dt;
-        float increment = tq * dt / ea + rain_depth;
+        float flux = tq * dt;
+        // flux / ea for flux = +-0 is flux itself: skip the division
+        float increment = (flux == 0.0f ? flux : flux / ea) + rain_depth;
         float previous = sh_h[slot];
         float raw_depth = previous + increment;
         float removed = minf(infil * dt, maxf(raw_depth, 0.0f));
@@ -378,22 +422,26 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
         float h = maxf(depth, 0.01f);
         float u = 0.0f, v = 0.0f;
         if (depth >= d.min_h) {
-            u = (ql + qr) / m.height[g] / h / 2.0f;
-            v = (qb + qt) / m.width[g] / h / 2.0f;
+            // x / 2 and x * 0.5 are the same correctly rounded value
+            u = (ql + qr) / in_hgt[kk] / h * 0.5f;
+            v = (qb + qt) / in_wid[kk] / h * 0.5f;
         }
-        float speed = sqrtf(u * u + v * v);
-        if (speed > m.max_speed[g]) m.max_speed[g] = speed;
-        if (depth > m.max_depth[g]) {
+        float s2 = u * u + v * v;
+        float speed = s2 == 0.0f ? 0.0f : sqrtf(s2);
+        if (speed > in_ms[kk]) m.max_speed[g] = speed;
+        if (depth > in_md[kk]) {
             m.max_depth[g] = depth;
             m.peak_hi[g] = step_hi; m.peak_lo[g] = step_lo;
         }
         my_wet += depth >= d.min_h ? 1u : 0u;
         if (T <= 32) {
             uint32_t mask = 0;
-            for (int t = 0; t < T; ++t)
-                if (term_value(t, B, terms.removed[kk], terms.floor_v[kk], terms.level[kk], terms.discharge[kk],
-                               bi, kind) != 0.0f)
-                    mask |= 1u << t;
+            if (terms.removed[kk] != 0.0f) mask |= 1u;
+            if (terms.floor_v[kk] != 0.0f) mask |= kind == 0 ? 4u : 2u;
+            if (kind == 0)
+                for (int q5 = 0; q5 < 5; ++q5)
+                    if (terms.level[kk][q5] != 0.0f) mask |= 1u << (4 + 5 * bi + q5);
+            if (kind == 1 && terms.discharge[kk] != 0.0f) mask |= 1u << (4 + 5 * B + bi);
             if (mask) atomicOr(&sh_mask[kk][tid >> 8], mask);
         }
     }
@@ -426,7 +474,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
         float tq = fl[0] - fl[1] + fl[2] - fl[3] + ssq;
         float ea = sh_area[i];
         float rain_depth = rainq * dt;
-        float increment = tq * dt / ea + rain_depth;
+        float flux = tq * dt;
+        float increment = (flux == 0.0f ? flux : flux / ea) + rain_depth;
         float raw_depth = sh_h[i] + increment;
         float removed = minf(infil * dt, maxf(raw_depth, 0.0f));
         raw_depth -= removed;
@@ -459,6 +508,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
 
     // P5: owned sides: final q out, CFL with the new depths.
     unsigned long long best = kCflEmpty;
+    // A side at the 0.01 m face-depth floor with q = 0 has the CFL value
+    // afa * L / sqrt(g * 0.01); it is reused while L repeats.
+    float dry_len = -1.0f, dry_cfl = 0.0f;
     for (int j = tid; j < tl.n_owned; j += NT) {
         const int gid = tl.sbase + tl.srel[j];
         const uint32_t lh = tl.lohi[j];
@@ -469,7 +521,16 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
             float zl = sh_z[a], zh = sh_z[b];
             float head = maxf(zl + sh_s[a], zh + sh_s[b]);
             float h = maxf(head - maxf(maxf(zl, zh), kDh), 0.01f);
-            float cfl = d.afa * sh_len[j] / (sqrtf(d.g * h) + fabsf(qv) / h);
+            float cfl;
+            if (h == 0.01f && qv == 0.0f) {
+                if (sh_len[j] != dry_len) {
+                    dry_len = sh_len[j];
+                    dry_cfl = d.afa * dry_len / (sqrtf(d.g * h) + fabsf(qv) / h);
+                }
+                cfl = dry_cfl;
+            } else {
+                cfl = d.afa * sh_len[j] / (sqrtf(d.g * h) + fabsf(qv) / h);
+            }
             unsigned long long key = ((unsigned long long)__float_as_uint(cfl) << 32) | (unsigned)gid;
             best = key < best ? key : best;
         }
@@ -658,7 +719,7 @@ bool consistent(const HostMesh &hm, std::string &why)
 
 int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::vector<int32_t> &tile_pattern,
                std::vector<int32_t> &tile_cbase, std::vector<int32_t> &tile_sbase, int &max_ext, int &max_sides,
-               std::string &why)
+               int &max_faces, std::string &why)
 {
     const int e = hm.e, s = hm.s;
     // cell adjacency through interior sides
@@ -684,7 +745,7 @@ int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::v
     tile_pattern.assign(n_tiles, 0);
     tile_cbase.assign(n_tiles, 0);
     tile_sbase.assign(n_tiles, 0);
-    max_ext = max_sides = 0;
+    max_ext = max_sides = max_faces = 0;
     std::vector<int> ext, sides;
     for (int t = 0; t < n_tiles; ++t) {
         const int cbase = t * T;
@@ -742,7 +803,8 @@ int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::v
         if ((int)ext.size() > 65535 || (int)sides.size() > 65535) { why = "tile halo too large"; return 1; }
         int sbase = sides.empty() ? 0 : *std::min_element(sides.begin(), sides.end());
         Pattern p;
-        p.counts = {(int)ext.size(), n_r0, n_r01, n_r012, (int)sides.size(), n_owned, n_qf, r0_first - cbase};
+        p.counts = {(int)ext.size(), n_r0, n_r01, n_r012, (int)sides.size(), n_owned, n_qf, r0_first - cbase,
+                    0, 0, 0, 0};
         p.ext.resize(ext.size());
         p.ext[0] = 0;
         for (size_t i = 1; i < ext.size(); ++i) p.ext[i] = ext[i] - cbase;
@@ -768,6 +830,8 @@ int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::v
             p.fdesc[i] = start | (counts << 16);
         }
         if (p.fidx.size() > 65535) { why = "tile face table too large"; return 1; }
+        p.counts[8] = (int)p.fidx.size();
+        max_faces = std::max(max_faces, (int)p.fidx.size());
         max_ext = std::max(max_ext, (int)ext.size());
         max_sides = std::max(max_sides, (int)sides.size());
         uint64_t hsh = pattern_hash(p);
@@ -906,15 +970,15 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     if (!consistent(hm, reason)) return bad(reason);
     std::vector<Pattern> patterns;
     std::vector<int32_t> tp, tc, ts;
-    int max_ext = 0, max_sides = 0, tile = 0;
+    int max_ext = 0, max_sides = 0, max_faces = 0, tile = 0;
     size_t smem = 0;
     // Small meshes take small tiles so that every SM gets work.
     std::vector<int> sizes = {1024, 512, 256};
     if (m.e_num < 148 * 2 * 1024) sizes = {256};
     else if (m.e_num < 148 * 4 * 1024) sizes = {512, 256};
     for (int T : sizes) {
-        if (plan_tiles(hm, T, patterns, tp, tc, ts, max_ext, max_sides, reason)) return bad(reason);
-        smem = (size_t)max_ext * 28 + (size_t)max_sides * 8;
+        if (plan_tiles(hm, T, patterns, tp, tc, ts, max_ext, max_sides, max_faces, reason)) return bad(reason);
+        smem = (size_t)max_ext * 32 + (size_t)max_sides * 16 + (size_t)max_faces * 2 + 16;
         if (smem <= (size_t)kMaxSharedBytes) { tile = T; break; }
     }
     if (!tile) return bad("tile halos exceed shared memory (cell numbering is not spatially coherent)");
