@@ -303,3 +303,236 @@ def simulate(workload: Workload, domain_dir, *, engine_factory=None, end_time=No
                             workload.sbf, workload.geometry, workload.forcing, engine_factory=engine_factory,
                             batch_size=batch_size, state=workload.initial_state())
     return row, record
+
+
+# ------------------------------------------------------------ quadtree mesh
+
+def _morton(i: np.ndarray, j: np.ndarray) -> np.ndarray:
+    """Interleave the bits of two nonnegative < 2**16 integer arrays."""
+    def spread(v):
+        v = v.astype(np.uint64) & np.uint64(0xFFFF)
+        v = (v | (v << np.uint64(8))) & np.uint64(0x00FF00FF)
+        v = (v | (v << np.uint64(4))) & np.uint64(0x0F0F0F0F)
+        v = (v | (v << np.uint64(2))) & np.uint64(0x33333333)
+        v = (v | (v << np.uint64(1))) & np.uint64(0x55555555)
+        return v
+    return spread(i) | (spread(j) << np.uint64(1))
+
+
+def quadtree_mesh(leaf_level: np.ndarray, leaf_i: np.ndarray, leaf_j: np.ndarray, base: float, levels: int,
+                  nx0: int, ny0: int, bed_at, land_at) -> MeshData:
+    """Mesh of the leaves (level, i, j) of a 2:1-balanced quadtree over an
+    nx0 x ny0 grid of level-0 cells of size ``base``; a level-L cell has size
+    base / 2**L. Leaves are numbered in Morton order of their lower-left
+    corner on the finest grid. Each side is created once from its lower
+    (west/south) cell; a face with two finer neighbours has two sides,
+    ordered along the face."""
+    fine = 1 << (levels - 1)
+    L = leaf_level.astype(np.int64)
+    span = fine >> L                                   # size in finest cells
+    fi, fj = leaf_i.astype(np.int64) * span, leaf_j.astype(np.int64) * span
+    order = np.argsort(_morton(fi, fj), kind='stable')
+    L, span, fi, fj = L[order], span[order], fi[order], fj[order]
+    ii, jj = leaf_i.astype(np.int64)[order], leaf_j.astype(np.int64)[order]
+    n = len(L)
+    ids = np.arange(1, n + 1, dtype=np.int64)
+    key = (L << 40) | (ii << 20) | jj
+    sort_key = np.argsort(key)
+    sorted_keys = key[sort_key]
+
+    def lookup(lv, i, j):
+        k = (lv << 40) | (i << 20) | j
+        pos = np.searchsorted(sorted_keys, k)
+        pos = np.minimum(pos, n - 1)
+        hit = (sorted_keys[pos] == k) & (lv >= 0) & (lv < levels) & (i >= 0) & (j >= 0)
+        return np.where(hit, ids[sort_key[pos]], 0)
+
+    size = base / (1 << L).astype(np.float64)
+    nxl = nx0 << L
+    nyl = ny0 << L
+    sides = []  # (orient, lo, hi, length, x, y)
+
+    def neighbour_sides(orient):
+        # east (orient 2) or north (orient 1) neighbours of every leaf
+        di, dj = (1, 0) if orient == 2 else (0, 1)
+        ni, nj = ii + di, jj + dj
+        inside = (ni < nxl) if orient == 2 else (nj < nyl)
+        same = lookup(L, ni, nj)
+        coarse = np.where(L > 0, lookup(L - 1, ni >> 1, nj >> 1), 0)
+        f1 = lookup(L + 1, 2 * ni, 2 * nj)
+        f2 = lookup(L + 1, 2 * ni + (0 if orient == 2 else 1), 2 * nj + (1 if orient == 2 else 0))
+        out = []
+        # exterior
+        m = ~inside
+        if orient == 2:
+            out.append((ids[m], np.zeros(m.sum(), np.int64), size[m], (ii[m] + 1) * size[m], (jj[m] + .5) * size[m]))
+        else:
+            out.append((ids[m], np.zeros(m.sum(), np.int64), size[m], (ii[m] + .5) * size[m], (jj[m] + 1) * size[m]))
+        m = inside & (same > 0)
+        x = (ii + 1) * size if orient == 2 else (ii + .5) * size
+        y = (jj + .5) * size if orient == 2 else (jj + 1) * size
+        out.append((ids[m], same[m], size[m], x[m], y[m]))
+        m = inside & (same == 0) & (coarse > 0)
+        out.append((ids[m], coarse[m], size[m], x[m], y[m]))
+        m = inside & (same == 0) & (coarse == 0)
+        if np.any(m & ((f1 == 0) | (f2 == 0))):
+            raise ValueError('quadtree is not 2:1 balanced')
+        half = size / 2
+        for which, fid in ((0, f1), (1, f2)):
+            if orient == 2:
+                xs, ys = (ii + 1) * size, jj * size + (which + .5) * half
+            else:
+                xs, ys = ii * size + (which + .5) * half, (jj + 1) * size
+            out.append((ids[m], fid[m], half[m], xs[m], ys[m]))
+        lo = np.concatenate([o[0] for o in out]); hi = np.concatenate([o[1] for o in out])
+        return (np.full(len(lo), orient), lo, hi, np.concatenate([o[2] for o in out]),
+                np.concatenate([o[3] for o in out]), np.concatenate([o[4] for o in out]))
+
+    def edge_sides(orient):
+        # west (orient 2) or south (orient 1) exterior sides: lower cell 0
+        m = (ii == 0) if orient == 2 else (jj == 0)
+        x = np.zeros(m.sum()) if orient == 2 else (ii[m] + .5) * size[m]
+        y = (jj[m] + .5) * size[m] if orient == 2 else np.zeros(m.sum())
+        return (np.full(m.sum(), orient), np.zeros(m.sum(), np.int64), ids[m], size[m], x, y)
+
+    parts = [neighbour_sides(2), neighbour_sides(1), edge_sides(2), edge_sides(1)]
+    so = np.concatenate([p[0] for p in parts]); lo = np.concatenate([p[1] for p in parts])
+    hi = np.concatenate([p[2] for p in parts]); ln = np.concatenate([p[3] for p in parts])
+    sx = np.concatenate([p[4] for p in parts]); sy = np.concatenate([p[5] for p in parts])
+    owner = np.where(lo > 0, lo, hi)
+    sord = np.lexsort((sx, sy, so, owner))
+    so, lo, hi, ln, sx, sy = so[sord], lo[sord], hi[sord], ln[sord], sx[sord], sy[sord]
+    s = len(so) + 1
+    sid = np.arange(1, s, dtype=np.int64)
+    # faces: a vertical side is the right face of lo and the left face of hi
+    cell = np.concatenate([lo, hi])
+    direction = np.concatenate([np.where(so == 2, 1, 3), np.where(so == 2, 0, 2)])
+    pos = np.concatenate([np.where(so == 2, sy, sx)] * 2)
+    side = np.concatenate([sid, sid])
+    keep = cell > 0
+    cell, direction, pos, side = cell[keep], direction[keep], pos[keep], side[keep]
+    fo = np.lexsort((pos, direction, cell))
+    cell, direction, side = cell[fo], direction[fo], side[fo]
+    e = n + 1
+    counts = np.zeros((e, 4), np.int32)
+    np.add.at(counts, (cell, direction), 1)
+    flat = counts.reshape(-1)
+    starts = np.zeros(len(flat), np.int64)
+    starts[1:] = np.cumsum(flat)[:-1]
+    face_ptr = starts.reshape(e, 4).astype(np.int32)
+    face_ptr[0] = 0
+    x = np.zeros(e, np.float32); y = np.zeros(e, np.float32)
+    x[1:] = (ii + .5) * size; y[1:] = (jj + .5) * size
+    z = np.zeros(e, np.float32)
+    z[1:] = bed_at(x[1:].astype(np.float64), y[1:].astype(np.float64), L)
+    land = np.zeros(e, np.uint8)
+    land[1:] = land_at(x[1:].astype(np.float64), y[1:].astype(np.float64), L)
+    topo = np.zeros((s, 3), np.int32)
+    topo[1:, 0], topo[1:, 1], topo[1:, 2] = so, lo, hi
+    length = np.zeros(s, np.float32); length[1:] = ln
+    sxa = np.zeros(s, np.float32); sxa[1:] = sx
+    sya = np.zeros(s, np.float32); sya[1:] = sy
+    mesh = MeshData(x=x, y=y, z=z, land_type=land, counts=counts, face_ptr=face_ptr,
+                    isl_data=side.astype(np.int32), index=np.arange(e, dtype=np.uint32), side_length=length,
+                    side_x=sxa, side_y=sya, side_z=np.zeros(s, np.float32), side_attr=np.zeros(s, np.uint8),
+                    side_index=np.arange(s, dtype=np.uint32), topology=topo)
+    mesh.level = np.concatenate([[0], L]).astype(np.int8)
+    return mesh
+
+
+def meander_leaves(seed: int, width: float, base: float, buffer: float, half_channel: float):
+    """Leaves of a 3-level quadtree: 5 m cells within the channel, 10 m cells
+    within ``buffer`` of its centreline, 20 m elsewhere (base = 20 m)."""
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.1, 0.2) * width
+    wavelength = rng.uniform(0.25, 0.45) * width
+    phase = rng.uniform(0, 2 * np.pi)
+
+    def distance(x, y):
+        yc = width / 2 + amp * np.sin(2 * np.pi * x / wavelength + phase)
+        slope = amp * 2 * np.pi / wavelength * np.cos(2 * np.pi * x / wavelength + phase)
+        return np.abs(y - yc) / np.sqrt(1 + slope ** 2)
+
+    n0 = int(round(width / base))
+    j0, i0 = np.divmod(np.arange(n0 * n0, dtype=np.int64), n0)
+    c0x, c0y = (i0 + .5) * base, (j0 + .5) * base
+    refine0 = distance(c0x, c0y) - base * 0.7072 < buffer
+    leaves = [(np.zeros((~refine0).sum(), np.int64), i0[~refine0], j0[~refine0])]
+    pi, pj = i0[refine0], j0[refine0]
+    ci = np.concatenate([2 * pi, 2 * pi + 1, 2 * pi, 2 * pi + 1])
+    cj = np.concatenate([2 * pj, 2 * pj, 2 * pj + 1, 2 * pj + 1])
+    s1 = base / 2
+    refine1 = distance((ci + .5) * s1, (cj + .5) * s1) - s1 * 0.7072 < half_channel
+    leaves.append((np.ones((~refine1).sum(), np.int64), ci[~refine1], cj[~refine1]))
+    qi, qj = ci[refine1], cj[refine1]
+    gi = np.concatenate([2 * qi, 2 * qi + 1, 2 * qi, 2 * qi + 1])
+    gj = np.concatenate([2 * qj, 2 * qj, 2 * qj + 1, 2 * qj + 1])
+    leaves.append((np.full(len(gi), 2, np.int64), gi, gj))
+    lv = np.concatenate([l[0] for l in leaves]); li = np.concatenate([l[1] for l in leaves])
+    lj = np.concatenate([l[2] for l in leaves])
+    return lv, li, lj, distance, n0
+
+
+def multires_quadtree(seed: int = 2, width: float = 20000.0, duration: int = 7200) -> Workload:
+    """The multi-resolution configuration: 3-level 2:1 quadtree (20/10/5 m)
+    around a carved meandering channel (30 m wide, 3 m deep), fractal bed
+    (5 octaves, 20 m relief) plus a 0.0005 slope towards the east, 4 land
+    classes (channel n = 0.015 without infiltration; 0.035/0.05/0.08 with
+    Horton f0 = 60, fc = 10 mm/h, k = 4 /h), a translating Gaussian storm
+    (peak 80 mm/h, sigma 3 km, 5 m/s) in 200 m x 300 s raster bands and a
+    tidal east level boundary (1.5 m amplitude, 12.42 h period, 300 s knots)."""
+    base = 20.0
+    lv, li, lj, distance, n0 = meander_leaves(seed, width, base, buffer=500.0, half_channel=15.0)
+    rng = np.random.default_rng(seed + 1)
+    noise_n = 512
+    noise = fractal_noise((noise_n, noise_n), 5, rng)
+    classes_noise = fractal_noise((64, 64), 3, rng)
+
+    def sample(field, x, y):
+        k = field.shape[0]
+        ix = np.clip((x / width * k).astype(np.int64), 0, k - 1)
+        iy = np.clip((y / width * k).astype(np.int64), 0, k - 1)
+        return field[iy, ix]
+
+    def bed_at(x, y, level):
+        z = 20.0 * sample(noise, x, y) + 0.0005 * (width - x)
+        return (z - 3.0 * (distance(x, y) < 15.0)).astype(np.float32)
+
+    def land_at(x, y, level):
+        cls = 1 + np.minimum((sample(classes_noise, x, y) * 3).astype(np.int64), 2)
+        return np.where(distance(x, y) < 15.0, 0, cls).astype(np.uint8)
+
+    mesh = quadtree_mesh(lv, li, lj, base, 3, n0, n0, bed_at, land_at)
+    geometry = MeshGeometry.from_mesh(mesh)
+    # translating Gaussian storm, integrated per 300 s band on 200 m pixels
+    px = 200.0
+    npx = int(width / px)
+    starts = np.arange(0, duration, 300.0)
+    ends = starts + 300.0
+    cx = (np.arange(npx) + .5) * px
+    X, Y = np.meshgrid(cx, cx[::-1])
+    bands = np.zeros((len(starts), npx, npx))
+    for b, (a, e_) in enumerate(zip(starts, ends)):
+        t = 0.5 * (a + e_)
+        sx, sy = -4000.0 + 5.0 * t, width / 2
+        rate = 80.0 * np.exp(-((X - sx) ** 2 + (Y - sy) ** 2) / (2 * 3000.0 ** 2))   # mm/h
+        bands[b] = rate * (e_ - a) / 3600.0
+    raster = Raster(bands.astype(np.float32).astype(np.float64), from_origin(0, width, px, px), EPSG, None)
+    rain = RainField.from_raster(raster, geometry, starts, ends)
+    east = mesh.x[1:] > width - base
+    datum = float(np.percentile(mesh.z[1:][east], 10)) + 1.0
+    knots = np.arange(0, duration + 300, 300.0)
+    tide = datum + 1.5 * np.sin(2 * np.pi * knots / 44712.0)
+    lines = [np.array([[width, 0.0], [width, width]])]
+    claimed = np.zeros(mesh.e_num, bool)
+    boundary = select_boundary('tide', 'level', lines, TimeSeries(knots, tide), geometry, claimed)
+    forcing = Forcing.assemble([boundary], rain, duration)
+    horton = dict(f0_mm_h=60.0, fc_mm_h=10.0, k_per_h=4.0)
+    land_parameters = {0: LandParameters(manning_n=0.015, infiltration='none'),
+                       1: LandParameters(manning_n=0.035, infiltration=horton),
+                       2: LandParameters(manning_n=0.05, infiltration=horton),
+                       3: LandParameters(manning_n=0.08, infiltration=horton)}
+    return Workload('multires_quadtree', mesh, geometry, forcing, land_parameters, duration=duration,
+                    yield_step=300, rain_raster=raster,
+                    meta={'lines': {'tide': lines}, 'seed': seed,
+                          'cells_by_level': [int((mesh.level[1:] == k).sum()) for k in range(3)]})

@@ -119,3 +119,26 @@ def test_plain_uniform_256_full_run_bit_exact(tmp_path, cuda_available, path):
     for (_, pa), (_, pb) in zip(fa, fb):
         np.testing.assert_array_equal(read_depth_frame(pa).view(np.uint32), read_depth_frame(pb).view(np.uint32))
     assert row_a == row_b
+
+
+@pytest.mark.parametrize('path', PATHS)
+def test_multires_quadtree_bit_exact(tmp_path, cuda_available, path):
+    """2:1 quadtree (20/10/5 m) with hanging-edge pressure reconstruction,
+    Horton infiltration, moving rain and a tidal level boundary, started wet
+    so that water crosses the resolution interfaces from the first step."""
+    from nhflood.output import list_depth_frames, read_depth_frame
+    from nhflood.workloads import multires_quadtree, simulate
+    from runner import oracle_factory
+    w = multires_quadtree(width=2000.0, duration=600)
+    depth = np.where(w.mesh.land_type == 0, 1.5, 0.3).astype(np.float32)
+    depth[0] = 0.0
+    w.initial_depth = depth
+    assert w.step_arrays().hang_cells > 1000
+    row_a, rec_a = simulate(w, tmp_path / 'oracle', engine_factory=oracle_factory)
+    row_b, rec_b = simulate(w, tmp_path / 'cuda', engine_factory=cuda_engine(path))
+    np.testing.assert_array_equal(rec_a.trace, rec_b.trace)
+    assert rec_a.trace[:, 6].sum() >= 0 and rec_a.trace[:, 9].min() > 1000
+    for (_, pa), (_, pb) in zip(list_depth_frames(tmp_path / 'oracle' / 'output'),
+                                list_depth_frames(tmp_path / 'cuda' / 'output')):
+        np.testing.assert_array_equal(read_depth_frame(pa).view(np.uint32), read_depth_frame(pb).view(np.uint32))
+    assert row_a == row_b

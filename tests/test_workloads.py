@@ -1,0 +1,56 @@
+"""Synthetic workload generators: mesh consistency (every face side touches
+its cell with the right orientation, every side listed by exactly its
+cells), 2:1 balance, hanging interfaces, and the forcing they carry."""
+import numpy as np
+import pytest
+
+from nhflood.geometry import MeshGeometry
+from nhflood.workloads import dambreak, multires_quadtree, plain_uniform_256, uniform_grid
+
+
+def check_mesh(m):
+    topo = m.topology
+    listed = np.zeros(m.s_num, int)
+    for c in range(1, m.e_num):
+        for d in range(4):
+            p, n = m.face_ptr[c, d], m.counts[c, d]
+            assert n >= 1
+            for sid in m.isl_data[p:p + n]:
+                orient = 2 if d in (0, 1) else 1
+                assert topo[sid, 0] == orient
+                assert topo[sid, 2 if d in (0, 2) else 1] == c
+                listed[sid] += 1
+    expected = (topo[:, 1] != 0).astype(int) + (topo[:, 2] != 0)
+    np.testing.assert_array_equal(listed[1:], expected[1:])
+    MeshGeometry.from_mesh(m)  # square cells, exterior sides on faces
+
+
+def test_tile_major_uniform_grid_is_consistent():
+    check_mesh(uniform_grid(70, 45, 2.0, np.zeros((45, 70)), np.ones((45, 70), np.uint8), tile=32))
+
+
+def test_small_quadtree_is_balanced_and_has_hanging_interfaces():
+    w = multires_quadtree(width=2000.0, duration=600)
+    check_mesh(w.mesh)
+    levels = w.mesh.level[1:]
+    assert set(np.unique(levels)) == {0, 1, 2}
+    arrays = w.step_arrays()
+    assert arrays.hang_cells > 1000 and arrays.hang_edges > 1000
+    # every coarse face with two sides has half-length sides
+    two = w.mesh.counts[1:] == 2
+    assert two.any()
+    assert np.isclose(w.mesh.side_length[w.mesh.isl_data[w.mesh.face_ptr[1:][two]]], 0.0).sum() == 0
+
+
+def test_configs_have_the_stated_shape():
+    w = plain_uniform_256()
+    assert w.cells == 65536 and w.duration == 3600 and w.yield_step == 300
+    assert len(w.forcing.boundaries) == 1 and w.forcing.boundaries[0].kind == 'level'
+    assert len(w.forcing.boundaries[0].cells) == 256  # the south edge
+    assert w.forcing.boundaries[0].series.values[0] < w.mesh.z[1:].min() - 99
+    np.testing.assert_array_equal(w.forcing.rain.millimetres[:, 0], [25.0, 0.0])
+    d = dambreak(n=128, duration=60)
+    assert d.cells == 128 * 128
+    assert np.all(d.initial_depth[1:][d.mesh.x[1:] < 12.8] == 2.0)
+    assert np.all(d.initial_depth[1:][d.mesh.x[1:] >= 12.8] == 0.0)
+    assert len(d.forcing.boundaries[0].cells) == 4 * 128 - 4
