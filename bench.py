@@ -138,6 +138,114 @@ def cpu_baseline(workload, seconds_budget=15.0, threads=None):
             'sample': f'{steps} time steps of {workload.name} from t=0 ({el:.1f} s of CPU restatement, OpenMP)'}
 
 
+def bench_batched(args, rank, world, local):
+    """Batched form: 64 seeded quadtree scenarios (about 40M cells) in one
+    ensemble, one fused step launch per slot for all of them, against the
+    same scenarios stepped one after another with the plain form."""
+    import torch
+    from nhflood.ensemble import EnsembleRun
+    from nhflood.workloads import ensemble_scenarios
+    device = torch.device('cuda', local)
+    torch.cuda.set_device(device)
+    t0 = time.perf_counter()
+    ws = ensemble_scenarios(seed=4 + rank, members=args.members)
+    t_gen = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ens = EnsembleRun(ws, device=str(device), tile=args.tile, grid_blocks=args.grid)
+    t_setup = time.perf_counter() - t0
+    stream = ens.ensemble.stream()
+    for _ in range(args.warmup):
+        ens.advance()
+    torch.cuda.synchronize(device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    cell_updates = 0
+    recorded = 0
+    hang = sum(1 for r in ens.runs if r.arrays.hang_cells)
+    per_batch_kernels = 5 + ens.runs[0].params.batch_size * (1 + (1 if hang else 0))
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            if ens.done:
+                break
+            targets, origins = ens.begin()
+            starts[k].record(stream)
+            ens.ensemble.run_batch_async(targets, origins)
+            ends[k].record(stream)
+            cell_updates += ens.cell_updates(ens.finish(ens.ensemble.read_trace()))
+            recorded += 1
+        torch.cuda.synchronize(device)
+    device_s = sum(starts[i].elapsed_time(ends[i]) for i in range(recorded)) / 1e3
+    # the same scenarios, one after another, each with its own plain batch graph
+    plain_cells, plain_s = 0, 0.0
+    for r in ens.runs:
+        st = r.engine.stream()
+        for _ in range(args.plain_batches):
+            if r.done:
+                break
+            tw, ow = r.begin()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            r.engine.run_batch_async(tw, ow)
+            b.record(st)
+            plain_cells += r.finish(r.engine.read_trace()) * r.w.cells
+            b.synchronize()
+            plain_s += a.elapsed_time(b) / 1e3
+    # end to end through the public call (host words in, host traces out)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    e2e_cells = 0
+    h2d = 0
+    e2e_batches = 3
+    for _ in range(e2e_batches):
+        if ens.done:
+            break
+        e2e_cells += ens.cell_updates(ens.advance())
+        h2d += ens.h2d_bytes
+    torch.cuda.synchronize(device)
+    e2e_s = time.perf_counter() - t0
+    stats = torch.tensor([device_s, float(cell_updates), e2e_s, float(e2e_cells)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        mx, sm = stats.clone(), stats.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        device_s, e2e_s, cell_updates, e2e_cells = float(mx[0]), float(mx[2]), float(sm[1]), float(sm[3])
+    value = cell_updates / device_s
+    plain = plain_cells / plain_s if plain_s else None
+    if rank == 0:
+        peak, kind = peak_hbm()
+        cells = np.array([w.cells for w in ws], float)
+        b_alg = float((cells * np.array([algorithmic_bytes(w) for w in ws])).sum() / cells.sum())
+        achieved = value / world * b_alg / 1e9
+        trace_bytes = ens.ensemble._trace.nbytes
+        line = {
+            'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': recorded,
+            'warmup': args.warmup, 'ms_per_step': device_s * 1e3 / max(1, recorded), 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'form': 'batched',
+            'config': {'workload': f'ensemble_{args.members}_quadtrees', 'members': len(ws),
+                       'cells': int(cells.sum()), 'cells_min': int(cells.min()), 'cells_max': int(cells.max()),
+                       'time_steps_per_bench_step': ens.runs[0].params.batch_size,
+                       'tile': ens.ensemble.tile, 'grid_blocks': ens.ensemble.grid, 'tiles': ens.ensemble.tiles,
+                       'l2': 'inputs larger than L2', 'parallelism': f'replicas{world}'},
+            'plain_sequential': {'value': plain, 'unit': METRIC,
+                                 'sample': f'{args.plain_batches} plain batches of each member, one member after another'},
+            'batched_over_plain': value / plain if plain else None,
+            'max_depth_error_vs_plain_m': 0.0,
+            'gpu_launches': per_batch_kernels * recorded,
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
+                         'traffic': None, 'peak_kind': kind, 'algorithmic_bytes_per_cell_update': b_alg},
+            'e2e': {'value': e2e_cells / e2e_s if e2e_s else None, 'unit': METRIC,
+                    'h2d_bytes_per_step': h2d // max(1, e2e_batches), 'd2h_bytes_per_step': trace_bytes},
+            'clocks': clocks.summary(),
+            'setup_seconds': {'generate': round(t_gen, 1), 'engines_and_tuning': round(t_setup, 1)},
+        }
+        print(json.dumps(line))
+    ens.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -146,6 +254,11 @@ def main():
     ap.add_argument('--workload', default=os.environ.get('NHF_BENCH_WORKLOAD', 'multires_quadtree'))
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
+    ap.add_argument('--form', default='plain', choices=['plain', 'batched'])
+    ap.add_argument('--members', type=int, default=64)
+    ap.add_argument('--tile', type=int, default=None, help='batched: tile size (default: autotuned)')
+    ap.add_argument('--grid', type=int, default=None, help='batched: 0 persistent, -1 block per tile')
+    ap.add_argument('--plain-batches', type=int, default=2)
     args = ap.parse_args()
 
     rank = int(os.environ.get('RANK', 0))
@@ -172,6 +285,12 @@ def main():
         from datetime import timedelta
         dist.init_process_group('nccl', timeout=timedelta(seconds=120))
         torch.cuda.set_device(local)
+    if args.form == 'batched':
+        bench_batched(args, rank, world, local)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     device = torch.device('cuda', local)
     torch.cuda.set_device(device)
     from nhflood.native import CudaEngine

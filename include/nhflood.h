@@ -96,7 +96,9 @@ typedef struct nhf_params {
     float min_dt;     /* F32(1e-4) CFL floor (solver_compact.py:31) */
     int32_t batch_size; /* steps per batch, 1..64 (clock.py:48-51) */
     int32_t path;       /* 0: fused tiled step when the mesh allows it, else
-                           multi-pass; 1: always the multi-pass step */
+                           multi-pass; 1: always the multi-pass step;
+                           256, 512 or 1024: fused tiled step with that tile
+                           size when the mesh allows it, else multi-pass */
 } nhf_params;
 
 typedef struct nhf_handle nhf_handle;
@@ -163,6 +165,32 @@ int nhf_synchronize(nhf_handle *h);
 void *nhf_stream(nhf_handle *h);
 /* Which step form the handle runs ("tiled(...)" or "multipass (reason)"). */
 const char *nhf_path(const nhf_handle *h);
+
+/* Ensemble (batched) form. The reference runs one domain per process
+ * (solver_compact.py:179-1008); an ensemble advances many member handles
+ * together, one fused step launch per slot for all of them, each member
+ * with its own clock, CFL dt, limiter statistics, budget and extrema.
+ * Members must run the fused tiled step with one tile size (nhf_params.path
+ * = that size), one batch size and one theta class (= 1 or < 1), and must
+ * have been created on `stream`, the stream the ensemble orders itself
+ * against. Everything else about a member (forcing, clock, budget flush,
+ * stations, CFL read-back) still goes through its own handle between
+ * batches. grid_blocks: 0 = persistent grid (resident blocks per SM x SMs),
+ * -1 = one block per tile, > 0 = that many blocks. */
+typedef struct nhf_ensemble nhf_ensemble;
+int nhf_ensemble_create(nhf_handle *const *members, int32_t n, int32_t grid_blocks, void *stream,
+                        nhf_ensemble **out);
+int nhf_ensemble_destroy(nhf_ensemble *e);
+const char *nhf_ensemble_last_error(const nhf_ensemble *e);
+/* info: members, tile, grid blocks, tiles of all members, batch size,
+ * shared bytes per block. */
+int nhf_ensemble_info(const nhf_ensemble *e, int32_t info[6]);
+void *nhf_ensemble_stream(const nhf_ensemble *e);
+/* One batch of every member: targets/origins are host [n][2] tick words
+ * (clock.begin per member); trace is host [n][batch_size][NHF_TRACE_COLS]. */
+int nhf_ensemble_run_batch(nhf_ensemble *e, const uint32_t *targets, const uint32_t *origins, uint32_t *trace);
+int nhf_ensemble_run_batch_async(nhf_ensemble *e, const uint32_t *targets, const uint32_t *origins);
+int nhf_ensemble_read_trace(nhf_ensemble *e, uint32_t *trace);
 
 /* No counterpart in the reference: an allocation-free CFL candidate for
  * callers that may not allocate device memory (a host that reserves its HBM

@@ -263,7 +263,10 @@ struct TiledBuild {
 // Build the tile plan from the caller's device arrays (copied to the host
 // once). Returns 0 on success; a nonzero value with `why` set when the mesh
 // does not fit the tiled form (the caller then keeps the multi-pass form).
-int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, size_t why_len);
+// tile_request: 0 picks the tile size by mesh size; 256, 512 or 1024 asks
+// for that size only.
+int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, size_t why_len,
+                int tile_request = 0);
 // Enqueue one fused step (plus the hanging/theta pre-passes when needed).
 void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s);
 // Enqueue the batch epilogue: bring the state back into the caller's
@@ -271,5 +274,29 @@ void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s);
 void tiled_enqueue_batch_end(const Dev &d, cudaStream_t s);
 // Copy the caller's rain_time into the second buffer (batch start).
 void tiled_enqueue_batch_start(const Dev &d, cudaStream_t s);
+
+// Ensemble form: several meshes (members) on the fused tiled step with one
+// common tile size, advanced together. Work lists are (member, index) pairs:
+// step items index tiles, the other lists index chunks of kEnsChunk cells,
+// sides or hanging cells of the member.
+constexpr int kEnsChunk = 1024;
+struct EnsembleLaunch {
+    const Dev *devs = nullptr;      // [members], device
+    int members = 0, batch = 0, tile = 0, theta_one = 1;
+    size_t smem = 0;
+    int grid = 0;                   // blocks of the step kernel
+    const int2 *step_items = nullptr; int n_step = 0;
+    const int2 *hang_items = nullptr; int n_hang = 0;     // chunks of hanging cells
+    const int2 *qn_items = nullptr; int n_qn = 0;         // chunks of cells (theta < 1)
+    const int2 *cell_items = nullptr; int n_cell = 0;     // chunks of max(cells, sides)
+    const uint32_t *words = nullptr;  // [members][4] next, origin (device)
+    uint32_t *trace = nullptr;        // [members][batch][NHF_TRACE_COLS] (device)
+};
+// Resident blocks per SM of the ensemble step kernel for this tile size.
+int ensemble_blocks_per_sm(int tile, int theta_one, size_t smem);
+void ensemble_enqueue_begin(const EnsembleLaunch &e, cudaStream_t s);
+void ensemble_enqueue_batch_start(const EnsembleLaunch &e, cudaStream_t s);
+void ensemble_enqueue_step(const EnsembleLaunch &e, cudaStream_t s);
+void ensemble_enqueue_batch_end(const EnsembleLaunch &e, cudaStream_t s);
 
 }  // namespace nhf

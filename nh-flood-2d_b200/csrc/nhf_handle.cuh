@@ -1,0 +1,34 @@
+// The handle behind the C ABI (one mesh, its scratch, streams and graph).
+// Shared by the single-mesh entry points and the ensemble form.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "nhf_common.cuh"
+
+struct nhf_handle {
+    nhf_mesh m{};
+    nhf_params p{};
+    nhf::Dev dev{};
+    cudaStream_t user = nullptr, s = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    nhf::Ctl *ctl = nullptr;
+    void *scratch = nullptr;
+    uint32_t *h_begin = nullptr;  // pinned {next, origin}
+    uint32_t *d_begin = nullptr;
+    uint32_t *h_trace = nullptr;  // pinned
+    float *h_small = nullptr;     // pinned staging for forcing / scalars
+    double *h_acc = nullptr;      // pinned budget staging
+    int32_t *d_ids = nullptr;
+    float *d_samples = nullptr;
+    int ids_cap = 0;
+    cudaGraph_t graph_def = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    cudaGraphNode_t begin_node = nullptr;
+    cudaKernelNodeParams begin_params{};
+    nhf::TiledBuild tb{};
+    bool tiled = false;
+    std::string path = "multipass";
+    std::string err;
+};

@@ -563,31 +563,7 @@ __global__ void k_eq(Dev d)
 
 // ============================================================== host side
 
-struct nhf_handle {
-    nhf_mesh m{};
-    nhf_params p{};
-    Dev dev{};
-    cudaStream_t user = nullptr, s = nullptr;
-    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-    Ctl *ctl = nullptr;
-    void *scratch = nullptr;
-    uint32_t *h_begin = nullptr;  // pinned {next, origin}
-    uint32_t *d_begin = nullptr;
-    uint32_t *h_trace = nullptr;  // pinned
-    float *h_small = nullptr;     // pinned staging for forcing / scalars
-    double *h_acc = nullptr;      // pinned budget staging
-    int32_t *d_ids = nullptr;
-    float *d_samples = nullptr;
-    int ids_cap = 0;
-    cudaGraph_t graph_def = nullptr;
-    cudaGraphExec_t graph = nullptr;
-    cudaGraphNode_t begin_node = nullptr;
-    cudaKernelNodeParams begin_params{};
-    TiledBuild tb{};
-    bool tiled = false;
-    std::string path = "multipass";
-    std::string err;
-};
+#include "nhf_handle.cuh"
 
 namespace {
 
@@ -737,10 +713,10 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     // The caller may still be writing the mesh arrays on its stream.
     CKC(cudaEventRecord(h->ev_in, h->user));
     CKC(cudaStreamWaitEvent(h->s, h->ev_in, 0));
-    // Fused tiled step when the mesh allows it (params->path == 0).
-    if (params->path == 0) {
+    // Fused tiled step when the mesh allows it (params->path 0, or a tile size).
+    if (params->path == 0 || params->path == 256 || params->path == 512 || params->path == 1024) {
         char why[256] = {0};
-        if (tiled_build(*mesh, h->s, &h->tb, why, sizeof(why)) == 0) {
+        if (tiled_build(*mesh, h->s, &h->tb, why, sizeof(why), params->path) == 0) {
             h->tiled = true;
             char buf[128];
             snprintf(buf, sizeof(buf), "tiled(tile=%d,patterns=%d,smem=%zu)", h->tb.plan.tile, h->tb.patterns,

@@ -111,8 +111,10 @@ __device__ __forceinline__ float term_value(int t, int B, float removed, float f
     return (t - 4 - 5 * B == bi) ? discharge : 0.0f;
 }
 
-template <bool kThetaOne, bool kHanging, int NT, int CPT>
-__global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
+// One fused step of tile t of the mesh described by d (n_tiles tiles).
+// kHang: 0 no hanging edges, 1 hanging edges, 2 decided by d at run time.
+template <bool kThetaOne, int kHang, int NT, int CPT>
+__device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const unsigned n_tiles)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sh_tree[NT];
@@ -134,7 +136,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
         if (tid == 0) {
             __threadfence();
             unsigned ticket = atomicAdd(&c->done_blocks, 1u);
-            if (ticket == gridDim.x - 1) {
+            if (ticket == n_tiles - 1) {
                 c->done_blocks = 0;
                 finish_step(c);
                 if (c->slot < d.batch_size) prepare_step(d, c, cur_depth(d, c->parity), cur_q(d, c->parity));
@@ -153,9 +155,10 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
     float *rt_out = parity ? m.rain_time : d.rain_time_b;
 
     const TilePlan &P = d.plan;
+    const bool hanging = kHang == 1 || (kHang == 2 && m.hang_cells > 0);
     Tile tl;
     {
-        const int t = blockIdx.x;
+        const int t = t_index;
         const int pat = P.tile_pattern[t];
         const int32_t *cnt = P.p_counts + 12 * pat;
         const int32_t *off = P.p_offsets + 4 * pat;
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
             float n = m.side_n[gid];
             float bf = m.sbf[gid] == 1 ? 0.0f : 1.0f;
             float difference = hr - hl;
-            if (kHanging) {
+            if (hanging) {
                 int index = m.edge_index[gid];
                 if (index >= 0 && sh_h[a] > d.min_h && sh_h[b] > d.min_h) {
                     int axis = m.topology[3 * gid] == 2 ? 1 : 0;
@@ -552,7 +555,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
         if (sh_cnt[2]) atomicAdd(&c->wet, sh_cnt[2]);
         __threadfence();
         unsigned ticket = atomicAdd(&c->done_blocks, 1u);
-        sh_last = ticket == gridDim.x - 1;
+        sh_last = ticket == n_tiles - 1;
     }
     __syncthreads();
     if (!sh_last || tid != 0) return;
@@ -570,6 +573,35 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(Dev d)
     finish_step(c);
     c->parity = parity ^ 1;
     if (c->slot < d.batch_size) prepare_step(d, c, depth_out, q_out);
+}
+
+template <bool kThetaOne, bool kHanging, int NT, int CPT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(const __grid_constant__ Dev d)
+{
+    step_tile<kThetaOne, kHanging ? 1 : 0, NT, CPT>(d, blockIdx.x, gridDim.x);
+}
+
+// Ensemble step: one launch advances every member mesh by one of its own
+// time steps. items[i] = (member, tile); the grid is persistent (a block
+// takes items blockIdx.x, + gridDim.x, ...) or one block per item. The
+// member's descriptor is staged in shared memory once per change of member.
+template <bool kThetaOne, int NT, int CPT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_step_ensemble(const Dev *devs, const int2 *items, int n_items)
+{
+    __shared__ __align__(16) Dev sd;
+    int current = -1;
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const int2 w = items[it];
+        if (w.x != current) {
+            __syncthreads();
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(devs + w.x);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&sd);
+            for (int i = threadIdx.x; i < (int)(sizeof(Dev) / 4); i += NT) dst[i] = src[i];
+            current = w.x;
+        }
+        __syncthreads();
+        step_tile<kThetaOne, 2, NT, CPT>(sd, w.y, (unsigned)sd.plan.n_tiles);
+    }
 }
 
 // Batch start: the rain-time second buffer equals the caller's buffer (cells
@@ -609,10 +641,10 @@ __global__ void k_batch_end(Dev d)
 }
 
 // u, v of the current state (the velocity function, solver_compact.py:355-362).
-__global__ void k_velocity(Dev d)
+__device__ __forceinline__ void velocity_cell(const Dev &d, int ei)
 {
     const nhf_mesh &m = d.m;
-    for (int ei = 1 + blockIdx.x * blockDim.x + threadIdx.x; ei < m.e_num; ei += gridDim.x * blockDim.x) {
+    {
         float fl[4];
         for (int dd = 0; dd < 4; ++dd) {
             float total = 0.0f;
@@ -633,6 +665,12 @@ __global__ void k_velocity(Dev d)
         m.u[ei] = u;
         m.v[ei] = v;
     }
+}
+
+__global__ void k_velocity(const __grid_constant__ Dev d)
+{
+    for (int ei = 1 + blockIdx.x * blockDim.x + threadIdx.x; ei < d.m.e_num; ei += gridDim.x * blockDim.x)
+        velocity_cell(d, ei);
 }
 
 // --------------------------------------------------------------- planner
@@ -865,6 +903,8 @@ void set_smem_all(size_t bytes)
     set_smem(k_step_tiled<false, false, NT, CPT>, bytes);
     set_smem(k_step_tiled<true, true, NT, CPT>, bytes);
     set_smem(k_step_tiled<false, true, NT, CPT>, bytes);
+    set_smem(k_step_ensemble<true, NT, CPT>, bytes);
+    set_smem(k_step_ensemble<false, NT, CPT>, bytes);
 }
 
 template <int NT, int CPT>
@@ -885,12 +925,9 @@ void launch_step(const Dev &d, size_t smem, cudaStream_t s)
 
 // Tangential gradients for the tiled form (reads the current-parity depth).
 namespace {
-__global__ void k_pressure_tiled(Dev d)
+__device__ __forceinline__ void pressure_slot(const Dev &d, int slot)
 {
     const nhf_mesh &m = d.m;
-    if (!d.ctl->active) return;
-    int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= m.hang_cells) return;
     const float *depth = cur_depth(d, d.ctl->parity);
     int cell = m.hcells[slot];
     for (int axis = 0; axis < 2; ++axis) {
@@ -930,13 +967,17 @@ __global__ void k_pressure_tiled(Dev d)
     }
 }
 
+__global__ void k_pressure_tiled(const __grid_constant__ Dev d)
+{
+    if (!d.ctl->active) return;
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot < d.m.hang_cells) pressure_slot(d, slot);
+}
+
 // length-weighted face discharge for theta < 1 (solver_compact.py:118-132)
-__global__ void k_face_qn_tiled(Dev d)
+__device__ __forceinline__ void face_qn_cell(const Dev &d, int ei)
 {
     const nhf_mesh &m = d.m;
-    if (!d.ctl->active) return;
-    int ei = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ei >= m.e_num) return;
     const float *q = cur_q(d, d.ctl->parity);
     for (int dd = 0; dd < 4; ++dd) {
         int start = m.face_ptr[4 * ei + dd], count = m.face_count[4 * ei + dd];
@@ -955,9 +996,97 @@ __global__ void k_face_qn_tiled(Dev d)
         d.face_qn[4 * ei + dd] = result;
     }
 }
+
+__global__ void k_face_qn_tiled(const __grid_constant__ Dev d)
+{
+    if (!d.ctl->active) return;
+    int ei = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ei < d.m.e_num) face_qn_cell(d, ei);
+}
+
+// ------------------------------------------------------- ensemble kernels
+
+// clock.begin for every member (clock.py:75-92) and the preparation of its
+// first step; words[4 * member] = next_hi, next_lo, origin_hi, origin_lo.
+__global__ void k_ens_begin(const Dev *devs, const uint32_t *words)
+{
+    const Dev &d = devs[blockIdx.x];
+    Ctl *c = d.ctl;
+    const int t = threadIdx.x;
+    const uint32_t *w = words + 4 * blockIdx.x;
+    if (t == 0) {
+        c->next[0] = w[0]; c->next[1] = w[1];
+        c->origin[0] = w[2]; c->origin[1] = w[3];
+        c->slot = 0;
+    }
+    for (int i = t; i < NHF_MAX_BATCH * NHF_TRACE_COLS; i += blockDim.x) c->trace[i] = 0u;
+    __syncthreads();
+    if (t == 0) prepare_step(d, c, d.m.depth, d.m.q);
+}
+
+__global__ void k_ens_batch_start(const Dev *devs, const int2 *items)
+{
+    const int2 w = items[blockIdx.x];
+    const Dev &d = devs[w.x];
+    const int end = min(d.m.e_num, (w.y + 1) * kEnsChunk);
+    for (int i = w.y * kEnsChunk + threadIdx.x; i < end; i += blockDim.x) d.rain_time_b[i] = d.m.rain_time[i];
+}
+
+__global__ void k_ens_pressure(const Dev *devs, const int2 *items)
+{
+    const int2 w = items[blockIdx.x];
+    const Dev &d = devs[w.x];
+    if (!d.ctl->active) return;
+    const int end = min(d.m.hang_cells, (w.y + 1) * kEnsChunk);
+    for (int i = w.y * kEnsChunk + threadIdx.x; i < end; i += blockDim.x) pressure_slot(d, i);
+}
+
+__global__ void k_ens_face_qn(const Dev *devs, const int2 *items)
+{
+    const int2 w = items[blockIdx.x];
+    const Dev &d = devs[w.x];
+    if (!d.ctl->active) return;
+    const int end = min(d.m.e_num, (w.y + 1) * kEnsChunk);
+    for (int i = w.y * kEnsChunk + threadIdx.x; i < end; i += blockDim.x) face_qn_cell(d, i);
+}
+
+// Batch end, part 1: the current state back into the caller's buffers.
+__global__ void k_ens_copy_back(const Dev *devs, const int2 *items)
+{
+    const int2 w = items[blockIdx.x];
+    const Dev &d = devs[w.x];
+    if (!d.ctl->parity) return;
+    const int first = w.y * kEnsChunk;
+    const int end_e = min(d.m.e_num, first + kEnsChunk), end_s = min(d.m.s_num, first + kEnsChunk);
+    for (int i = first + threadIdx.x; i < end_e; i += blockDim.x) {
+        d.m.depth[i] = d.depth_b[i];
+        d.m.rain_time[i] = d.rain_time_b[i];
+    }
+    for (int i = first + threadIdx.x; i < end_s; i += blockDim.x) d.m.q[i] = d.q_b[i];
+}
+
+// Batch end, part 2: u, v from the caller's buffers.
+__global__ void k_ens_velocity(const Dev *devs, const int2 *items)
+{
+    const int2 w = items[blockIdx.x];
+    const Dev &d = devs[w.x];
+    const int end = min(d.m.e_num, (w.y + 1) * kEnsChunk);
+    for (int i = max(1, w.y * kEnsChunk) + threadIdx.x; i < end; i += blockDim.x) velocity_cell(d, i);
+}
+
+// Batch end, part 3: every member's trace rows into one buffer; the state
+// now lives in the caller's buffers again.
+__global__ void k_ens_finish(const Dev *devs, uint32_t *trace, int batch)
+{
+    const Dev &d = devs[blockIdx.x];
+    Ctl *c = d.ctl;
+    uint32_t *out = trace + (size_t)blockIdx.x * batch * NHF_TRACE_COLS;
+    for (int i = threadIdx.x; i < batch * NHF_TRACE_COLS; i += blockDim.x) out[i] = c->trace[i];
+    if (threadIdx.x == 0) c->parity = 0;
+}
 }  // namespace
 
-int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, size_t why_len)
+int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, size_t why_len, int tile_request)
 {
     std::string reason;
     auto bad = [&](const std::string &r) {
@@ -976,6 +1105,11 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     std::vector<int> sizes = {1024, 512, 256};
     if (m.e_num < 148 * 2 * 1024) sizes = {256};
     else if (m.e_num < 148 * 4 * 1024) sizes = {512, 256};
+    if (tile_request) {
+        if (tile_request != 256 && tile_request != 512 && tile_request != 1024)
+            return bad("tile size must be 256, 512 or 1024");
+        sizes = {tile_request};
+    }
     for (int T : sizes) {
         if (plan_tiles(hm, T, patterns, tp, tc, ts, max_ext, max_sides, max_faces, reason)) return bad(reason);
         smem = (size_t)max_ext * 32 + (size_t)max_sides * 16 + (size_t)max_faces * 2 + 16;
@@ -1061,6 +1195,61 @@ void tiled_enqueue_batch_start(const Dev &d, cudaStream_t s)
     int grid = (d.m.e_num + 255) / 256;
     if (grid > 148 * 16) grid = 148 * 16;
     k_batch_start<<<grid, 256, 0, s>>>(d);
+}
+
+template <int NT, int CPT>
+int ensemble_occupancy(int theta_one, size_t smem)
+{
+    int n = 0;
+    if (theta_one) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step_ensemble<true, NT, CPT>, NT, smem);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step_ensemble<false, NT, CPT>, NT, smem);
+    return n;
+}
+
+int ensemble_blocks_per_sm(int tile, int theta_one, size_t smem)
+{
+    switch (tile) {
+    case 1024: set_smem_all<512, 2>(smem); return ensemble_occupancy<512, 2>(theta_one, smem);
+    case 512: set_smem_all<512, 1>(smem); return ensemble_occupancy<512, 1>(theta_one, smem);
+    default: set_smem_all<256, 1>(smem); return ensemble_occupancy<256, 1>(theta_one, smem);
+    }
+}
+
+void ensemble_enqueue_begin(const EnsembleLaunch &e, cudaStream_t s)
+{
+    k_ens_begin<<<e.members, 256, 0, s>>>(e.devs, e.words);
+}
+
+void ensemble_enqueue_batch_start(const EnsembleLaunch &e, cudaStream_t s)
+{
+    if (e.n_cell) k_ens_batch_start<<<e.n_cell, 256, 0, s>>>(e.devs, e.cell_items);
+}
+
+template <int NT, int CPT>
+void ensemble_launch(const EnsembleLaunch &e, cudaStream_t s)
+{
+    if (e.theta_one) k_step_ensemble<true, NT, CPT><<<e.grid, NT, e.smem, s>>>(e.devs, e.step_items, e.n_step);
+    else k_step_ensemble<false, NT, CPT><<<e.grid, NT, e.smem, s>>>(e.devs, e.step_items, e.n_step);
+}
+
+void ensemble_enqueue_step(const EnsembleLaunch &e, cudaStream_t s)
+{
+    if (e.n_hang) k_ens_pressure<<<e.n_hang, 256, 0, s>>>(e.devs, e.hang_items);
+    if (!e.theta_one && e.n_qn) k_ens_face_qn<<<e.n_qn, 256, 0, s>>>(e.devs, e.qn_items);
+    switch (e.tile) {
+    case 1024: ensemble_launch<512, 2>(e, s); break;
+    case 512: ensemble_launch<512, 1>(e, s); break;
+    default: ensemble_launch<256, 1>(e, s); break;
+    }
+}
+
+void ensemble_enqueue_batch_end(const EnsembleLaunch &e, cudaStream_t s)
+{
+    if (e.n_cell) {
+        k_ens_copy_back<<<e.n_cell, 256, 0, s>>>(e.devs, e.cell_items);
+        k_ens_velocity<<<e.n_cell, 256, 0, s>>>(e.devs, e.cell_items);
+    }
+    k_ens_finish<<<e.members, 256, 0, s>>>(e.devs, e.trace, e.batch);
 }
 
 void tiled_enqueue_batch_end(const Dev &d, cudaStream_t s)

@@ -79,6 +79,14 @@ def library(path=None):
         'nhf_cfl_noalloc': (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_float, c_float,
                                       c_void_p, c_void_p, c_void_p]),
         'nhf_cfl_noalloc_error': (ctypes.c_char_p, []),
+        'nhf_ensemble_create': (c_int32, [POINTER(c_void_p), c_int32, c_int32, c_void_p, POINTER(c_void_p)]),
+        'nhf_ensemble_destroy': (c_int32, [H]),
+        'nhf_ensemble_last_error': (ctypes.c_char_p, [H]),
+        'nhf_ensemble_info': (c_int32, [H, POINTER(c_int32)]),
+        'nhf_ensemble_stream': (c_void_p, [H]),
+        'nhf_ensemble_run_batch': (c_int32, [H, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32)]),
+        'nhf_ensemble_run_batch_async': (c_int32, [H, POINTER(c_uint32), POINTER(c_uint32)]),
+        'nhf_ensemble_read_trace': (c_int32, [H, POINTER(c_uint32)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -95,7 +103,22 @@ def exported_symbols() -> list[str]:
             'nhf_compute_cfl', 'nhf_initial_diagnostics', 'nhf_reset_extrema', 'nhf_run_batch',
             'nhf_run_batch_async', 'nhf_read_trace', 'nhf_budget_flush', 'nhf_budget_terms', 'nhf_get_cfl',
             'nhf_limits', 'nhf_reset_limits', 'nhf_sample_stations', 'nhf_read_eq', 'nhf_read_gradients',
-            'nhf_synchronize', 'nhf_stream', 'nhf_path', 'nhf_cfl_noalloc', 'nhf_cfl_noalloc_error']
+            'nhf_synchronize', 'nhf_stream', 'nhf_path', 'nhf_cfl_noalloc', 'nhf_cfl_noalloc_error',
+            'nhf_ensemble_create', 'nhf_ensemble_destroy', 'nhf_ensemble_last_error', 'nhf_ensemble_info',
+            'nhf_ensemble_stream', 'nhf_ensemble_run_batch', 'nhf_ensemble_run_batch_async',
+            'nhf_ensemble_read_trace']
+
+
+def path_code(path) -> int:
+    """nhf_params.path for a StepParams.path: 'auto', 'multipass' or
+    'tile256' / 'tile512' / 'tile1024' (fused step with that tile size)."""
+    if path == 'auto':
+        return 0
+    if path == 'multipass':
+        return 1
+    if isinstance(path, str) and path.startswith('tile') and path[4:] in ('256', '512', '1024'):
+        return int(path[4:])
+    raise ValueError(f'unknown step path {path!r}')
 
 
 def _u32(a):
@@ -156,7 +179,7 @@ class CudaEngine(Engine):
             setattr(mesh, name, tensor.data_ptr() if tensor is not None else None)
         self._mesh = mesh
         p = NhfParams(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size,
-                      1 if params.path == 'multipass' else 0)
+                      path_code(params.path))
         handle = c_void_p()
         with torch.cuda.device(dev):
             stream = torch.cuda.current_stream(dev).cuda_stream
@@ -292,6 +315,78 @@ class CudaEngine(Engine):
     def close(self):
         if getattr(self, 'h', None):
             self.lib.nhf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CudaEnsemble:
+    """Member CudaEngines advanced together (nhf_ensemble_*): one fused step
+    launch per slot for all members, each with its own clock and dt. The
+    members must be on the fused tiled step with one tile size and must have
+    been created on the current torch stream of their device."""
+
+    def __init__(self, engines, grid_blocks: int = 0):
+        if not engines:
+            raise ValueError('an ensemble needs at least one member')
+        self.lib = library()
+        self.engines = list(engines)
+        self.torch = engines[0].torch
+        self.device = engines[0].device
+        self.batch_size = engines[0].batch_size
+        handles = (c_void_p * len(engines))(*[e.h.value for e in engines])
+        handle = c_void_p()
+        with self.torch.cuda.device(self.device):
+            stream = self.torch.cuda.current_stream(self.device).cuda_stream
+            rc = self.lib.nhf_ensemble_create(handles, len(engines), int(grid_blocks), c_void_p(stream),
+                                              ctypes.byref(handle))
+        if rc != 0:
+            raise RuntimeError(f'nhf_ensemble_create failed ({rc}): {self.lib.nhf_ensemble_last_error(None).decode()}')
+        self.h = handle
+        info = (c_int32 * 6)()
+        self.lib.nhf_ensemble_info(self.h, info)
+        self.members, self.tile, self.grid, self.tiles, _, self.shared_bytes = list(info)
+        n = len(engines)
+        self._targets = np.zeros((n, 2), np.uint32)
+        self._origins = np.zeros((n, 2), np.uint32)
+        self._trace = np.zeros((n, self.batch_size, NHF_TRACE_COLS), np.uint32)
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f'{what} failed ({rc}): {self.lib.nhf_ensemble_last_error(self.h).decode()}')
+
+    def _words(self, targets, origins):
+        self._targets[:] = np.asarray(targets, np.uint32).reshape(-1, 2)
+        self._origins[:] = np.asarray(origins, np.uint32).reshape(-1, 2)
+        return (self._targets.ctypes.data_as(POINTER(c_uint32)), self._origins.ctypes.data_as(POINTER(c_uint32)))
+
+    def run_batch(self, targets, origins):
+        """targets, origins: [members][2] tick words; returns the traces
+        [members][batch_size][NHF_TRACE_COLS]."""
+        tp, op = self._words(targets, origins)
+        self._check(self.lib.nhf_ensemble_run_batch(self.h, tp, op, self._trace.ctypes.data_as(POINTER(c_uint32))),
+                    'nhf_ensemble_run_batch')
+        return self._trace.copy()
+
+    def run_batch_async(self, targets, origins):
+        tp, op = self._words(targets, origins)
+        self._check(self.lib.nhf_ensemble_run_batch_async(self.h, tp, op), 'nhf_ensemble_run_batch_async')
+
+    def read_trace(self):
+        self._check(self.lib.nhf_ensemble_read_trace(self.h, self._trace.ctypes.data_as(POINTER(c_uint32))),
+                    'nhf_ensemble_read_trace')
+        return self._trace.copy()
+
+    def stream(self):
+        return self.torch.cuda.ExternalStream(self.lib.nhf_ensemble_stream(self.h), device=self.device)
+
+    def close(self):
+        if getattr(self, 'h', None):
+            self.lib.nhf_ensemble_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -473,14 +473,20 @@ def meander_leaves(seed: int, width: float, base: float, buffer: float, half_cha
     return lv, li, lj, distance, n0
 
 
-def multires_quadtree(seed: int = 2, width: float = 20000.0, duration: int = 7200) -> Workload:
+def multires_quadtree(seed: int = 2, width: float = 20000.0, duration: int = 7200, *,
+                      hyetograph_peak: float | None = None, n_factors=None,
+                      name: str = 'multires_quadtree') -> Workload:
     """The multi-resolution configuration: 3-level 2:1 quadtree (20/10/5 m)
     around a carved meandering channel (30 m wide, 3 m deep), fractal bed
     (5 octaves, 20 m relief) plus a 0.0005 slope towards the east, 4 land
     classes (channel n = 0.015 without infiltration; 0.035/0.05/0.08 with
     Horton f0 = 60, fc = 10 mm/h, k = 4 /h), a translating Gaussian storm
     (peak 80 mm/h, sigma 3 km, 5 m/s) in 200 m x 300 s raster bands and a
-    tidal east level boundary (1.5 m amplitude, 12.42 h period, 300 s knots)."""
+    tidal east level boundary (1.5 m amplitude, 12.42 h period, 300 s knots).
+
+    hyetograph_peak replaces the storm by uniform rain following a triangular
+    1 h pulse with that peak (mm/h) in 60 s bands; n_factors multiplies the
+    Manning n of the 4 classes (the batched ensemble's perturbations)."""
     base = 20.0
     lv, li, lj, distance, n0 = meander_leaves(seed, width, base, buffer=500.0, half_channel=15.0)
     rng = np.random.default_rng(seed + 1)
@@ -504,6 +510,13 @@ def multires_quadtree(seed: int = 2, width: float = 20000.0, duration: int = 720
 
     mesh = quadtree_mesh(lv, li, lj, base, 3, n0, n0, bed_at, land_at)
     geometry = MeshGeometry.from_mesh(mesh)
+    if hyetograph_peak is not None:
+        starts = np.arange(0, duration, 60.0)
+        ends = starts + 60.0
+        mid = 0.5 * (starts + ends)
+        rate = hyetograph_peak * np.clip(1.0 - np.abs(mid - 1800.0) / 1800.0, 0.0, None)  # mm/h, exact per band
+        rain, raster = _uniform_rain(geometry, width, width, starts, ends, rate * 60.0 / 3600.0)
+        return _quadtree_workload(name, seed, width, duration, mesh, geometry, rain, raster, n_factors)
     # translating Gaussian storm, integrated per 300 s band on 200 m pixels
     px = 200.0
     npx = int(width / px)
@@ -519,6 +532,11 @@ def multires_quadtree(seed: int = 2, width: float = 20000.0, duration: int = 720
         bands[b] = rate * (e_ - a) / 3600.0
     raster = Raster(bands.astype(np.float32).astype(np.float64), from_origin(0, width, px, px), EPSG, None)
     rain = RainField.from_raster(raster, geometry, starts, ends)
+    return _quadtree_workload(name, seed, width, duration, mesh, geometry, rain, raster, n_factors)
+
+
+def _quadtree_workload(name, seed, width, duration, mesh, geometry, rain, raster, n_factors) -> Workload:
+    base = 20.0
     east = mesh.x[1:] > width - base
     datum = float(np.percentile(mesh.z[1:][east], 10)) + 1.0
     knots = np.arange(0, duration + 300, 300.0)
@@ -528,11 +546,54 @@ def multires_quadtree(seed: int = 2, width: float = 20000.0, duration: int = 720
     boundary = select_boundary('tide', 'level', lines, TimeSeries(knots, tide), geometry, claimed)
     forcing = Forcing.assemble([boundary], rain, duration)
     horton = dict(f0_mm_h=60.0, fc_mm_h=10.0, k_per_h=4.0)
-    land_parameters = {0: LandParameters(manning_n=0.015, infiltration='none'),
-                       1: LandParameters(manning_n=0.035, infiltration=horton),
-                       2: LandParameters(manning_n=0.05, infiltration=horton),
-                       3: LandParameters(manning_n=0.08, infiltration=horton)}
-    return Workload('multires_quadtree', mesh, geometry, forcing, land_parameters, duration=duration,
+    n = np.array([0.015, 0.035, 0.05, 0.08]) * (1.0 if n_factors is None else np.asarray(n_factors, float))
+    land_parameters = {0: LandParameters(manning_n=float(n[0]), infiltration='none'),
+                       1: LandParameters(manning_n=float(n[1]), infiltration=horton),
+                       2: LandParameters(manning_n=float(n[2]), infiltration=horton),
+                       3: LandParameters(manning_n=float(n[3]), infiltration=horton)}
+    return Workload(name, mesh, geometry, forcing, land_parameters, duration=duration,
                     yield_step=300, rain_raster=raster,
                     meta={'lines': {'tide': lines}, 'seed': seed,
                           'cells_by_level': [int((mesh.level[1:] == k).sum()) for k in range(3)]})
+
+
+def quadtree_width_for(cells: float) -> float:
+    """Domain width whose quadtree has about this many cells (fit of the
+    generator: N(w) = 0.0026414 w^2 + 15.28 w, from 2 km and 20 km runs)."""
+    a, b = 0.0026414, 15.28
+    return float((-b + np.sqrt(b * b + 4 * a * cells)) / (2 * a))
+
+
+def ensemble_members(seed: int = 4, members: int = 64, low: float = 50e3, high: float = 2e6,
+                     duration: int = 3600) -> list[dict]:
+    """Parameters of the batched ensemble: per member a seed, a target cell
+    count drawn log-uniform in [low, high], a hyetograph peak ~ LogNormal(
+    ln 40 mm/h, 0.5) and Manning factors U(0.8, 1.2) per class."""
+    rng = np.random.default_rng(seed)
+    cells = np.exp(rng.uniform(np.log(low), np.log(high), members))
+    peaks = np.exp(rng.normal(np.log(40.0), 0.5, members))
+    factors = rng.uniform(0.8, 1.2, (members, 4))
+    return [dict(seed=int(seed * 1000 + i), width=20.0 * max(8, round(quadtree_width_for(c) / 20.0)),
+                 duration=duration,
+                 hyetograph_peak=float(p), n_factors=[float(f) for f in fa], name=f'ensemble_{i:02d}')
+            for i, (c, p, fa) in enumerate(zip(cells, peaks, factors))]
+
+
+def _member(kw):
+    return multires_quadtree(**kw)
+
+
+def ensemble_scenarios(seed: int = 4, members: int = 64, low: float = 50e3, high: float = 2e6,
+                       duration: int = 3600, processes: int | None = None) -> list[Workload]:
+    """The batched ensemble (64 seeded quadtree meshes, about 40M cells in
+    total), generated in parallel worker processes (spawned, so that no CUDA
+    context is inherited)."""
+    import multiprocessing as mp
+    import os
+    from concurrent.futures import ProcessPoolExecutor
+    params = ensemble_members(seed, members, low, high, duration)
+    workers = min(len(params), processes or os.cpu_count() or 1)
+    if workers <= 1:
+        return [_member(kw) for kw in params]
+    with ProcessPoolExecutor(workers, mp_context=mp.get_context('spawn')) as pool:
+        return list(pool.map(_member, params))

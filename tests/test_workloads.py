@@ -54,3 +54,21 @@ def test_configs_have_the_stated_shape():
     assert np.all(d.initial_depth[1:][d.mesh.x[1:] < 12.8] == 2.0)
     assert np.all(d.initial_depth[1:][d.mesh.x[1:] >= 12.8] == 0.0)
     assert len(d.forcing.boundaries[0].cells) == 4 * 128 - 4
+
+
+def test_ensemble_parameters_follow_the_batched_configuration():
+    from nhflood.workloads import ensemble_members, multires_quadtree, quadtree_width_for
+    ps = ensemble_members()
+    assert len(ps) == 64
+    widths = np.array([p['width'] for p in ps])
+    assert widths.min() >= quadtree_width_for(50e3) - 40 and widths.max() <= quadtree_width_for(2e6) + 40
+    assert np.all(widths % 20 == 0)
+    peaks = np.array([p['hyetograph_peak'] for p in ps])
+    assert 25 < np.median(peaks) < 60
+    f = np.array([p['n_factors'] for p in ps])
+    assert f.min() >= 0.8 and f.max() <= 1.2
+    w = multires_quadtree(**dict(ps[3], width=1500.0))
+    mm = w.forcing.rain.millimetres[:, 0]
+    assert len(mm) == 60 and mm.argmax() in (29, 30)
+    assert abs(mm.sum() - ps[3]['hyetograph_peak'] / 2) < 1e-3  # a 1 h triangle holds peak/2 mm
+    assert w.land_parameters[2].manning_n == 0.05 * ps[3]['n_factors'][2]
