@@ -246,6 +246,79 @@ def bench_batched(args, rank, world, local):
     ens.close()
 
 
+def _request_workload(params):
+    from nhflood.workloads import multires_quadtree
+    return multires_quadtree(**params)
+
+
+def bench_served(args, rank, world, local):
+    """Served form: a Poisson stream of flood-solve requests of uneven mesh
+    size, admitted under an HBM budget and stepped together (continuous
+    batching), replayed in real time; then the same stream through the plain
+    form one request at a time."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    import torch
+    from nhflood.serving import FloodServer, Request, latency_summary, serve, serve_sequential
+    from nhflood.workloads import served_requests
+    device = torch.device('cuda', local)
+    torch.cuda.set_device(device)
+    stream = served_requests(seed=5 + rank, count=args.requests)
+    t0 = time.perf_counter()
+    with ProcessPoolExecutor(min(len(stream), os.cpu_count() or 1), mp_context=mp.get_context('spawn')) as pool:
+        workloads = list(pool.map(_request_workload, [r['params'] for r in stream]))
+    t_gen = time.perf_counter() - t0
+    reqs = [Request(r['id'], r['arrival'], w) for r, w in zip(stream, workloads)]
+    for r in reqs:
+        r.prepare()
+    # warm-up: one small request through both paths (module loads, first graph)
+    warm = [Request(-1, 0.0, _request_workload(dict(stream[0]['params'], width=1000.0, duration=60)))]
+    server = FloodServer(hbm_budget=args.hbm_budget, tile=args.tile or 512, device=str(device))
+    serve(warm, server, realtime=False)
+    serve_sequential([Request(-1, 0.0, warm[0].workload)], tile=args.tile or 512, device=str(device), realtime=False)
+    server = FloodServer(hbm_budget=args.hbm_budget, tile=args.tile or 512, device=str(device))
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        served = serve(reqs, server, realtime=True)
+        served_wall = time.perf_counter() - t0
+    server.close()
+    t0 = time.perf_counter()
+    sequential = serve_sequential(reqs, tile=args.tile or 512, device=str(device), realtime=True)
+    seq_wall = time.perf_counter() - t0
+    by_id = {c.id: c for c in sequential}
+    max_err = 0.0
+    for c in served:
+        o = by_id[c.id]
+        max_err = max(max_err, float(np.abs(c.depth - o.depth).max()), float(np.abs(c.max_depth - o.max_depth).max()))
+    cell_updates = sum(c.cell_updates for c in served)
+    value = cell_updates / served_wall
+    seq_value = sum(c.cell_updates for c in sequential) / seq_wall
+    if rank == 0:
+        cells = np.array([r.workload.cells for r in reqs])
+        line = {
+            'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': server.rounds,
+            'warmup': 1, 'ms_per_step': served_wall * 1e3 / max(1, server.rounds), 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'form': 'served',
+            'config': {'workload': f'served_{len(reqs)}_requests', 'arrival_rate_per_s': 2.0,
+                       'cells_total': int(cells.sum()), 'cells_min': int(cells.min()), 'cells_max': int(cells.max()),
+                       'hbm_budget_bytes': args.hbm_budget, 'tile': args.tile or 512, 'parallelism': f'replicas{world}',
+                       'l2': 'inputs larger than L2 once several solves are resident'},
+            'timing': 'wall clock of the whole session, arrivals replayed in real time',
+            'latency': latency_summary(served),
+            'plain_sequential': {'value': seq_value, 'unit': METRIC, 'latency': latency_summary(sequential),
+                                 'wall_s': seq_wall},
+            'served_over_plain': value / seq_value,
+            'max_depth_error_vs_plain_m': max_err,
+            'peak_resident_bytes_estimate': server.peak_used,
+            'session_wall_s': served_wall,
+            'gpu_launches': None,
+            'e2e': {'value': value, 'unit': METRIC, 'h2d_bytes_per_step': None, 'd2h_bytes_per_step': None},
+            'clocks': clocks.summary(),
+            'setup_seconds': {'generate': round(t_gen, 1)},
+        }
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -254,7 +327,9 @@ def main():
     ap.add_argument('--workload', default=os.environ.get('NHF_BENCH_WORKLOAD', 'multires_quadtree'))
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
-    ap.add_argument('--form', default='plain', choices=['plain', 'batched'])
+    ap.add_argument('--form', default='plain', choices=['plain', 'batched', 'served'])
+    ap.add_argument('--requests', type=int, default=48, help='served: requests in the stream')
+    ap.add_argument('--hbm-budget', type=float, default=150e9, help='served: admission budget in bytes')
     ap.add_argument('--members', type=int, default=64)
     ap.add_argument('--tile', type=int, default=None, help='batched: tile size (default: autotuned)')
     ap.add_argument('--grid', type=int, default=None, help='batched: 0 persistent, -1 block per tile')
@@ -285,8 +360,8 @@ def main():
         from datetime import timedelta
         dist.init_process_group('nccl', timeout=timedelta(seconds=120))
         torch.cuda.set_device(local)
-    if args.form == 'batched':
-        bench_batched(args, rank, world, local)
+    if args.form in ('batched', 'served'):
+        (bench_batched if args.form == 'batched' else bench_served)(args, rank, world, local)
         if world > 1:
             dist.barrier()
             dist.destroy_process_group()

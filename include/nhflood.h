@@ -171,12 +171,13 @@ const char *nhf_path(const nhf_handle *h);
  * together, one fused step launch per slot for all of them, each member
  * with its own clock, CFL dt, limiter statistics, budget and extrema.
  * Members must run the fused tiled step with one tile size (nhf_params.path
- * = that size), one batch size and one theta class (= 1 or < 1), and must
- * have been created on `stream`, the stream the ensemble orders itself
- * against. Everything else about a member (forcing, clock, budget flush,
- * stations, CFL read-back) still goes through its own handle between
- * batches. grid_blocks: 0 = persistent grid (resident blocks per SM x SMs),
- * -1 = one block per tile, > 0 = that many blocks. */
+ * = that size), one batch size and one theta class (= 1 or < 1). A batch
+ * starts after the work queued so far on `stream` and on every member's
+ * creation stream, and those streams wait for the batch. Everything else
+ * about a member (forcing, clock, budget flush, stations, CFL read-back)
+ * still goes through its own handle between batches. grid_blocks: 0 =
+ * persistent grid (resident blocks per SM x SMs), -1 = one block per tile,
+ * > 0 = that many blocks. */
 typedef struct nhf_ensemble nhf_ensemble;
 int nhf_ensemble_create(nhf_handle *const *members, int32_t n, int32_t grid_blocks, void *stream,
                         nhf_ensemble **out);

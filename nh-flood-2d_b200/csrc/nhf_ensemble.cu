@@ -21,6 +21,7 @@ using namespace nhf;
 
 struct nhf_ensemble {
     std::vector<nhf_handle *> members;
+    std::vector<cudaStream_t> streams;  // distinct caller streams of the ensemble and its members
     cudaStream_t user = nullptr, s = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     EnsembleLaunch launch{};
@@ -120,13 +121,18 @@ int nhf_ensemble_create(nhf_handle *const *members, int32_t n, int32_t grid_bloc
         if (h->tb.plan.tile != tile) return efail(nullptr, NHF_EINVAL, "member %d has tile %d, member 0 has %d", i, h->tb.plan.tile, tile);
         if (h->p.batch_size != h0->p.batch_size) return efail(nullptr, NHF_EINVAL, "member %d has another batch size", i);
         if (h->dev.theta_one != h0->dev.theta_one) return efail(nullptr, NHF_EINVAL, "members mix theta = 1 and theta < 1");
-        if (h->user != (cudaStream_t)stream) return efail(nullptr, NHF_EINVAL, "member %d was created on another stream", i);
         for (int j = 0; j < i; ++j)
             if (members[j] == h) return efail(nullptr, NHF_EINVAL, "member %d is listed twice", i);
     }
     nhf_ensemble *e = new nhf_ensemble();
     e->members.assign(members, members + n);
     e->user = (cudaStream_t)stream;
+    e->streams.push_back(e->user);
+    for (int i = 0; i < n; ++i) {
+        bool seen = false;
+        for (cudaStream_t st : e->streams) seen = seen || st == members[i]->user;
+        if (!seen) e->streams.push_back(members[i]->user);
+    }
     int rc;
 #define ECKC(call)                                                                                  \
     do {                                                                                            \
@@ -224,14 +230,17 @@ int nhf_ensemble_run_batch_async(nhf_ensemble *e, const uint32_t *targets, const
         e->h_words[4 * i + 2] = origins[2 * i];
         e->h_words[4 * i + 3] = origins[2 * i + 1];
     }
-    ECK(e, cudaEventRecord(e->ev_in, e->user));
-    ECK(e, cudaStreamWaitEvent(e->s, e->ev_in, 0));
+    // after all work queued on the caller streams of the ensemble and of its members
+    for (cudaStream_t st : e->streams) {
+        ECK(e, cudaEventRecord(e->ev_in, st));
+        ECK(e, cudaStreamWaitEvent(e->s, e->ev_in, 0));
+    }
     if (!e->graph) { int rc = build_graph(e); if (rc) return rc; }
     ECK(e, cudaGraphLaunch(e->graph, e->s));
     e->in_flight = true;
     ECK(e, cudaGetLastError());
     ECK(e, cudaEventRecord(e->ev_out, e->s));
-    ECK(e, cudaStreamWaitEvent(e->user, e->ev_out, 0));
+    for (cudaStream_t st : e->streams) ECK(e, cudaStreamWaitEvent(st, e->ev_out, 0));
     return NHF_OK;
 }
 

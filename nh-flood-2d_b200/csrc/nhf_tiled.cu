@@ -890,10 +890,14 @@ int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::v
     return 0;
 }
 
+// The attribute only permits dynamic shared memory up to a size; it is set
+// to the planner's limit once, so that building one mesh never lowers it
+// below what an already captured graph of another mesh launches with.
 template <typename K>
 void set_smem(K kernel, size_t bytes)
 {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(bytes > (size_t)kMaxSharedBytes ? bytes : (size_t)kMaxSharedBytes));
 }
 
 template <int NT, int CPT>

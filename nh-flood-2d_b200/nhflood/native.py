@@ -242,7 +242,7 @@ class CudaEngine(Engine):
     def apply_initial_levels(self, targets):
         t = self.torch.from_numpy(np.ascontiguousarray(targets, dtype=np.float32)).to(self.device)
         self._check(self.lib.nhf_apply_initial_levels(self.h, c_void_p(t.data_ptr())), 'nhf_apply_initial_levels')
-        self.torch.cuda.synchronize(self.device)
+        self.torch.cuda.current_stream(self.device).synchronize()  # t stays alive until the kernel has read it
 
     def compute_cfl(self):
         self._check(self.lib.nhf_compute_cfl(self.h), 'nhf_compute_cfl')
@@ -327,8 +327,9 @@ class CudaEngine(Engine):
 class CudaEnsemble:
     """Member CudaEngines advanced together (nhf_ensemble_*): one fused step
     launch per slot for all members, each with its own clock and dt. The
-    members must be on the fused tiled step with one tile size and must have
-    been created on the current torch stream of their device."""
+    members must be on the fused tiled step with one tile size. Batches are
+    ordered after the current torch stream and the members' creation
+    streams."""
 
     def __init__(self, engines, grid_blocks: int = 0):
         if not engines:

@@ -22,10 +22,10 @@ FRAME = 900
 
 
 class PlainRun:
-    def __init__(self, workload, engine_factory, batch_size: int = 32):
+    def __init__(self, workload, engine_factory, batch_size: int = 32, arrays=None):
         self.w = workload
         self.params = StepParams(afa=workload.afa, sita=workload.sita, min_h=workload.min_h, batch_size=batch_size)
-        self.arrays = workload.step_arrays()
+        self.arrays = workload.step_arrays() if arrays is None else arrays
         self.engine = engine_factory(self.arrays, self.params)
         self.clock = HostClock(0.0, batch_size=batch_size)
         eng = self.engine

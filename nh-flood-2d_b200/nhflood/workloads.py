@@ -474,7 +474,7 @@ def meander_leaves(seed: int, width: float, base: float, buffer: float, half_cha
 
 
 def multires_quadtree(seed: int = 2, width: float = 20000.0, duration: int = 7200, *,
-                      hyetograph_peak: float | None = None, n_factors=None,
+                      hyetograph_peak: float | None = None, n_factors=None, uniform_rain: float | None = None,
                       name: str = 'multires_quadtree') -> Workload:
     """The multi-resolution configuration: 3-level 2:1 quadtree (20/10/5 m)
     around a carved meandering channel (30 m wide, 3 m deep), fractal bed
@@ -486,7 +486,9 @@ def multires_quadtree(seed: int = 2, width: float = 20000.0, duration: int = 720
 
     hyetograph_peak replaces the storm by uniform rain following a triangular
     1 h pulse with that peak (mm/h) in 60 s bands; n_factors multiplies the
-    Manning n of the 4 classes (the batched ensemble's perturbations)."""
+    Manning n of the 4 classes (the batched ensemble's perturbations);
+    uniform_rain replaces it by constant uniform rain (mm/h) for the whole
+    duration (the served requests)."""
     base = 20.0
     lv, li, lj, distance, n0 = meander_leaves(seed, width, base, buffer=500.0, half_channel=15.0)
     rng = np.random.default_rng(seed + 1)
@@ -510,6 +512,10 @@ def multires_quadtree(seed: int = 2, width: float = 20000.0, duration: int = 720
 
     mesh = quadtree_mesh(lv, li, lj, base, 3, n0, n0, bed_at, land_at)
     geometry = MeshGeometry.from_mesh(mesh)
+    if uniform_rain is not None:
+        rain, raster = _uniform_rain(geometry, width, width, [0.0], [float(duration)],
+                                     [uniform_rain * duration / 3600.0])
+        return _quadtree_workload(name, seed, width, duration, mesh, geometry, rain, raster, n_factors)
     if hyetograph_peak is not None:
         starts = np.arange(0, duration, 60.0)
         ends = starts + 60.0
@@ -597,3 +603,22 @@ def ensemble_scenarios(seed: int = 4, members: int = 64, low: float = 50e3, high
         return [_member(kw) for kw in params]
     with ProcessPoolExecutor(workers, mp_context=mp.get_context('spawn')) as pool:
         return list(pool.map(_member, params))
+
+
+def served_requests(seed: int = 5, count: int = 512, rate: float = 2.0, low: float = 16e3, high: float = 4e6,
+                    duration_range=(600, 3600), rain_range=(10.0, 100.0)) -> list[dict]:
+    """The served request stream: Poisson arrivals (rate per second), per
+    request a seeded quadtree with a cell count drawn log-uniform in
+    [low, high], uniform rain U(rain_range) mm/h and a duration
+    U(duration_range) s. Returns [{'id', 'arrival', 'params'}]."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+    cells = np.exp(rng.uniform(np.log(low), np.log(high), count))
+    rain = rng.uniform(*rain_range, count)
+    durations = rng.integers(duration_range[0], duration_range[1] + 1, count)
+    out = []
+    for i in range(count):
+        params = dict(seed=int(seed * 100000 + i), width=20.0 * max(8, round(quadtree_width_for(cells[i]) / 20.0)),
+                      duration=int(durations[i]), uniform_rain=float(rain[i]), name=f'request_{i:03d}')
+        out.append(dict(id=i, arrival=float(arrivals[i]), params=params))
+    return out

@@ -17,6 +17,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / '_build' / 'liboracle.so'
+LIB_PATH_F64 = HERE / '_build' / 'liboracle_f64.so'  # same step with real = double (precision study)
 TRACE_COLS = 10
 STATE_F32 = ('bed', 'depth', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_speed', 'u', 'v')
 STATE_U32 = ('peak_hi', 'peak_lo')
@@ -24,8 +25,10 @@ STATE_U32 = ('peak_hi', 'peak_lo')
 
 def build() -> Path:
     sources = [HERE / 'step_ref.c', HERE / 'mathref.c', HERE / 'step_ref.h', HERE / 'Makefile']
-    if not LIB_PATH.exists() or any(p.stat().st_mtime > LIB_PATH.stat().st_mtime for p in sources):
-        subprocess.run(['make', '-s', '-C', str(HERE)], check=True)
+    for lib in (LIB_PATH, LIB_PATH_F64):
+        if not lib.exists() or any(p.stat().st_mtime > lib.stat().st_mtime for p in sources):
+            subprocess.run(['make', '-s', '-C', str(HERE)], check=True)
+            break
     return LIB_PATH
 
 
@@ -37,45 +40,58 @@ _STATE = ('bed', 'depth', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_sp
           'peak_hi', 'peak_lo', 'pipe_q')
 
 
-class OraMesh(ctypes.Structure):
-    _fields_ = ([(n, c_int32) for n in ('e_num', 's_num', 'b_num', 'n_rates', 'isl_len', 'batch_size')]
-                + [(n, c_float) for n in ('g', 'afa', 'sita', 'min_h', 'min_dt')]
-                + [(n, c_void_p) for n in _PTRS]
-                + [('hang_cells', c_int32), ('hang_edges', c_int32)]
-                + [(n, c_void_p) for n in _HANG]
-                + [(n, c_void_p) for n in _STATE])
+def _mesh_type(real):
+    class OraMeshT(ctypes.Structure):
+        _fields_ = ([(n, c_int32) for n in ('e_num', 's_num', 'b_num', 'n_rates', 'isl_len', 'batch_size')]
+                    + [(n, real) for n in ('g', 'afa', 'sita', 'min_h')] + [('min_dt', c_float)]
+                    + [(n, c_void_p) for n in _PTRS]
+                    + [('hang_cells', c_int32), ('hang_edges', c_int32)]
+                    + [(n, c_void_p) for n in _HANG]
+                    + [(n, c_void_p) for n in _STATE])
+    return OraMeshT
 
 
+OraMesh = _mesh_type(c_float)
+_MESH = {'f32': OraMesh, 'f64': _mesh_type(c_double)}
+_REAL = {'f32': c_float, 'f64': c_double}
+_LIBS = {}
 _LIB = None
 
 
-def library():
+def library(precision: str = 'f32'):
+    """The F32 restatement, or with precision='f64' the same step in F64."""
     global _LIB
-    if _LIB is None:
-        lib = ctypes.CDLL(str(build()))
+    if precision not in _LIBS:
+        build()
+        lib = ctypes.CDLL(str(LIB_PATH if precision == 'f32' else LIB_PATH_F64))
         H = c_void_p
         U2 = POINTER(c_uint32)
+        R = _REAL[precision]
+        RP = POINTER(R)
         for name, res, args in [
-            ('ora_create', H, [POINTER(OraMesh)]), ('ora_destroy', None, [H]), ('ora_initialize', None, [H]),
+            ('ora_create', H, [POINTER(_MESH[precision])]), ('ora_destroy', None, [H]),
+            ('ora_initialize', None, [H]),
             ('ora_set_threads', None, [c_int]), ('ora_set_clock', None, [H, U2]), ('ora_get_clock', None, [H, U2]),
             ('ora_set_active', None, [H, c_int]),
-            ('ora_set_forcing', None, [H, POINTER(c_float), POINTER(c_float), c_int]),
-            ('ora_apply_initial_levels', None, [H, POINTER(c_float)]), ('ora_compute_cfl', None, [H]),
+            ('ora_set_forcing', None, [H, RP, RP, c_int]),
+            ('ora_apply_initial_levels', None, [H, RP]), ('ora_compute_cfl', None, [H]),
             ('ora_initial_diagnostics', None, [H]), ('ora_reset_extrema', None, [H]),
             ('ora_run_batch', None, [H, U2, U2, U2]), ('ora_budget_flush', None, [H, POINTER(c_double)]),
-            ('ora_budget_terms', c_int, [H]), ('ora_ndt', c_float, [H]), ('ora_cfl_arg', c_int32, [H]),
-            ('ora_limits', None, [H, POINTER(c_float), POINTER(c_int32)]), ('ora_reset_limits', None, [H]),
-            ('ora_read_eq', None, [H, POINTER(c_float)]), ('ora_read_flow_depth', None, [H, POINTER(c_float)]),
-            ('ora_read_gradients', None, [H, POINTER(c_float)]), ('ora_update_pressure', None, [H]),
-            ('ora_pressure_difference', c_float, [H, c_int, c_int, c_int, c_float]),
+            ('ora_budget_terms', c_int, [H]), ('ora_ndt', R, [H]), ('ora_cfl_arg', c_int32, [H]),
+            ('ora_limits', None, [H, RP, POINTER(c_int32)]), ('ora_reset_limits', None, [H]),
+            ('ora_read_eq', None, [H, RP]), ('ora_read_flow_depth', None, [H, RP]),
+            ('ora_read_gradients', None, [H, RP]), ('ora_update_pressure', None, [H]),
+            ('ora_pressure_difference', R, [H, c_int, c_int, c_int, R]),
             ('ora_ln', c_double, [c_double]), ('ora_exp', c_double, [c_double]),
             ('ora_powf', c_float, [c_float, c_float]), ('ora_expf', c_float, [c_float]),
         ]:
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
-        _LIB = lib
-    return _LIB
+        _LIBS[precision] = lib
+        if precision == 'f32':
+            _LIB = lib
+    return _LIBS[precision]
 
 
 def set_threads(n: int) -> None:
@@ -87,8 +103,11 @@ class OracleEngine:
 
     backend = 'cpu-oracle'
 
-    def __init__(self, arrays, params, threads: int | None = None):
-        self.lib = library()
+    def __init__(self, arrays, params, threads: int | None = None, precision: str = 'f32'):
+        self.lib = library(precision)
+        self.precision = precision
+        self.real = np.float32 if precision == 'f32' else np.float64
+        self.creal = _REAL[precision]
         if threads:
             self.lib.ora_set_threads(int(threads))
         self.device_name = f'CPU restatement ({os.cpu_count()} cores)'
@@ -104,11 +123,11 @@ class OracleEngine:
             self.keep[name] = a
             return a.ctypes.data
 
-        m = OraMesh()
+        m = _MESH[precision]()
         m.e_num, m.s_num, m.b_num, m.n_rates = e, s, arrays.b_num, arrays.n_rates
         m.isl_len, m.batch_size = len(arrays.isl_data), params.batch_size
         m.g, m.afa, m.sita, m.min_h, m.min_dt = params.g, params.afa, params.sita, params.min_h, params.min_dt
-        f32 = np.float32
+        f32 = self.real
         for name, dtype in [('x', f32), ('y', f32), ('area', f32), ('width', f32), ('height', f32), ('f0', f32),
                             ('fc', f32), ('k', f32), ('boundary_id', np.int32), ('rain_index', np.int32),
                             ('face_ptr', np.int32), ('face_count', np.int32), ('isl_data', np.int32),
@@ -156,16 +175,18 @@ class OracleEngine:
     def set_active(self, active):
         self.lib.ora_set_active(self.h, int(active))
 
+    def _ptr(self, a):
+        return a.ctypes.data_as(POINTER(self.creal))
+
     def set_forcing(self, coefficients, rain_rates, raining):
-        coef = None if coefficients is None else np.ascontiguousarray(coefficients, np.float32)
-        rates = None if rain_rates is None else np.ascontiguousarray(rain_rates, np.float32)
-        self.lib.ora_set_forcing(self.h, coef.ctypes.data_as(POINTER(c_float)) if coef is not None else None,
-                                 rates.ctypes.data_as(POINTER(c_float)) if rates is not None else None,
-                                 int(bool(raining)))
+        coef = None if coefficients is None else np.ascontiguousarray(coefficients, self.real)
+        rates = None if rain_rates is None else np.ascontiguousarray(rain_rates, self.real)
+        self.lib.ora_set_forcing(self.h, self._ptr(coef) if coef is not None else None,
+                                 self._ptr(rates) if rates is not None else None, int(bool(raining)))
 
     def apply_initial_levels(self, targets):
-        t = np.ascontiguousarray(targets, np.float32)
-        self.lib.ora_apply_initial_levels(self.h, t.ctypes.data_as(POINTER(c_float)))
+        t = np.ascontiguousarray(targets, self.real)
+        self.lib.ora_apply_initial_levels(self.h, self._ptr(t))
 
     def compute_cfl(self):
         self.lib.ora_compute_cfl(self.h)
@@ -190,14 +211,14 @@ class OracleEngine:
 
     def cfl(self):
         si = int(self.lib.ora_cfl_arg(self.h))
-        fd = np.zeros(self.arrays.s_num, np.float32)
-        self.lib.ora_read_flow_depth(self.h, fd.ctypes.data_as(POINTER(c_float)))
+        fd = np.zeros(self.arrays.s_num, self.real)
+        self.lib.ora_read_flow_depth(self.h, self._ptr(fd))
         return float(self.lib.ora_ndt(self.h)), si, float(fd[si])
 
     def limits(self):
-        values = np.zeros(5, np.float32)
+        values = np.zeros(5, self.real)
         ids = np.zeros(3, np.int32)
-        self.lib.ora_limits(self.h, values.ctypes.data_as(POINTER(c_float)), ids.ctypes.data_as(POINTER(c_int32)))
+        self.lib.ora_limits(self.h, self._ptr(values), ids.ctypes.data_as(POINTER(c_int32)))
         return values, ids
 
     def reset_limits(self):
@@ -206,7 +227,7 @@ class OracleEngine:
     def sample_stations(self, ids):
         ids = np.asarray(ids, dtype=np.int64)
         d, z = self.state['depth'], self.state['bed']
-        out = np.zeros((len(ids), 4), np.float32)
+        out = np.zeros((len(ids), 4), self.real)
         if len(ids):
             out[:, 0] = d[ids]
             out[:, 1] = z[ids] + d[ids]
@@ -215,13 +236,13 @@ class OracleEngine:
         return out
 
     def read_eq(self):
-        out = np.zeros((self.arrays.e_num, 4), np.float32)
-        self.lib.ora_read_eq(self.h, out.ctypes.data_as(POINTER(c_float)))
+        out = np.zeros((self.arrays.e_num, 4), self.real)
+        self.lib.ora_read_eq(self.h, self._ptr(out))
         return out
 
     def read_gradients(self):
-        out = np.zeros((max(1, self.arrays.hang_cells), 2), np.float32)
-        self.lib.ora_read_gradients(self.h, out.ctypes.data_as(POINTER(c_float)))
+        out = np.zeros((max(1, self.arrays.hang_cells), 2), self.real)
+        self.lib.ora_read_gradients(self.h, self._ptr(out))
         return out[:self.arrays.hang_cells]
 
     def peak_memory(self):

@@ -36,8 +36,23 @@
 #define SNAP_TICKS 1099512u /* ceil(1e-6 * 2**40), clock.py:11 */
 #define BLOCK 256
 
-static inline float maxf(float a, float b) { return a > b ? a : b; }
-static inline float minf(float a, float b) { return b < a ? b : a; }
+typedef ora_real real;
+#ifdef ORA_REAL_DOUBLE
+#define R(x) x
+#define RABS(x) fabs(x)
+#define RSQRT(x) sqrt(x)
+#define RPOW(x, y) pow(x, y)
+#define REXP(x) exp(x)
+#else
+#define R(x) x##f
+#define RABS(x) fabsf(x)
+#define RSQRT(x) sqrtf(x)
+#define RPOW(x, y) ora_powf(x, y)
+#define REXP(x) ora_expf(x)
+#endif
+
+static inline real maxf(real a, real b) { return a > b ? a : b; }
+static inline real minf(real a, real b) { return b < a ? b : a; }
 static inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
 static inline float bitsf(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
 
@@ -46,25 +61,25 @@ struct ora_ctx {
     int terms, blocks;
     /* clock (clock.py:60-68) */
     uint32_t now[2], next[2], origin[2], step_end[2];
-    float dt, local, end_local;
+    float dt, local, end_local;  /* the clock's F32 values */
     int active, slot;
     /* scalars */
-    float ndt;
+    real ndt;
     int32_t cfl_arg;
     uint32_t limited_cells, limited_faces;
-    float minimum_scale;
+    real minimum_scale;
     uint32_t wet;
-    float limit_value[5];
+    real limit_value[5];
     int32_t limit_ids[3];
     int raining;
     /* per-boundary */
-    float *coefficients, *values, *level_values;
-    const float *rain_rates_ext;
-    float *rain_rates;
+    real *coefficients, *values, *level_values;
+    const real *rain_rates_ext;
+    real *rain_rates;
     /* work */
-    float *sdc, *dh, *eq, *increment, *rain_depth, *donor_scale, *cfl, *flow_depth, *face_qn, *ssq;
-    float *gradients;
-    float *diag;      /* [blocks*terms] per-step f32 values per cell collected per block */
+    real *sdc, *dh, *eq, *increment, *rain_depth, *donor_scale, *cfl, *flow_depth, *face_qn, *ssq;
+    real *gradients;
+    real *diag;      /* [blocks*terms] per-step f32 values per cell collected per block */
     double *acc_sum, *acc_comp; /* [blocks*terms] */
     uint32_t *trace;  /* [batch][10] */
 };
@@ -86,21 +101,21 @@ ora_ctx *ora_create(const ora_mesh *mesh)
     c->terms = 4 + 6 * b;
     c->blocks = (e + BLOCK - 1) / BLOCK;
     int bb = b > 0 ? b : 1;
-    c->coefficients = (float *)calloc((size_t)bb * 2, sizeof(float));
-    c->values = (float *)calloc(bb, sizeof(float));
-    c->level_values = (float *)calloc(bb, sizeof(float));
-    c->rain_rates = (float *)calloc(mesh->n_rates > 0 ? mesh->n_rates : 1, sizeof(float));
-    c->sdc = (float *)calloc(s, sizeof(float));
-    c->dh = (float *)calloc(s, sizeof(float));
-    c->eq = (float *)calloc((size_t)e * 4, sizeof(float));
-    c->increment = (float *)calloc(e, sizeof(float));
-    c->rain_depth = (float *)calloc(e, sizeof(float));
-    c->donor_scale = (float *)calloc(e, sizeof(float));
-    c->cfl = (float *)calloc(s, sizeof(float));
-    c->flow_depth = (float *)calloc(s, sizeof(float));
-    c->face_qn = (float *)calloc((size_t)e * 4, sizeof(float));
-    c->ssq = (float *)calloc(e, sizeof(float));
-    c->gradients = (float *)calloc((size_t)(mesh->hang_cells > 0 ? mesh->hang_cells : 1) * 2, sizeof(float));
+    c->coefficients = (real *)calloc((size_t)bb * 2, sizeof(real));
+    c->values = (real *)calloc(bb, sizeof(real));
+    c->level_values = (real *)calloc(bb, sizeof(real));
+    c->rain_rates = (real *)calloc(mesh->n_rates > 0 ? mesh->n_rates : 1, sizeof(real));
+    c->sdc = (real *)calloc(s, sizeof(real));
+    c->dh = (real *)calloc(s, sizeof(real));
+    c->eq = (real *)calloc((size_t)e * 4, sizeof(real));
+    c->increment = (real *)calloc(e, sizeof(real));
+    c->rain_depth = (real *)calloc(e, sizeof(real));
+    c->donor_scale = (real *)calloc(e, sizeof(real));
+    c->cfl = (real *)calloc(s, sizeof(real));
+    c->flow_depth = (real *)calloc(s, sizeof(real));
+    c->face_qn = (real *)calloc((size_t)e * 4, sizeof(real));
+    c->ssq = (real *)calloc(e, sizeof(real));
+    c->gradients = (real *)calloc((size_t)(mesh->hang_cells > 0 ? mesh->hang_cells : 1) * 2, sizeof(real));
     c->acc_sum = (double *)calloc((size_t)c->blocks * c->terms, sizeof(double));
     c->acc_comp = (double *)calloc((size_t)c->blocks * c->terms, sizeof(double));
     c->trace = (uint32_t *)calloc((size_t)mesh->batch_size * ORA_TRACE_COLS, sizeof(uint32_t));
@@ -122,10 +137,10 @@ void ora_set_clock(ora_ctx *c, const uint32_t now[2]) { c->now[0] = now[0]; c->n
 void ora_get_clock(const ora_ctx *c, uint32_t now[2]) { now[0] = c->now[0]; now[1] = c->now[1]; }
 void ora_set_active(ora_ctx *c, int active) { c->active = active; }
 int ora_budget_terms(const ora_ctx *c) { return c->terms; }
-float ora_ndt(const ora_ctx *c) { return c->ndt; }
+real ora_ndt(const ora_ctx *c) { return c->ndt; }
 int32_t ora_cfl_arg(const ora_ctx *c) { return c->cfl_arg; }
 
-void ora_limits(const ora_ctx *c, float values[5], int32_t ids[3])
+void ora_limits(const ora_ctx *c, real values[5], int32_t ids[3])
 {
     memcpy(values, c->limit_value, sizeof(c->limit_value));
     memcpy(ids, c->limit_ids, sizeof(c->limit_ids));
@@ -133,18 +148,18 @@ void ora_limits(const ora_ctx *c, float values[5], int32_t ids[3])
 
 void ora_reset_limits(ora_ctx *c) { c->limit_value[0] = INFINITY; }
 
-void ora_read_eq(const ora_ctx *c, float *eq) { memcpy(eq, c->eq, sizeof(float) * 4 * (size_t)c->m.e_num); }
-void ora_read_flow_depth(const ora_ctx *c, float *out) { memcpy(out, c->flow_depth, sizeof(float) * (size_t)c->m.s_num); }
-void ora_read_gradients(const ora_ctx *c, float *out)
+void ora_read_eq(const ora_ctx *c, real *eq) { memcpy(eq, c->eq, sizeof(real) * 4 * (size_t)c->m.e_num); }
+void ora_read_flow_depth(const ora_ctx *c, real *out) { memcpy(out, c->flow_depth, sizeof(real) * (size_t)c->m.s_num); }
+void ora_read_gradients(const ora_ctx *c, real *out)
 {
-    if (c->m.hang_cells > 0) memcpy(out, c->gradients, sizeof(float) * 2 * (size_t)c->m.hang_cells);
+    if (c->m.hang_cells > 0) memcpy(out, c->gradients, sizeof(real) * 2 * (size_t)c->m.hang_cells);
 }
 
-void ora_set_forcing(ora_ctx *c, const float *coefficients, const float *rain_rates, int raining)
+void ora_set_forcing(ora_ctx *c, const real *coefficients, const real *rain_rates, int raining)
 {
     int bb = c->m.b_num > 0 ? c->m.b_num : 1;
-    if (coefficients) memcpy(c->coefficients, coefficients, sizeof(float) * 2 * (size_t)bb);
-    if (rain_rates && c->m.n_rates > 0) memcpy(c->rain_rates, rain_rates, sizeof(float) * (size_t)c->m.n_rates);
+    if (coefficients) memcpy(c->coefficients, coefficients, sizeof(real) * 2 * (size_t)bb);
+    if (rain_rates && c->m.n_rates > 0) memcpy(c->rain_rates, rain_rates, sizeof(real) * (size_t)c->m.n_rates);
     c->raining = raining;
 }
 
@@ -171,7 +186,7 @@ static void acc_add(ora_ctx *c, size_t idx, double p)
 
 /* Reduce a per-cell diagnostic matrix diag[cell*terms + term] (0 where the
  * reference skips add_diagnostic because value == 0) into the accumulator. */
-static void collect(ora_ctx *c, const float *diag)
+static void collect(ora_ctx *c, const real *diag)
 {
     int T = c->terms, e = c->m.e_num;
 #pragma omp parallel for schedule(static)
@@ -181,9 +196,9 @@ static void collect(ora_ctx *c, const float *diag)
             int any = 0;
             for (int i = 0; i < BLOCK; ++i) {
                 int ei = blk * BLOCK + i;
-                float val = ei < e ? diag[(size_t)ei * T + t] : 0.0f;
-                v[i] = val != 0.0f ? (double)val : 0.0;
-                any |= val != 0.0f;
+                real val = ei < e ? diag[(size_t)ei * T + t] : R(0.0);
+                v[i] = val != R(0.0) ? (double)val : 0.0;
+                any |= val != R(0.0);
             }
             if (!any) continue;
             acc_add(c, (size_t)blk * T + t, block_tree(v));
@@ -219,26 +234,26 @@ void ora_initialize(ora_ctx *c)
 {
     const ora_mesh *m = &c->m;
     for (int ei = 1; ei < m->e_num; ++ei) {
-        m->depth[ei] = 0.0f;
+        m->depth[ei] = R(0.0);
         m->infiltration[ei] = m->f0[ei];
     }
     for (int si = 1; si < m->s_num; ++si) {
-        c->dh[si] = -999.0f;
+        c->dh[si] = -R(999.0);
         int so = m->topology[3 * si], el = m->topology[3 * si + 1], eh = m->topology[3 * si + 2];
-        if (so == 2) c->sdc[si] = maxf(fabsf(m->x[eh] - m->x[el]), 0.01f);
-        else c->sdc[si] = maxf(fabsf(m->y[eh] - m->y[el]), 0.01f);
+        if (so == 2) c->sdc[si] = maxf(RABS(m->x[eh] - m->x[el]), R(0.01));
+        else c->sdc[si] = maxf(RABS(m->y[eh] - m->y[el]), R(0.01));
     }
 }
 
-void ora_apply_initial_levels(ora_ctx *c, const float *targets)
+void ora_apply_initial_levels(ora_ctx *c, const real *targets)
 {
     const ora_mesh *m = &c->m;
     int T = c->terms;
-    float *diag = (float *)calloc((size_t)m->e_num * T, sizeof(float));
+    real *diag = (real *)calloc((size_t)m->e_num * T, sizeof(real));
     for (int ei = 1; ei < m->e_num; ++ei) {
         int bi = m->boundary_id[ei];
         if (bi >= 0 && m->kind[bi] == 0) {
-            float previous = m->depth[ei];
+            real previous = m->depth[ei];
             m->depth[ei] = targets[ei];
             diag[(size_t)ei * T + 4 + 5 * bi] = (m->depth[ei] - previous) * m->area[ei];
         }
@@ -247,14 +262,14 @@ void ora_apply_initial_levels(ora_ctx *c, const float *targets)
     free(diag);
 }
 
-static void velocity(const ora_ctx *c, int ei, float *u, float *v)
+static void velocity(const ora_ctx *c, int ei, real *u, real *v)
 {
     const ora_mesh *m = &c->m;
-    float h = maxf(m->depth[ei], 0.01f);
-    *u = 0.0f; *v = 0.0f;
+    real h = maxf(m->depth[ei], R(0.01));
+    *u = R(0.0); *v = R(0.0);
     if (m->depth[ei] >= m->min_h) {
-        *u = (c->eq[4 * ei + 0] + c->eq[4 * ei + 1]) / m->height[ei] / h / 2.0f;
-        *v = (c->eq[4 * ei + 2] + c->eq[4 * ei + 3]) / m->width[ei] / h / 2.0f;
+        *u = (c->eq[4 * ei + 0] + c->eq[4 * ei + 1]) / m->height[ei] / h / R(2.0);
+        *v = (c->eq[4 * ei + 2] + c->eq[4 * ei + 3]) / m->width[ei] / h / R(2.0);
     }
 }
 
@@ -262,16 +277,16 @@ void ora_compute_cfl(ora_ctx *c)
 {
     const ora_mesh *m = &c->m;
     if (!c->active) return;
-    float ndt = INFINITY;
+    real ndt = INFINITY;
 #pragma omp parallel for schedule(static) reduction(min : ndt)
     for (int si = 1; si < m->s_num; ++si) {
         int el = m->topology[3 * si + 1], eh = m->topology[3 * si + 2];
         c->cfl[si] = INFINITY;
         if (el != 0 && eh != 0) {
-            float head = maxf(m->bed[el] + m->depth[el], m->bed[eh] + m->depth[eh]);
-            float h = maxf(head - maxf(maxf(m->bed[el], m->bed[eh]), c->dh[si]), 0.01f);
+            real head = maxf(m->bed[el] + m->depth[el], m->bed[eh] + m->depth[eh]);
+            real h = maxf(head - maxf(maxf(m->bed[el], m->bed[eh]), c->dh[si]), R(0.01));
             c->flow_depth[si] = h;
-            float val = m->afa * m->length[si] / (sqrtf(m->g * h) + fabsf(m->q[si]) / h);
+            real val = m->afa * m->length[si] / (RSQRT(m->g * h) + RABS(m->q[si]) / h);
             c->cfl[si] = val;
             ndt = minf(ndt, val);
         }
@@ -292,7 +307,7 @@ void ora_initial_diagnostics(ora_ctx *c)
 #pragma omp parallel for schedule(static)
     for (int ei = 1; ei < m->e_num; ++ei) {
         for (int d = 0; d < 4; ++d) {
-            float total = 0.0f;
+            real total = R(0.0);
             int p = m->face_ptr[4 * ei + d];
             for (int j = 0; j < m->face_count[4 * ei + d]; ++j) {
                 int si = m->isl_data[p + j];
@@ -300,10 +315,10 @@ void ora_initial_diagnostics(ora_ctx *c)
             }
             c->eq[4 * ei + d] = total;
         }
-        float u, v;
+        real u, v;
         velocity(c, ei, &u, &v);
         m->u[ei] = u; m->v[ei] = v;
-        m->max_speed[ei] = maxf(m->max_speed[ei], sqrtf(u * u + v * v));
+        m->max_speed[ei] = maxf(m->max_speed[ei], RSQRT(u * u + v * v));
         if (m->depth[ei] > m->max_depth[ei]) {
             m->max_depth[ei] = m->depth[ei];
             m->peak_hi[ei] = c->now[0]; m->peak_lo[ei] = c->now[1];
@@ -316,7 +331,7 @@ void ora_reset_extrema(ora_ctx *c)
     const ora_mesh *m = &c->m;
     for (int ei = 1; ei < m->e_num; ++ei) {
         m->max_depth[ei] = m->depth[ei];
-        m->max_speed[ei] = sqrtf(m->u[ei] * m->u[ei] + m->v[ei] * m->v[ei]);
+        m->max_speed[ei] = RSQRT(m->u[ei] * m->u[ei] + m->v[ei] * m->v[ei]);
         m->peak_hi[ei] = c->now[0]; m->peak_lo[ei] = c->now[1];
     }
 }
@@ -386,21 +401,21 @@ static void clock_choose(ora_ctx *c, float candidate, int slot)
 static void prepare_step(ora_ctx *c)
 {
     const ora_mesh *m = &c->m;
-    clock_choose(c, c->ndt, c->slot);
+    clock_choose(c, (float)c->ndt, c->slot);
     if (!c->active) return;
-    c->limited_cells = 0; c->limited_faces = 0; c->minimum_scale = 1.0f;
+    c->limited_cells = 0; c->limited_faces = 0; c->minimum_scale = R(1.0);
     for (int bi = 0; bi < m->b_num; ++bi) {
-        c->values[bi] = c->coefficients[2 * bi] + c->coefficients[2 * bi + 1] * (c->local + c->dt / 2.0f);
+        c->values[bi] = c->coefficients[2 * bi] + c->coefficients[2 * bi + 1] * (c->local + c->dt / R(2.0));
         c->level_values[bi] = c->coefficients[2 * bi] + c->coefficients[2 * bi + 1] * c->end_local;
     }
     if (c->ndt < c->limit_value[0]) {
         int si = c->cfl_arg;
         int el = m->topology[3 * si + 1], eh = m->topology[3 * si + 2];
-        float h = c->flow_depth[si];
+        real h = c->flow_depth[si];
         c->limit_value[0] = c->ndt;
         c->limit_value[1] = m->depth[el]; c->limit_value[2] = m->depth[eh];
         c->limit_value[3] = h;
-        c->limit_value[4] = m->q[si] / maxf(h, 1e-30f);
+        c->limit_value[4] = m->q[si] / maxf(h, R(1e-30));
         c->limit_ids[0] = si; c->limit_ids[1] = el; c->limit_ids[2] = eh;
     }
 }
@@ -411,7 +426,7 @@ static void finish_step(ora_ctx *c)
     if (c->active) {
         row[6] = c->limited_cells;
         row[7] = c->limited_faces;
-        row[8] = fbits(c->minimum_scale);
+        row[8] = fbits((float)c->minimum_scale);
         row[9] = c->wet;
         c->now[0] = c->step_end[0]; c->now[1] = c->step_end[1];
         row[0] = fbits(c->dt);
@@ -424,12 +439,12 @@ static void finish_step(ora_ctx *c)
 /* ---- pressure reconstruction (pressure.py:65-129) ------------------------ */
 
 static void face_difference(const ora_ctx *c, int cell, int direction, int axis,
-                            float *value_out, float *distance_out, int *usable_out)
+                            real *value_out, real *distance_out, int *usable_out)
 {
     const ora_mesh *m = &c->m;
-    float value = 0.0f, distance = 0.0f, total = 0.0f;
+    real value = R(0.0), distance = R(0.0), total = R(0.0);
     int usable = 1;
-    float eta = m->bed[cell] + m->depth[cell];
+    real eta = m->bed[cell] + m->depth[cell];
     int start = m->face_ptr[4 * cell + direction];
     for (int j = 0; j < m->face_count[4 * cell + direction]; ++j) {
         int side = m->isl_data[start + j];
@@ -437,25 +452,25 @@ static void face_difference(const ora_ctx *c, int cell, int direction, int axis,
         if (other == 0 || m->depth[other] <= m->min_h) {
             usable = 0;
         } else {
-            float weight = m->length[side];
+            real weight = m->length[side];
             value += weight * ((m->bed[other] + m->depth[other]) - eta);
-            float delta = axis == 1 ? m->y[other] - m->y[cell] : m->x[other] - m->x[cell];
+            real delta = axis == 1 ? m->y[other] - m->y[cell] : m->x[other] - m->x[cell];
             distance += weight * delta;
             total += weight;
         }
     }
-    if (total > 0.0f) { value /= total; distance /= total; }
+    if (total > R(0.0)) { value /= total; distance /= total; }
     else usable = 0;
     *value_out = value; *distance_out = distance; *usable_out = usable;
 }
 
-static float gradient(const ora_ctx *c, int cell, int axis)
+static real gradient(const ora_ctx *c, int cell, int axis)
 {
     int minus = axis == 1 ? 2 : 0, plus = axis == 1 ? 3 : 1;
-    float dm, xm, dp, xp; int okm, okp;
+    real dm, xm, dp, xp; int okm, okp;
     face_difference(c, cell, minus, axis, &dm, &xm, &okm);
     face_difference(c, cell, plus, axis, &dp, &xp, &okp);
-    float result = 0.0f;
+    real result = R(0.0);
     if (okm && okp) result = (dp - dm) / (xp - xm);
     else if (okm) result = dm / xm;
     else if (okp) result = dp / xp;
@@ -470,7 +485,7 @@ void ora_update_pressure(ora_ctx *c)
         int cell = m->hcells[slot];
         for (int axis = 0; axis < 2; ++axis) {
             if (m->axes[2 * slot + axis] == 1) {
-                float value = 0.0f;
+                real value = R(0.0);
                 if (m->depth[cell] > m->min_h) value = gradient(c, cell, axis);
                 c->gradients[2 * slot + axis] = value;
             }
@@ -478,17 +493,17 @@ void ora_update_pressure(ora_ctx *c)
     }
 }
 
-float ora_pressure_difference(const ora_ctx *c, int side, int lower, int higher, float raw)
+real ora_pressure_difference(const ora_ctx *c, int side, int lower, int higher, real raw)
 {
     const ora_mesh *m = &c->m;
-    float result = raw;
+    real result = raw;
     int index = m->edge_index[side];
     if (index >= 0) {
         if (m->depth[lower] > m->min_h && m->depth[higher] > m->min_h) {
             int axis = m->topology[3 * side] == 2 ? 1 : 0;
-            if (m->offsets[2 * index] != 0.0f)
+            if (m->offsets[2 * index] != R(0.0))
                 result -= c->gradients[2 * m->slots[2 * index] + axis] * m->offsets[2 * index];
-            if (m->offsets[2 * index + 1] != 0.0f)
+            if (m->offsets[2 * index + 1] != R(0.0))
                 result += c->gradients[2 * m->slots[2 * index + 1] + axis] * m->offsets[2 * index + 1];
         }
     }
@@ -497,13 +512,13 @@ float ora_pressure_difference(const ora_ctx *c, int side, int lower, int higher,
 
 /* ---- tick (solver_compact.py:422-613) ------------------------------------ */
 
-static float face_discharge(const float *qn, const float *lengths, const int32_t *ids, int start, int count)
+static real face_discharge(const real *qn, const real *lengths, const int32_t *ids, int start, int count)
 {
-    float result = 0.0f;
+    real result = R(0.0);
     if (count == 1) {
         result = qn[ids[start]];
     } else if (count > 1) {
-        float total = 0.0f, width = 0.0f;
+        real total = R(0.0), width = R(0.0);
         for (int o = 0; o < count; ++o) {
             int side = ids[start + o];
             total += qn[side] * lengths[side];
@@ -514,16 +529,16 @@ static float face_discharge(const float *qn, const float *lengths, const int32_t
     return result;
 }
 
-static float boundary_neighbor_sum(float q, float left, float right, float lext, float rext)
+static real boundary_neighbor_sum(real q, real left, real right, real lext, real rext)
 {
-    float result = left + right;
-    if (lext > 0.0f || rext > 0.0f) {
-        if (lext == 1.0f || rext == 1.0f) {
-            result = 2.0f * q;
+    real result = left + right;
+    if (lext > R(0.0) || rext > R(0.0)) {
+        if (lext == R(1.0) || rext == R(1.0)) {
+            result = R(2.0) * q;
         } else {
-            float product = lext * rext;
-            result = ((1.0f - rext) * left + (1.0f - lext) * right
-                      + 2.0f * q * (lext + rext - 2.0f * product)) / (1.0f - product);
+            real product = lext * rext;
+            result = ((R(1.0) - rext) * left + (R(1.0) - lext) * right
+                      + R(2.0) * q * (lext + rext - R(2.0) * product)) / (R(1.0) - product);
         }
     }
     return result;
@@ -533,16 +548,16 @@ static void tick(ora_ctx *c)
 {
     const ora_mesh *m = &c->m;
     if (!c->active) return;
-    const float dt = c->dt;
+    const real dt = c->dt;
     const int raining = c->raining;
     const int T = c->terms;
-    const int theta_one = m->sita == 1.0f;
-    const float g = m->g;
-    const float neg_g = -g;
-    const float sita = m->sita;
+    const int theta_one = m->sita == R(1.0);
+    const real g = m->g;
+    const real neg_g = -g;
+    const real sita = m->sita;
     /* (1.0 - sita) / 2.0 folds in F64 (Python constants), then rounds to F32. */
-    const float half_rest = (float)((1.0 - (double)m->sita) / 2.0);
-    const float seven_thirds = (float)(7.0 / 3.0);
+    const real half_rest = (real)((1.0 - (double)m->sita) / 2.0);
+    const real seven_thirds = (real)(7.0 / 3.0);
 
     if (!theta_one) {
 #pragma omp parallel for schedule(static)
@@ -555,54 +570,54 @@ static void tick(ora_ctx *c)
     /* side momentum (solver_compact.py:439-486) */
 #pragma omp parallel for schedule(static)
     for (int si = 1; si < m->s_num; ++si) {
-        float bf = m->sbf[si] == 1 ? 0.0f : 1.0f;
+        real bf = m->sbf[si] == 1 ? R(0.0) : R(1.0);
         int so = m->topology[3 * si], el = m->topology[3 * si + 1], eh = m->topology[3 * si + 2];
-        float hl = m->bed[el] + m->depth[el], hr = m->bed[eh] + m->depth[eh];
-        float dx = c->sdc[si];
-        float xq = m->q[si];
-        float xwh = maxf(hl, hr) - maxf(maxf(m->bed[el], m->bed[eh]), c->dh[si]);
-        float difference = hr - hl;
+        real hl = m->bed[el] + m->depth[el], hr = m->bed[eh] + m->depth[eh];
+        real dx = c->sdc[si];
+        real xq = m->q[si];
+        real xwh = maxf(hl, hr) - maxf(maxf(m->bed[el], m->bed[eh]), c->dh[si]);
+        real difference = hr - hl;
         if (m->hang_cells > 0) difference = ora_pressure_difference(c, si, el, eh, difference);
-        float xdq = (neg_g * difference / dx) * maxf(xwh, 0.0f) * dt;
-        float n = m->side_n[si];
-        float xf = 1.0f + g * dt * (n * n) * fabsf(xq / ora_powf(maxf(xwh, 0.00001f), seven_thirds));
+        real xdq = (neg_g * difference / dx) * maxf(xwh, R(0.0)) * dt;
+        real n = m->side_n[si];
+        real xf = R(1.0) + g * dt * (n * n) * RABS(xq / RPOW(maxf(xwh, R(0.00001)), seven_thirds));
         int dl = so == 2 ? 0 : 2, dr = so == 2 ? 1 : 3;
-        float nb = c->face_qn[4 * el + dl] + c->face_qn[4 * eh + dr];
+        real nb = c->face_qn[4 * el + dl] + c->face_qn[4 * eh + dr];
         if (!theta_one)
             nb = boundary_neighbor_sum(xq, c->face_qn[4 * el + dl], c->face_qn[4 * eh + dr],
                                        m->open_face[4 * el + dl], m->open_face[4 * eh + dr]);
-        float new_q = (sita * xq + half_rest * nb + xdq) / xf;
-        new_q = xwh < m->min_h ? 0.0f : new_q;
+        real new_q = (sita * xq + half_rest * nb + xdq) / xf;
+        new_q = xwh < m->min_h ? R(0.0) : new_q;
         new_q *= bf;
         m->q[si] = new_q;
     }
 
     /* donor factor (solver_compact.py:491-514) */
     uint32_t limited_cells = 0;
-    float minimum_scale = c->minimum_scale;
+    real minimum_scale = c->minimum_scale;
 #pragma omp parallel for schedule(static) reduction(+ : limited_cells) reduction(min : minimum_scale)
     for (int ei = 1; ei < m->e_num; ++ei) {
         int bi = m->boundary_id[ei];
-        float discharge = 0.0f;
+        real discharge = R(0.0);
         if (bi >= 0 && m->kind[bi] == 1) discharge = c->values[bi] * m->weight[ei];
-        float rainq = 0.0f;
+        real rainq = R(0.0);
         if (raining) rainq = c->rain_rates[m->rain_index[ei]];
-        float pipe = m->pipe_q ? m->pipe_q[ei] : 0.0f;
-        float positive = (maxf(pipe, 0.0f) + maxf(discharge, 0.0f)) * dt;
-        float available = m->depth[ei] * m->area[ei] + positive + rainq * dt * m->area[ei];
-        float outgoing = (maxf(-pipe, 0.0f) + maxf(-discharge, 0.0f)) * dt;
+        real pipe = m->pipe_q ? m->pipe_q[ei] : R(0.0);
+        real positive = (maxf(pipe, R(0.0)) + maxf(discharge, R(0.0))) * dt;
+        real available = m->depth[ei] * m->area[ei] + positive + rainq * dt * m->area[ei];
+        real outgoing = (maxf(-pipe, R(0.0)) + maxf(-discharge, R(0.0))) * dt;
         for (int d = 0; d < 4; ++d) {
             int p = m->face_ptr[4 * ei + d];
             for (int j = 0; j < m->face_count[4 * ei + d]; ++j) {
                 int side = m->isl_data[p + j];
-                float signed_q = m->q[side] * m->length[side];
+                real signed_q = m->q[side] * m->length[side];
                 if (d == 0 || d == 2) signed_q = -signed_q;
-                outgoing += maxf(signed_q, 0.0f) * dt;
+                outgoing += maxf(signed_q, R(0.0)) * dt;
             }
         }
-        c->donor_scale[ei] = 1.0f;
+        c->donor_scale[ei] = R(1.0);
         if (outgoing > available && !(bi >= 0 && m->kind[bi] == 0)) {
-            float sc = available / outgoing;
+            real sc = available / outgoing;
             c->donor_scale[ei] = sc;
             limited_cells += 1;
             minimum_scale = minf(minimum_scale, sc);
@@ -616,8 +631,8 @@ static void tick(ora_ctx *c)
 #pragma omp parallel for schedule(static) reduction(+ : limited_faces)
     for (int si = 1; si < m->s_num; ++si) {
         int el = m->topology[3 * si + 1], eh = m->topology[3 * si + 2];
-        int donor = m->q[si] >= 0.0f ? el : eh;
-        if (m->q[si] != 0.0f && c->donor_scale[donor] < 1.0f) limited_faces += 1;
+        int donor = m->q[si] >= R(0.0) ? el : eh;
+        if (m->q[si] != R(0.0) && c->donor_scale[donor] < R(1.0)) limited_faces += 1;
         m->q[si] *= c->donor_scale[donor];
     }
     c->limited_faces += limited_faces;
@@ -628,32 +643,32 @@ static void tick(ora_ctx *c)
     uint32_t wet = 0;
 #pragma omp parallel for schedule(static) reduction(+ : wet)
     for (int blk = 0; blk < c->blocks; ++blk) {
-        float *diag = (float *)calloc((size_t)BLOCK * T, sizeof(float));
+        real *diag = (real *)calloc((size_t)BLOCK * T, sizeof(real));
         int e0 = blk * BLOCK;
         for (int i = 0; i < BLOCK; ++i) {
             int ei = e0 + i;
             if (ei < 1 || ei >= m->e_num) continue;
-            float *dg = diag + (size_t)i * T;
+            real *dg = diag + (size_t)i * T;
             int bi = m->boundary_id[ei];
-            float pq = m->pipe_q ? m->pipe_q[ei] : 0.0f;
-            float pipe = maxf(pq, 0.0f) + minf(pq, 0.0f) * c->donor_scale[ei];
-            float discharge = 0.0f;
+            real pq = m->pipe_q ? m->pipe_q[ei] : R(0.0);
+            real pipe = maxf(pq, R(0.0)) + minf(pq, R(0.0)) * c->donor_scale[ei];
+            real discharge = R(0.0);
             if (bi >= 0 && m->kind[bi] == 1) {
-                float requested = c->values[bi] * m->weight[ei];
-                discharge = maxf(requested, 0.0f) + minf(requested, 0.0f) * c->donor_scale[ei];
-                if (discharge * dt != 0.0f) dg[4 + 5 * B + bi] += discharge * dt;
+                real requested = c->values[bi] * m->weight[ei];
+                discharge = maxf(requested, R(0.0)) + minf(requested, R(0.0)) * c->donor_scale[ei];
+                if (discharge * dt != R(0.0)) dg[4 + 5 * B + bi] += discharge * dt;
             }
             c->ssq[ei] = pipe + discharge;
-            float rainq = 0.0f;
+            real rainq = R(0.0);
             if (raining) rainq = c->rain_rates[m->rain_index[ei]];
-            if (rainq > 0.0f) {
+            if (rainq > R(0.0)) {
                 m->rain_time[ei] += dt;
                 m->infiltration[ei] = m->fc[ei] + (m->f0[ei] - m->fc[ei])
-                    * ora_expf(-m->k[ei] * m->rain_time[ei] / 3600.0f);
+                    * REXP(-m->k[ei] * m->rain_time[ei] / R(3600.0));
             }
-            float fl[4];
+            real fl[4];
             for (int d = 0; d < 4; ++d) {
-                float face_flux = 0.0f;
+                real face_flux = R(0.0);
                 int p = m->face_ptr[4 * ei + d];
                 for (int j = 0; j < m->face_count[4 * ei + d]; ++j) {
                     int si = m->isl_data[p + j];
@@ -661,25 +676,25 @@ static void tick(ora_ctx *c)
                 }
                 fl[d] = face_flux;
             }
-            float ql = fl[0], qr = fl[1], qb = fl[2], qt = fl[3];
-            float tq = ql - qr + qb - qt + c->ssq[ei];
+            real ql = fl[0], qr = fl[1], qb = fl[2], qt = fl[3];
+            real tq = ql - qr + qb - qt + c->ssq[ei];
             c->eq[4 * ei + 0] = ql; c->eq[4 * ei + 1] = qr; c->eq[4 * ei + 2] = qb; c->eq[4 * ei + 3] = qt;
-            float ea = m->area[ei];
-            float rain_depth = rainq * dt;
+            real ea = m->area[ei];
+            real rain_depth = rainq * dt;
             c->increment[ei] = tq * dt / ea + rain_depth;
             c->rain_depth[ei] = rain_depth;
 
             /* depth update (solver_compact.py:567-610) */
-            float previous = m->depth[ei];
-            float raw_depth = previous + c->increment[ei];
-            float removed = minf(m->infiltration[ei] * dt, maxf(raw_depth, 0.0f));
+            real previous = m->depth[ei];
+            real raw_depth = previous + c->increment[ei];
+            real removed = minf(m->infiltration[ei] * dt, maxf(raw_depth, R(0.0)));
             raw_depth -= removed;
-            float floor_v = maxf(-raw_depth, 0.0f);
+            real floor_v = maxf(-raw_depth, R(0.0));
             dg[0] += removed * ea;
             dg[3] += pipe * dt;
             if (bi >= 0 && m->kind[bi] == 0) {
                 dg[2] += floor_v * ea;
-                float target = maxf(c->level_values[bi] - m->bed[ei], 0.0f);
+                real target = maxf(c->level_values[bi] - m->bed[ei], R(0.0));
                 int off = 4 + 5 * bi;
                 dg[off] += (target - previous) * ea;
                 dg[off + 1] += -(ql - qr + qb - qt) * dt;
@@ -689,12 +704,12 @@ static void tick(ora_ctx *c)
                 m->depth[ei] = target;
             } else {
                 dg[1] += floor_v * ea;
-                m->depth[ei] = maxf(raw_depth, 0.0f);
+                m->depth[ei] = maxf(raw_depth, R(0.0));
             }
-            float u, v;
+            real u, v;
             velocity(c, ei, &u, &v);
             m->u[ei] = u; m->v[ei] = v;
-            m->max_speed[ei] = maxf(m->max_speed[ei], sqrtf(u * u + v * v));
+            m->max_speed[ei] = maxf(m->max_speed[ei], RSQRT(u * u + v * v));
             if (m->depth[ei] > m->max_depth[ei]) {
                 m->max_depth[ei] = m->depth[ei];
                 m->peak_hi[ei] = c->step_end[0]; m->peak_lo[ei] = c->step_end[1];
@@ -706,9 +721,9 @@ static void tick(ora_ctx *c)
         for (int t = 0; t < T; ++t) {
             int any = 0;
             for (int i = 0; i < BLOCK; ++i) {
-                float val = diag[(size_t)i * T + t];
+                real val = diag[(size_t)i * T + t];
                 v[i] = (double)val;
-                any |= val != 0.0f;
+                any |= val != R(0.0);
             }
             if (any) acc_add(c, (size_t)blk * T + t, block_tree(v));
         }

@@ -31,35 +31,47 @@
 
 #define ORA_TRACE_COLS 10 /* reference 9 columns + wet-cell count */
 
+/* Arithmetic type of the state and the step. The default build is F32, the
+ * reference's Taichi default_fp; the precision study compiles the same
+ * source with -DORA_REAL_DOUBLE (liboracle_f64.so), where every state array
+ * and every step operation is F64 while the clock keeps its F32 dt choice
+ * and fixed-point ticks. */
+#ifdef ORA_REAL_DOUBLE
+typedef double ora_real;
+#else
+typedef float ora_real;
+#endif
+
 typedef struct {
     int32_t e_num, s_num, b_num, n_rates, isl_len;
     int32_t batch_size;
-    float g, afa, sita, min_h, min_dt;
+    ora_real g, afa, sita, min_h;
+    float min_dt;
     /* cells [e_num] */
-    const float *x, *y, *area, *width, *height, *f0, *fc, *k;
+    const ora_real *x, *y, *area, *width, *height, *f0, *fc, *k;
     const int32_t *boundary_id, *rain_index;
     const int32_t *face_ptr, *face_count; /* [e_num*4] */
     const int32_t *isl_data;              /* [isl_len] */
-    const float *weight;                  /* [e_num] */
+    const ora_real *weight;                  /* [e_num] */
     /* sides [s_num] */
     const int32_t *topology; /* [s_num*3] */
-    const float *length, *side_n;
+    const ora_real *length, *side_n;
     const uint8_t *sbf;
     /* boundaries [max(1,b_num)] */
     const int32_t *kind;
     /* theta < 1 only: open-face fractions [e_num*4] (may be NULL when sita == 1) */
-    const float *open_face;
+    const ora_real *open_face;
     /* hanging-edge reconstruction (hang_cells == 0 when absent) */
     int32_t hang_cells, hang_edges;
     const int32_t *edge_index; /* [s_num] */
-    const float *offsets;      /* [hang_edges*2] */
+    const ora_real *offsets;      /* [hang_edges*2] */
     const int32_t *slots;      /* [hang_edges*2] */
     const int32_t *hcells;     /* [hang_cells] */
     const int32_t *axes;       /* [hang_cells*2] */
     /* mutable state (caller-owned) */
-    float *bed, *depth, *q, *rain_time, *infiltration, *max_depth, *max_speed, *u, *v;
+    ora_real *bed, *depth, *q, *rain_time, *infiltration, *max_depth, *max_speed, *u, *v;
     uint32_t *peak_hi, *peak_lo;
-    float *pipe_q; /* [e_num] or NULL (no coupling) */
+    ora_real *pipe_q; /* [e_num] or NULL (no coupling) */
 } ora_mesh;
 
 typedef struct ora_ctx ora_ctx;
@@ -72,8 +84,8 @@ void ora_set_threads(int n);
 void ora_set_clock(ora_ctx *c, const uint32_t now[2]);
 void ora_get_clock(const ora_ctx *c, uint32_t now[2]);
 void ora_set_active(ora_ctx *c, int active);
-void ora_set_forcing(ora_ctx *c, const float *coefficients, const float *rain_rates, int raining);
-void ora_apply_initial_levels(ora_ctx *c, const float *targets);
+void ora_set_forcing(ora_ctx *c, const ora_real *coefficients, const ora_real *rain_rates, int raining);
+void ora_apply_initial_levels(ora_ctx *c, const ora_real *targets);
 void ora_compute_cfl(ora_ctx *c);
 void ora_initial_diagnostics(ora_ctx *c);
 void ora_reset_extrema(ora_ctx *c);
@@ -82,16 +94,16 @@ void ora_run_batch(ora_ctx *c, const uint32_t target[2], const uint32_t origin[2
 /* one prepared physical step with an externally supplied dt (parity probes) */
 void ora_budget_flush(ora_ctx *c, double *totals /* [4+6B] */);
 int ora_budget_terms(const ora_ctx *c);
-float ora_ndt(const ora_ctx *c);
+ora_real ora_ndt(const ora_ctx *c);
 int32_t ora_cfl_arg(const ora_ctx *c);
-void ora_limits(const ora_ctx *c, float values[5], int32_t ids[3]);
+void ora_limits(const ora_ctx *c, ora_real values[5], int32_t ids[3]);
 void ora_reset_limits(ora_ctx *c);
-void ora_read_eq(const ora_ctx *c, float *eq /* [e_num*4] */);
-void ora_read_flow_depth(const ora_ctx *c, float *out /* [s_num] */);
-void ora_read_gradients(const ora_ctx *c, float *out /* [hang_cells*2] */);
+void ora_read_eq(const ora_ctx *c, ora_real *eq /* [e_num*4] */);
+void ora_read_flow_depth(const ora_ctx *c, ora_real *out /* [s_num] */);
+void ora_read_gradients(const ora_ctx *c, ora_real *out /* [hang_cells*2] */);
 /* pressure-only probe for the reference's split-face tests */
 void ora_update_pressure(ora_ctx *c);
-float ora_pressure_difference(const ora_ctx *c, int side, int lower, int higher, float raw);
+ora_real ora_pressure_difference(const ora_ctx *c, int side, int lower, int higher, ora_real raw);
 
 /* mathref.c */
 double ora_ln(double x);

@@ -65,7 +65,7 @@ def test_members_match_their_single_runs(cuda_available, grid):
     ens.close()
 
 
-def test_members_must_share_tile_and_stream(cuda_available):
+def test_members_must_share_the_tile_size(cuda_available):
     from nhflood.ensemble import tiled_factory
     from nhflood.model import StepParams
     from nhflood.native import CudaEnsemble

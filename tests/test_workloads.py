@@ -72,3 +72,24 @@ def test_ensemble_parameters_follow_the_batched_configuration():
     assert len(mm) == 60 and mm.argmax() in (29, 30)
     assert abs(mm.sum() - ps[3]['hyetograph_peak'] / 2) < 1e-3  # a 1 h triangle holds peak/2 mm
     assert w.land_parameters[2].manning_n == 0.05 * ps[3]['n_factors'][2]
+
+
+def test_served_request_stream_has_the_configured_distribution():
+    from nhflood.serving import device_bytes_estimate
+    from nhflood.workloads import multires_quadtree, quadtree_width_for, served_requests
+    reqs = served_requests()
+    assert len(reqs) == 512
+    arrivals = np.array([r['arrival'] for r in reqs])
+    assert np.all(np.diff(arrivals) > 0)
+    assert 200 < arrivals[-1] < 320  # 512 arrivals at 2 per second
+    widths = np.array([r['params']['width'] for r in reqs])
+    assert widths.min() >= quadtree_width_for(16e3) - 40 and widths.max() <= quadtree_width_for(4e6) + 40
+    d = np.array([r['params']['duration'] for r in reqs])
+    assert d.min() >= 600 and d.max() <= 3600
+    rain = np.array([r['params']['uniform_rain'] for r in reqs])
+    assert rain.min() >= 10 and rain.max() <= 100
+    w = multires_quadtree(**dict(reqs[0]['params'], width=1000.0))
+    assert w.forcing.rain.millimetres.shape[0] == 1
+    assert abs(w.forcing.rain.millimetres[0, 0] - reqs[0]['params']['uniform_rain'] * w.duration / 3600) < 1e-3
+    a = w.step_arrays()
+    assert device_bytes_estimate(a) > a.nbytes() + 40 * a.e_num
