@@ -174,15 +174,17 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
         tl.fidx = P.face_idx + off[3];
     }
     const int E = P.max_ext;
+    // The first six arrays are dead once the depth update is done; the
+    // budget reduction then reuses their 24 * E bytes.
     float *sh_h = reinterpret_cast<float *>(smem_raw);
-    float *sh_z = sh_h + E;
-    float *sh_s = sh_z + E;      // donor factor, then the new depth
-    float *sh_rq = sh_s + E;     // rain rate of the cell (0 when not raining)
+    float *sh_rq = sh_h + E;     // rain rate of the cell (0 when not raining)
     float *sh_area = sh_rq + E;
     int *sh_g = reinterpret_cast<int *>(sh_area + E);
     int *sh_bi = sh_g + E;       // boundary id, -1 for none
     uint32_t *sh_fdesc = reinterpret_cast<uint32_t *>(sh_bi + E);
-    float *sh_q = reinterpret_cast<float *>(sh_fdesc + E);  // q*, then final q
+    float *sh_z = reinterpret_cast<float *>(sh_fdesc + E);
+    float *sh_s = sh_z + E;      // donor factor, then the new depth
+    float *sh_q = sh_s + E;      // q*, then final q
     float *sh_len = sh_q + P.max_sides;
     int32_t *sh_srel = reinterpret_cast<int32_t *>(sh_len + P.max_sides);
     uint32_t *sh_lohi = reinterpret_cast<uint32_t *>(sh_srel + P.max_sides);
@@ -487,24 +489,68 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
     }
     __syncthreads();
 
-    // Budget partials: one writer per (budget block, term), fixed tree.
+    // Budget partials: one writer per (budget block, term), the canonical
+    // pairwise tree of the 256 cells of a block (stride 128 .. 1). Terms
+    // whose values some cell of the tile holds are staged together in the
+    // dead shared arrays; one warp then reduces one (block, term): lane l
+    // forms ((v[l] + v[l+128]) + (v[l+64] + v[l+192])) + ((v[l+32] + v[l+160])
+    // + (v[l+96] + v[l+224])), which are the tree's strides 128, 64 and 32,
+    // and a shuffle tree does strides 16 .. 1.
+    if (T <= 32) {
+        double *buf = reinterpret_cast<double *>(smem_raw);
+        const int cap = (24 * E) / (NT * 8);  // >= 1: the planner pads E
+        const int lane_b = tid & 31, warp_b = tid >> 5;
 #pragma unroll
-    for (int kk = 0; kk < CPT; ++kk) {
-        const int blk0 = (tl.cbase >> 8) + kk * (NT / 256);
-        uint32_t any = 0;
-        for (int hh = 0; hh < NT / 256; ++hh) any |= sh_mask[kk][hh];
-        if (T > 32) any = 0xffffffffu;
-        for (int t = 0; t < T; ++t) {
-            if (t < 32 && !((any >> t) & 1u)) continue;
-            float val = term_value(t, B, terms.removed[kk], terms.floor_v[kk], terms.level[kk], terms.discharge[kk],
-                                   terms.bi[kk], terms.kind[kk]);
-            if (T > 32 && !__syncthreads_or(val != 0.0f)) continue;
-            double sum = tree_halves<NT>((double)val, sh_tree);
-            const int blk = blk0 + (tid >> 8);
-            const bool has = T > 32 ? true : ((sh_mask[kk][tid >> 8] >> t) & 1u) != 0;
-            if ((tid & 255) == 0 && blk < d.blocks && has) {
-                if (T > 32 && sum == 0.0) continue;
-                acc_add(d.acc_sum + (size_t)blk * T + t, d.acc_comp + (size_t)blk * T + t, sum);
+        for (int kk = 0; kk < CPT; ++kk) {
+            const int blk0 = (tl.cbase >> 8) + kk * (NT / 256);
+            uint32_t any = 0;
+            for (int hh = 0; hh < NT / 256; ++hh) any |= sh_mask[kk][hh];
+            while (any) {
+                uint32_t chunk = 0;
+                int n = 0;
+                for (uint32_t rest = any; rest && n < cap; rest &= rest - 1, ++n) chunk |= rest & (0u - rest);
+                any &= ~chunk;
+                int j = 0;
+                for (uint32_t rest = chunk; rest; rest &= rest - 1, ++j) {
+                    const int t = __ffs(rest) - 1;
+                    buf[j * NT + tid] = (double)term_value(t, B, terms.removed[kk], terms.floor_v[kk], terms.level[kk],
+                                                           terms.discharge[kk], terms.bi[kk], terms.kind[kk]);
+                }
+                __syncthreads();
+                const int halves = NT / 256;
+                for (int item = warp_b; item < halves * n; item += NT / 32) {
+                    const int h = item % halves, jj = item / halves;
+                    const double *v = buf + jj * NT + h * 256;
+                    double r = ((v[lane_b] + v[lane_b + 128]) + (v[lane_b + 64] + v[lane_b + 192])) +
+                               ((v[lane_b + 32] + v[lane_b + 160]) + (v[lane_b + 96] + v[lane_b + 224]));
+                    for (int stride = 16; stride >= 1; stride >>= 1) r += __shfl_down_sync(0xffffffffu, r, stride);
+                    if (lane_b == 0) {
+                        uint32_t rest = chunk;
+                        for (int q = 0; q < jj; ++q) rest &= rest - 1;
+                        const int t = __ffs(rest) - 1;
+                        const int blk = blk0 + h;
+                        if (blk < d.blocks && ((sh_mask[kk][h] >> t) & 1u))
+                            acc_add(d.acc_sum + (size_t)blk * T + t, d.acc_comp + (size_t)blk * T + t, r);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+    // More than 32 terms (over five boundaries): one term at a time, skipped
+    // when no cell of the tile holds it.
+    if (T > 32) {
+#pragma unroll
+        for (int kk = 0; kk < CPT; ++kk) {
+            const int blk0 = (tl.cbase >> 8) + kk * (NT / 256);
+            for (int t = 0; t < T; ++t) {
+                float val = term_value(t, B, terms.removed[kk], terms.floor_v[kk], terms.level[kk],
+                                       terms.discharge[kk], terms.bi[kk], terms.kind[kk]);
+                if (!__syncthreads_or(val != 0.0f)) continue;
+                double sum = tree_halves<NT>((double)val, sh_tree);
+                const int blk = blk0 + (tid >> 8);
+                if ((tid & 255) == 0 && blk < d.blocks && sum != 0.0)
+                    acc_add(d.acc_sum + (size_t)blk * T + t, d.acc_comp + (size_t)blk * T + t, sum);
             }
         }
     }
@@ -1116,6 +1162,11 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     }
     for (int T : sizes) {
         if (plan_tiles(hm, T, patterns, tp, tc, ts, max_ext, max_sides, max_faces, reason)) return bad(reason);
+        // The budget reduction stages one term of every thread (NT doubles)
+        // in the 24 * max_ext bytes of shared arrays that are dead after the
+        // depth update; meshes smaller than a tile need the padding.
+        const int nt = T == 256 ? 256 : 512;
+        if (24 * max_ext < 8 * nt) max_ext = (8 * nt + 23) / 24;
         smem = (size_t)max_ext * 32 + (size_t)max_sides * 16 + (size_t)max_faces * 2 + 16;
         if (smem <= (size_t)kMaxSharedBytes) { tile = T; break; }
     }

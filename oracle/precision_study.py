@@ -51,22 +51,23 @@ def compare(workload, yield_step=None):
     step = yield_step or workload.yield_step
     worst = {'max_abs_m': 0.0, 'p999_abs_m': 0.0, 'rms_m': 0.0, 'time_s': 0.0, 'max_depth_m': 0.0,
              'max_depth_extrema_abs_m': 0.0}
-    steps = {}
-    while not runs['f32'].done:
+    checkpoints = list(np.arange(step, workload.duration, step)) + [float(workload.duration)]
+    for t in checkpoints:
+        # batches end at every yield time, so both runs stop exactly there
+        # (their dt sequences, and so their batch ends in between, may differ)
         for r in runs.values():
-            r.advance()
+            while r.elapsed < t - 1e-9:
+                r.advance()
         if runs['f32'].elapsed != runs['f64'].elapsed:
-            raise RuntimeError('the two runs took different batch targets')
-        t = runs['f32'].elapsed
-        if abs(t / step - round(t / step)) < 1e-9 or runs['f32'].done:
-            a = runs['f32'].engine.get('depth').astype(np.float64)[1:]
-            b = runs['f64'].engine.get('depth')[1:]
-            d = np.abs(a - b)
-            if d.max() >= worst['max_abs_m']:
-                worst.update(max_abs_m=float(d.max()), time_s=float(t))
-            worst['p999_abs_m'] = max(worst['p999_abs_m'], float(np.percentile(d, 99.9)))
-            worst['rms_m'] = max(worst['rms_m'], float(np.sqrt((d * d).mean())))
-            worst['max_depth_m'] = max(worst['max_depth_m'], float(b.max()))
+            raise RuntimeError('the two runs did not stop at the same yield time')
+        a = runs['f32'].engine.get('depth').astype(np.float64)[1:]
+        b = runs['f64'].engine.get('depth')[1:]
+        d = np.abs(a - b)
+        if d.max() >= worst['max_abs_m']:
+            worst.update(max_abs_m=float(d.max()), time_s=float(t))
+        worst['p999_abs_m'] = max(worst['p999_abs_m'], float(np.percentile(d, 99.9)))
+        worst['rms_m'] = max(worst['rms_m'], float(np.sqrt((d * d).mean())))
+        worst['max_depth_m'] = max(worst['max_depth_m'], float(b.max()))
     ea = runs['f32'].engine.get('max_depth').astype(np.float64)[1:]
     eb = runs['f64'].engine.get('max_depth')[1:]
     worst['max_depth_extrema_abs_m'] = float(np.abs(ea - eb).max())
