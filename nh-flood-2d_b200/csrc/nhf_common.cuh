@@ -33,6 +33,9 @@ struct Ctl {
 // Tile plan of the fused step (built on the host by nhf_tiled.cu).
 struct TilePlan {
     int32_t n_tiles, tile, max_ext, max_sides, cells_per_thread;
+    // per tile: n_ext, n_r0, n_r01, n_r012, n_sides, n_owned, n_qf, r0_first_offset,
+    // n_faces, cbase, sbase, then the pattern's ext, side, face_desc and face_idx offsets, 0
+    const int4 *tile_head;     // [n_tiles][4]
     const int32_t *tile_pattern, *tile_cbase, *tile_sbase;  // [n_tiles]
     const int32_t *p_counts;   // [pattern][12]: n_ext, n_r0, n_r01, n_r012, n_sides, n_owned, n_qf,
                                // r0_first_offset, n_faces, 0, 0, 0
@@ -54,6 +57,7 @@ struct Dev {
     double *acc_sum, *acc_comp;
     // second buffers of the double-buffered state (tiled form)
     float *depth_b, *q_b, *rain_time_b;
+    float2 *sdn;  // per side {centre distance, Manning n} (tiled form; filled by initialize)
     TilePlan plan;
 };
 

@@ -46,6 +46,7 @@ __global__ void k_initialize(Dev d)
     if (i >= 1 && i < m.s_num) {
         int so = m.topology[3 * i], el = m.topology[3 * i + 1], eh = m.topology[3 * i + 2];
         d.sdc[i] = so == 2 ? maxf(fabsf(m.x[eh] - m.x[el]), 0.01f) : maxf(fabsf(m.y[eh] - m.y[el]), 0.01f);
+        if (d.sdn) d.sdn[i] = make_float2(d.sdc[i], m.side_n[i]);
     }
 }
 
@@ -745,6 +746,7 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     size_t o_db = h->tiled ? take(sizeof(float) * (size_t)e) : 0;
     size_t o_qb = h->tiled ? take(sizeof(float) * (size_t)sn) : 0;
     size_t o_rb = h->tiled ? take(sizeof(float) * (size_t)e) : 0;
+    size_t o_sdn = h->tiled ? take(sizeof(float2) * (size_t)sn) : 0;
     CKC(cudaMalloc(&h->scratch, off));
     CKC(cudaMemsetAsync(h->scratch, 0, off, h->s));
     char *base = (char *)h->scratch;
@@ -784,6 +786,7 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
         d.depth_b = (float *)(base + o_db);
         d.q_b = (float *)(base + o_qb);
         d.rain_time_b = (float *)(base + o_rb);
+        d.sdn = (float2 *)(base + o_sdn);
         d.plan = h->tb.plan;
     }
     // control block initial values

@@ -38,6 +38,19 @@ namespace {
 constexpr int kMaxSharedBytes = 108 * 1024;
 constexpr uint8_t kOwned = 1, kFinal = 2;
 
+// 4-byte asynchronous global -> shared copy (no register round trip); a
+// thread waits for all of its copies with cp_async_wait_all.
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // ----------------------------------------------------------------- kernels
 
 template <int CPT>
@@ -158,20 +171,18 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
     const bool hanging = kHang == 1 || (kHang == 2 && m.hang_cells > 0);
     Tile tl;
     {
-        const int t = t_index;
-        const int pat = P.tile_pattern[t];
-        const int32_t *cnt = P.p_counts + 12 * pat;
-        const int32_t *off = P.p_offsets + 4 * pat;
-        tl.n_ext = cnt[0]; tl.n_r0 = cnt[1]; tl.n_r01 = cnt[2]; tl.n_r012 = cnt[3];
-        tl.n_sides = cnt[4]; tl.n_owned = cnt[5]; tl.n_qf = cnt[6]; tl.r0off = cnt[7];
-        tl.n_faces = cnt[8];
-        tl.cbase = P.tile_cbase[t];
-        tl.sbase = P.tile_sbase[t];
-        tl.ext = P.ext_rel + off[0];
-        tl.srel = P.side_rel + off[1];
-        tl.lohi = P.side_lohi + off[1];
-        tl.fdesc = P.face_desc + off[2];
-        tl.fidx = P.face_idx + off[3];
+        const int4 *head = P.tile_head + 4 * t_index;
+        const int4 h0 = head[0], h1 = head[1], h2 = head[2], h3 = head[3];
+        tl.n_ext = h0.x; tl.n_r0 = h0.y; tl.n_r01 = h0.z; tl.n_r012 = h0.w;
+        tl.n_sides = h1.x; tl.n_owned = h1.y; tl.n_qf = h1.z; tl.r0off = h1.w;
+        tl.n_faces = h2.x;
+        tl.cbase = h2.y;
+        tl.sbase = h2.z;
+        tl.ext = P.ext_rel + h2.w;
+        tl.srel = P.side_rel + h3.x;
+        tl.lohi = P.side_lohi + h3.x;
+        tl.fdesc = P.face_desc + h3.y;
+        tl.fidx = P.face_idx + h3.z;
     }
     const int E = P.max_ext;
     // The first six arrays are dead once the depth update is done; the
@@ -190,29 +201,49 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
     uint32_t *sh_lohi = reinterpret_cast<uint32_t *>(sh_srel + P.max_sides);
     uint16_t *sh_fidx = reinterpret_cast<uint16_t *>(sh_lohi + P.max_sides);
 
-    // P0: stage the tile's index tables (contiguous per pattern) and, for the
-    // tile and its rings, depth and bed; cells of rings 0..2 also bring the
-    // per-cell inputs of the donor factor and the depth update.
-    for (int i = tid; i < tl.n_sides; i += NT) { sh_srel[i] = tl.srel[i]; sh_lohi[i] = tl.lohi[i]; }
-    for (int i = tid; i <= tl.n_r012; i += NT) sh_fdesc[i] = tl.fdesc[i];
-    for (int i = tid; i < tl.n_faces; i += NT) sh_fidx[i] = tl.fidx[i];
+    // P0: stage the tile in two asynchronous phases. (a) The pattern's index
+    // tables (contiguous in global memory; the ring list goes to sh_g for now).
+    for (int i = tid; i < tl.n_ext; i += NT) cp_async4(sh_g + i, tl.ext + i);
+    for (int i = tid; i < tl.n_sides; i += NT) {
+        cp_async4(sh_srel + i, tl.srel + i);
+        cp_async4(sh_lohi + i, tl.lohi + i);
+    }
+    for (int i = tid; i <= tl.n_r012; i += NT) cp_async4(sh_fdesc + i, tl.fdesc + i);
+    for (int i = tid; i < (tl.n_faces + 1) >> 1; i += NT)  // patterns keep an even length
+        cp_async4(reinterpret_cast<uint32_t *>(sh_fidx) + i, reinterpret_cast<const uint32_t *>(tl.fidx) + i);
+    cp_async_wait_all();
+    __syncthreads();
+    // (b) Gathers: depth and bed of the tile and its rings, the per-cell
+    // inputs of rings 0..2 (the rain pixel index parks in sh_rq), and q and
+    // length of every local side.
     for (int i = tid; i < tl.n_ext; i += NT) {
-        int g = i ? tl.cbase + tl.ext[i] : 0;
+        const int g = i ? tl.cbase + sh_g[i] : 0;
         sh_g[i] = g;
-        sh_h[i] = i ? depth_in[g] : m.depth[0];
-        sh_z[i] = m.bed[g];
+        if (i) cp_async4(sh_h + i, depth_in + g);
+        else sh_h[0] = m.depth[0];
+        cp_async4(sh_z + i, m.bed + g);
         sh_s[i] = 0.0f;  // donor_scale of the exterior sentinel stays 0
         if (i >= 1 && i <= tl.n_r012) {
-            sh_area[i] = m.area[g];
-            sh_bi[i] = m.boundary_id[g];
-            sh_rq[i] = raining ? d.rain_rates[m.rain_index[g]] : 0.0f;
+            cp_async4(sh_area + i, m.area + g);
+            cp_async4(sh_bi + i, m.boundary_id + g);
+            cp_async4(sh_rq + i, m.rain_index + g);
         }
+    }
+    for (int j = tid; j < tl.n_sides; j += NT) {
+        const int gid = tl.sbase + sh_srel[j];
+        cp_async4(sh_q + j, q_in + gid);
+        cp_async4(sh_len + j, m.length + gid);
     }
     tl.srel = sh_srel;
     tl.lohi = sh_lohi;
     tl.fdesc = sh_fdesc;
     tl.fidx = sh_fidx;
+    cp_async_wait_all();
     __syncthreads();
+    for (int i = 1 + tid; i <= tl.n_r012; i += NT) {
+        const int pixel = __float_as_int(sh_rq[i]);
+        sh_rq[i] = raining ? d.rain_rates[pixel] : 0.0f;
+    }
 
     // P1: momentum (solver_compact.py:439-486) for every local side. A side
     // whose flow height is below min_h gets q = +0 whatever its other inputs
@@ -221,16 +252,18 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
         const int gid = tl.sbase + tl.srel[j];
         const uint32_t lh = tl.lohi[j];
         const int a = (int)(lh & 0xffffu), b = (int)(lh >> 16);
-        float len = m.length[gid];
         float zl = sh_z[a], zh = sh_z[b];
         float hl = zl + sh_h[a], hr = zh + sh_h[b];
         float xwh = maxf(hl, hr) - maxf(maxf(zl, zh), kDh);
         float new_q = 0.0f;
         if (!(xwh < d.min_h)) {
-            float xq = q_in[gid];
-            float dx = d.sdc[gid];
-            float n = m.side_n[gid];
-            float bf = m.sbf[gid] == 1 ? 0.0f : 1.0f;
+            float xq = sh_q[j];
+            const float2 sdn = d.sdn[gid];
+            float dx = sdn.x;
+            float n = sdn.y;
+            // exterior sides (exactly one neighbour, the sentinel slot 0) are closed
+            // (sbf, build_boundary_fdb in domain.py:472-479; checked by the planner)
+            float bf = (a == 0) != (b == 0) ? 0.0f : 1.0f;
             float difference = hr - hl;
             if (hanging) {
                 int index = m.edge_index[gid];
@@ -259,7 +292,6 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
             new_q *= bf;
         }
         sh_q[j] = new_q;
-        sh_len[j] = len;
     }
     __syncthreads();
 
@@ -758,6 +790,7 @@ bool same(const Pattern &a, const Pattern &b)
 struct HostMesh {
     int e, s;
     std::vector<int32_t> topo, fptr, fcnt, isl;
+    std::vector<uint8_t> sbf;
 };
 
 int copy_back(const nhf_mesh &m, cudaStream_t st, HostMesh &hm)
@@ -767,7 +800,9 @@ int copy_back(const nhf_mesh &m, cudaStream_t st, HostMesh &hm)
     hm.fptr.resize((size_t)m.e_num * 4);
     hm.fcnt.resize((size_t)m.e_num * 4);
     hm.isl.resize((size_t)(m.isl_len > 0 ? m.isl_len : 1));
+    hm.sbf.resize((size_t)m.s_num);
     if (cudaMemcpyAsync(hm.topo.data(), m.topology, hm.topo.size() * 4, cudaMemcpyDeviceToHost, st) ||
+        cudaMemcpyAsync(hm.sbf.data(), m.sbf, hm.sbf.size(), cudaMemcpyDeviceToHost, st) ||
         cudaMemcpyAsync(hm.fptr.data(), m.face_ptr, hm.fptr.size() * 4, cudaMemcpyDeviceToHost, st) ||
         cudaMemcpyAsync(hm.fcnt.data(), m.face_count, hm.fcnt.size() * 4, cudaMemcpyDeviceToHost, st) ||
         (m.isl_len > 0 && cudaMemcpyAsync(hm.isl.data(), m.isl_data, (size_t)m.isl_len * 4, cudaMemcpyDeviceToHost, st)) ||
@@ -797,6 +832,8 @@ bool consistent(const HostMesh &hm, std::string &why)
         int lo = hm.topo[3 * sid + 1], hi = hm.topo[3 * sid + 2];
         int expect = (lo != 0) + (hi != 0);
         if (expect == 0 || listed[sid] != expect || lo == hi) { why = "a side is not listed by exactly its cells"; return false; }
+        // the fused step derives the closed-edge flag from the topology
+        if (hm.sbf[sid] != ((lo == 0) != (hi == 0) ? 1 : 0)) { why = "sbf differs from the exterior-side rule"; return false; }
     }
     return true;
 }
@@ -1186,8 +1223,19 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
         lohi.insert(lohi.end(), p.lohi.begin(), p.lohi.end());
         fdesc.insert(fdesc.end(), p.fdesc.begin(), p.fdesc.end());
         fidx.insert(fidx.end(), p.fidx.begin(), p.fidx.end());
+        if (fidx.size() & 1) fidx.push_back(0);  // the kernel copies face indices in pairs
     }
-    if (fidx.empty()) fidx.push_back(0);
+    if (fidx.empty()) { fidx.push_back(0); fidx.push_back(0); }
+    // per-tile header: the pattern's counts and offsets with the tile's bases
+    std::vector<int32_t> head((size_t)tp.size() * 16, 0);
+    for (size_t t = 0; t < tp.size(); ++t) {
+        const int32_t *cnt = counts.data() + 12 * (size_t)tp[t];
+        const int32_t *off = offsets.data() + 4 * (size_t)tp[t];
+        int32_t *h = head.data() + 16 * t;
+        for (int k = 0; k < 9; ++k) h[k] = cnt[k];
+        h[9] = tc[t]; h[10] = ts[t];
+        h[11] = off[0]; h[12] = off[1]; h[13] = off[2]; h[14] = off[3];
+    }
     if (srel.empty()) { srel.push_back(0); lohi.push_back(0); }
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
@@ -1195,6 +1243,7 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     size_t o_cnt = take(counts.size() * 4), o_off = take(offsets.size() * 4), o_ext = take(ext.size() * 4);
     size_t o_srel = take(srel.size() * 4), o_lohi = take(lohi.size() * 4), o_fd = take(fdesc.size() * 4);
     size_t o_fi = take(fidx.size() * 2);
+    size_t o_hd = take(head.size() * 4);
     void *mem = nullptr;
     if (cudaMalloc(&mem, off) != cudaSuccess) return bad("allocating the tile plan failed");
     char *b = (char *)mem;
@@ -1206,6 +1255,7 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
               up(o_off, offsets.data(), offsets.size() * 4) && up(o_ext, ext.data(), ext.size() * 4) &&
               up(o_srel, srel.data(), srel.size() * 4) && up(o_lohi, lohi.data(), lohi.size() * 4) &&
               up(o_fd, fdesc.data(), fdesc.size() * 4) && up(o_fi, fidx.data(), fidx.size() * 2) &&
+              up(o_hd, head.data(), head.size() * 4) &&
               cudaStreamSynchronize(s) == cudaSuccess;
     if (!ok) { cudaFree(mem); return bad("uploading the tile plan failed"); }
     TilePlan &P = out->plan;
@@ -1214,6 +1264,7 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     P.max_ext = max_ext;
     P.max_sides = max_sides;
     P.cells_per_thread = tile == 1024 ? 2 : 1;
+    P.tile_head = (const int4 *)(b + o_hd);
     P.tile_pattern = (const int32_t *)(b + o_tp);
     P.tile_cbase = (const int32_t *)(b + o_tc);
     P.tile_sbase = (const int32_t *)(b + o_ts);
