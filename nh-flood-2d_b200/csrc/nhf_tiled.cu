@@ -36,6 +36,14 @@ namespace nhf {
 namespace {
 
 constexpr int kMaxSharedBytes = 108 * 1024;
+// Resident blocks per SM the register budget is sized for: 5 x 256 threads
+// (48 registers) for 256-cell tiles, 2 x 512 threads (64) for larger ones.
+template <int NT>
+constexpr int kMinBlocks = NT == 256 ? 5 : 2;
+// The ensemble step reads its descriptor from shared memory and needs more
+// registers: 4 x 256 or 2 x 512 threads (64 registers).
+template <int NT>
+constexpr int kEnsembleMinBlocks = NT == 256 ? 4 : 2;
 constexpr uint8_t kOwned = 1, kFinal = 2;
 
 // 4-byte asynchronous global -> shared copy (no register round trip); a
@@ -118,8 +126,10 @@ __device__ __forceinline__ float term_value(int t, int B, float removed, float f
     if (t == 2) return kind == 0 ? floor_v : 0.0f;
     if (t == 3) return 0.0f;  // pipe exchange: no coupling
     if (t < 4 + 5 * B) {
-        int b = (t - 4) / 5;
-        return (b == bi && kind == 0) ? level[(t - 4) % 5] : 0.0f;
+        const int b = (t - 4) / 5, q = (t - 4) % 5;
+        if (b != bi || kind != 0) return 0.0f;
+        // selected without a dynamic index, so the terms stay in registers
+        return q == 0 ? level[0] : q == 1 ? level[1] : q == 2 ? level[2] : q == 3 ? level[3] : level[4];
     }
     return (t - 4 - 5 * B == bi) ? discharge : 0.0f;
 }
@@ -654,7 +664,7 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
 }
 
 template <bool kThetaOne, bool kHanging, int NT, int CPT>
-__global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(const __grid_constant__ Dev d)
+__global__ void __launch_bounds__(NT, kMinBlocks<NT>) k_step_tiled(const __grid_constant__ Dev d)
 {
     step_tile<kThetaOne, kHanging ? 1 : 0, NT, CPT>(d, blockIdx.x, gridDim.x);
 }
@@ -664,7 +674,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_step_tiled(const __grid_const
 // takes items blockIdx.x, + gridDim.x, ...) or one block per item. The
 // member's descriptor is staged in shared memory once per change of member.
 template <bool kThetaOne, int NT, int CPT>
-__global__ void __launch_bounds__(NT, 1024 / NT) k_step_ensemble(const Dev *devs, const int2 *items, int n_items)
+__global__ void __launch_bounds__(NT, kEnsembleMinBlocks<NT>) k_step_ensemble(const Dev *devs, const int2 *items, int n_items)
 {
     __shared__ __align__(16) Dev sd;
     int current = -1;
@@ -1189,8 +1199,11 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     int max_ext = 0, max_sides = 0, max_faces = 0, tile = 0;
     size_t smem = 0;
     // Small meshes take small tiles so that every SM gets work.
+    // Multi-resolution meshes (irregular halos, more work per cell) run best
+    // with 256-cell tiles and five blocks per SM; on uniform meshes large
+    // tiles amortise the halo.
     std::vector<int> sizes = {1024, 512, 256};
-    if (m.e_num < 148 * 2 * 1024) sizes = {256};
+    if (m.e_num < 148 * 2 * 1024 || m.hang_cells > 0) sizes = {256, 512, 1024};
     else if (m.e_num < 148 * 4 * 1024) sizes = {512, 256};
     if (tile_request) {
         if (tile_request != 256 && tile_request != 512 && tile_request != 1024)

@@ -78,6 +78,7 @@ def library(precision: str = 'f32'):
             ('ora_initial_diagnostics', None, [H]), ('ora_reset_extrema', None, [H]),
             ('ora_run_batch', None, [H, U2, U2, U2]), ('ora_budget_flush', None, [H, POINTER(c_double)]),
             ('ora_budget_terms', c_int, [H]), ('ora_ndt', R, [H]), ('ora_cfl_arg', c_int32, [H]),
+            ('ora_set_ndt', None, [H, c_float]),
             ('ora_limits', None, [H, RP, POINTER(c_int32)]), ('ora_reset_limits', None, [H]),
             ('ora_read_eq', None, [H, RP]), ('ora_read_flow_depth', None, [H, RP]),
             ('ora_read_gradients', None, [H, RP]), ('ora_update_pressure', None, [H]),
@@ -214,6 +215,13 @@ class OracleEngine:
         fd = np.zeros(self.arrays.s_num, self.real)
         self.lib.ora_read_flow_depth(self.h, self._ptr(fd))
         return float(self.lib.ora_ndt(self.h)), si, float(fd[si])
+
+    def ndt(self) -> float:
+        return float(self.lib.ora_ndt(self.h))
+
+    def set_ndt(self, value: float) -> None:
+        """Precision study only: the CFL candidate the next step uses."""
+        self.lib.ora_set_ndt(self.h, float(value))
 
     def limits(self):
         values = np.zeros(5, self.real)

@@ -7,7 +7,7 @@ the same source with real = double, the clock unchanged) is the error of the
 GPU's F32 state. Both runs take the same batch targets; at every yield time
 the depths are compared cell by cell.
 
-    python oracle/precision_study.py [--out FILE] [--cases NAMES]
+    python oracle/precision_study.py [--same-dt] [--out FILE] [--cases NAMES]
 
 Cases (the configurations' workloads; the large uniform grid is run at
 512 x 512 cells with the same 1 m spacing, because its full 16.8M-cell,
@@ -45,9 +45,16 @@ def cases():
     }
 
 
-def compare(workload, yield_step=None):
+def compare(workload, same_dt: bool = False, yield_step=None):
+    """Max/99.9th/RMS |h32 - h64| over all cells at every yield time. With
+    same_dt the F64 run takes the F32 run's CFL candidate before every step
+    (one step per batch), so both integrate with the identical dt sequence
+    and the difference is the arithmetic's alone; otherwise each run picks
+    its own dt, as a real F64 build would."""
     from nhflood.plain import PlainRun
-    runs = {p: PlainRun(workload, lambda a, q, p=p: OracleEngine(a, q, precision=p)) for p in ('f32', 'f64')}
+    bs = 1 if same_dt else 32
+    runs = {p: PlainRun(workload, lambda a, q, p=p: OracleEngine(a, q, precision=p), batch_size=bs)
+            for p in ('f32', 'f64')}
     step = yield_step or workload.yield_step
     worst = {'max_abs_m': 0.0, 'p999_abs_m': 0.0, 'rms_m': 0.0, 'time_s': 0.0, 'max_depth_m': 0.0,
              'max_depth_extrema_abs_m': 0.0}
@@ -55,9 +62,15 @@ def compare(workload, yield_step=None):
     for t in checkpoints:
         # batches end at every yield time, so both runs stop exactly there
         # (their dt sequences, and so their batch ends in between, may differ)
-        for r in runs.values():
-            while r.elapsed < t - 1e-9:
-                r.advance()
+        if same_dt:
+            while runs['f32'].elapsed < t - 1e-9:
+                runs['f64'].engine.set_ndt(runs['f32'].engine.ndt())
+                runs['f32'].advance()
+                runs['f64'].advance()
+        else:
+            for r in runs.values():
+                while r.elapsed < t - 1e-9:
+                    r.advance()
         if runs['f32'].elapsed != runs['f64'].elapsed:
             raise RuntimeError('the two runs did not stop at the same yield time')
         a = runs['f32'].engine.get('depth').astype(np.float64)[1:]
@@ -81,6 +94,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--out', default=None)
     ap.add_argument('--cases', default=','.join(cases()))
+    ap.add_argument('--same-dt', action='store_true', help='F64 follows the F32 dt sequence')
     args = ap.parse_args()
     table = {}
     for name in args.cases.split(','):
@@ -89,7 +103,7 @@ def main():
         members = made if isinstance(made, list) else [made]
         rows = []
         for w in members:
-            worst, steps = compare(w)
+            worst, steps = compare(w, same_dt=args.same_dt)
             rows.append(dict(workload=w.name, cells=w.cells, duration_s=w.duration, steps_f32=steps['f32'],
                              steps_f64=steps['f64'], **worst))
         table[name] = dict(members=rows, seconds=round(time.perf_counter() - t0, 1))

@@ -138,6 +138,7 @@ void ora_get_clock(const ora_ctx *c, uint32_t now[2]) { now[0] = c->now[0]; now[
 void ora_set_active(ora_ctx *c, int active) { c->active = active; }
 int ora_budget_terms(const ora_ctx *c) { return c->terms; }
 real ora_ndt(const ora_ctx *c) { return c->ndt; }
+void ora_set_ndt(ora_ctx *c, float ndt) { c->ndt = ndt; }
 int32_t ora_cfl_arg(const ora_ctx *c) { return c->cfl_arg; }
 
 void ora_limits(const ora_ctx *c, real values[5], int32_t ids[3])

@@ -95,6 +95,8 @@ void ora_run_batch(ora_ctx *c, const uint32_t target[2], const uint32_t origin[2
 void ora_budget_flush(ora_ctx *c, double *totals /* [4+6B] */);
 int ora_budget_terms(const ora_ctx *c);
 ora_real ora_ndt(const ora_ctx *c);
+/* precision study only: replace the CFL candidate of the next step */
+void ora_set_ndt(ora_ctx *c, float ndt);
 int32_t ora_cfl_arg(const ora_ctx *c);
 void ora_limits(const ora_ctx *c, ora_real values[5], int32_t ids[3]);
 void ora_reset_limits(ora_ctx *c);
