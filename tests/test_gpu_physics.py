@@ -45,3 +45,12 @@ def test_coarse_fine_channel_bit_exact(tmp_path, cuda_available, theta, path):
     _, a, _ = channel_case(tmp_path / 'oracle', theta)
     _, b, _ = channel_case(tmp_path / 'cuda', theta, engine=cuda_engine(path))
     assert_runs_identical(a, b)
+
+
+@pytest.mark.parametrize('path', PATHS)
+@pytest.mark.parametrize('theta', [0.7, 1.0])
+def test_open_channel_bit_exact(tmp_path, cuda_available, theta, path):
+    from test_oracle_physics import open_boundary_case
+    a = open_boundary_case(tmp_path / 'oracle', 'channel', theta, .1)[0]
+    b = open_boundary_case(tmp_path / 'cuda', 'channel', theta, .1, engine=cuda_engine(path))[0]
+    assert_runs_identical(a, b)

@@ -1,8 +1,10 @@
 """Known answers of the reference's physics tests, restated on the CPU
 restatement of the step (the oracle): donor-factor positivity
 (tests/test_positivity.py:116-160), hanging-interface pressure
-reconstruction (tests/test_pressure_gradient.py:98-151) and the coarse/fine
-channel's steady uniform flow (tests/test_face_flux.py:245-271). The meshes
+reconstruction (tests/test_pressure_gradient.py:98-151), the coarse/fine
+channel's steady uniform flow (tests/test_face_flux.py:245-271), and the
+open boundaries' steady channel outflow and tidal basin
+(tests/test_open_boundary.py:208-262). The meshes
 and seed states are rebuilt here from the reference tests' descriptions; the
 tolerances are the reference's."""
 import csv
@@ -200,3 +202,81 @@ def test_coarse_fine_channel_reaches_continuous_steady_flow(tmp_path, theta):
     assert interface == pytest.approx(1, abs=.02)
     b = r.budget
     assert abs(b['residual_m3']) / (b['initial_storage_m3'] + b['discharge:upstream_m3']) < 1e-4
+
+
+# ----------------------------------------------------------- open boundaries
+
+PERIOD = 86_400
+
+
+def open_boundary_case(path: Path, kind: str, theta: float, afa: float, engine='oracle'):
+    """A flat 40 x 2 strip: a channel between a 10 m3/s inflow and a 1 m level
+    (10 m cells, 6000 s), or a basin driven by a daily 1 m tide at its west
+    edge (100 m cells, two days); tests/test_open_boundary.py:135-205."""
+    from scenarios import strip_grid_mesh
+    path.mkdir(parents=True)
+    nx, ny = 40, 2
+    dx = 10 if kind == 'channel' else 100
+    duration = 6_000 if kind == 'channel' else 2 * PERIOD
+    strip_grid_mesh(path, nx, ny, dx)
+    rain = write_rain(path, [[[0]]], from_origin(0, ny * dx, nx * dx, ny * dx), [(0, duration)])
+    definitions = ([('upstream', 'discharge', 0, 10.), ('downstream', 'level', nx * dx, 1.)]
+                   if kind == 'channel' else [('sea', 'level', 0, None)])
+    boundaries = []
+    for name, bkind, x, constant in definitions:
+        if constant is not None:
+            rows = [(0, constant), (duration, constant)]
+        else:
+            rows = [(s, 3 + np.sin(2 * np.pi * s / PERIOD)) for s in range(0, duration + 300, 300)]
+        boundaries.append(dict(name=name, kind=bkind, line=write_line(path / f'{name}.geojson', [[x, .1], [x, ny * dx - .1]]),
+                               series=write_series(path / f'{name}.csv', rows)))
+    depth = np.r_[0., np.full(nx * ny, 1. if kind == 'channel' else 3.)].astype(np.float32)
+    seed = seed_checkpoint(path / 'seed.fdb', path / 'ne.txt', path / 'ns.txt', depth=depth)
+    dc = domain(path, duration=duration, yield_step=500 if kind == 'channel' else 600, restart=seed,
+                sita=theta, afa=afa)
+    r = run(dc, ForceConfig(boundaries=boundaries, rainfall=rain), engine)
+    from nhflood.output import list_depth_frames
+    return r, list_depth_frames(dc.output_dir), nx, ny, Path(dc.output_dir)
+
+
+def test_open_channel_steady_profile_is_stable_across_theta_and_time_step(tmp_path):
+    from nhflood.output import read_bed_at, read_depth_frame
+    profiles = []
+    for theta in (1., .7):
+        for afa in (.4, .1):
+            r, frames, nx, ny, out = open_boundary_case(tmp_path / f'ch_{theta}_{afa}', 'channel', theta, afa)
+            eta = [(read_bed_at(out, s) + read_depth_frame(f))[1:].reshape(ny, nx) for s, f in frames[-3:]]
+            profile = eta[-1].mean(axis=0)
+            profiles.append(profile)
+            assert abs(profile[0] - profile[1]) < .005
+            assert abs(profile[-2] - profile[-1]) < .005
+            assert np.max(np.abs(eta[-1] - eta[-2])) < 2e-4
+            rows = list(csv.DictReader((r.path / 'mass_balance.csv').open()))
+            outflow = [-(float(b['level:downstream_m3']) - float(a['level:downstream_m3']))
+                       / (float(b['elapsed_seconds']) - float(a['elapsed_seconds']))
+                       for a, b in zip(rows[-3:-1], rows[-2:])]
+            assert all(abs(q - 10.) < .01 for q in outflow), (theta, afa, outflow)
+            b = r.budget
+            assert abs(b['residual_m3']) / (b['initial_storage_m3'] + b['discharge:upstream_m3']) < 1e-4
+    assert np.ptp(np.stack(profiles), axis=0).max() < 2e-4
+
+
+def test_tidal_basin_keeps_amplitude_and_phase_across_time_steps(tmp_path):
+    from nhflood.output import read_depth_frame
+    metrics = []
+    omega = 2 * np.pi / PERIOD
+    for afa in (.04, .015):
+        _, frames, nx, _, _ = open_boundary_case(tmp_path / f'tide_{afa}', 'tide', .7, afa)
+        t = np.array([s for s, _ in frames], float)
+        y = np.array([float(read_depth_frame(f)[nx]) for _, f in frames])
+        last = t >= PERIOD
+        t, y = t[last], y[last]
+        basis = np.column_stack([np.sin(omega * t), np.cos(omega * t), np.ones(len(t)), (t - t.mean()) / PERIOD])
+        sine, cosine, _, _ = np.linalg.lstsq(basis, y, rcond=None)[0]
+        amplitude = float(np.hypot(sine, cosine))
+        phase_minutes = float(np.arctan2(-cosine, sine) / omega / 60)
+        metrics.append((amplitude, phase_minutes))
+        assert abs(amplitude - 1.) < .01
+        assert abs(phase_minutes) < 2.
+    assert abs(metrics[0][0] - metrics[1][0]) < .002
+    assert abs(metrics[0][1] - metrics[1][1]) < .1
