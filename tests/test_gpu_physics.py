@@ -54,3 +54,13 @@ def test_open_channel_bit_exact(tmp_path, cuda_available, theta, path):
     a = open_boundary_case(tmp_path / 'oracle', 'channel', theta, .1)[0]
     b = open_boundary_case(tmp_path / 'cuda', 'channel', theta, .1, engine=cuda_engine(path))[0]
     assert_runs_identical(a, b)
+
+
+@pytest.mark.parametrize('path', PATHS)
+def test_restart_continues_bitwise_on_the_gpu(tmp_path, cuda_available, path):
+    from test_oracle_restart import restart_continues_bitwise
+    full_o, resumed_o = restart_continues_bitwise(tmp_path / 'oracle', 'oracle')
+    full_c, resumed_c = restart_continues_bitwise(tmp_path / 'cuda', cuda_engine(path))
+    np.testing.assert_array_equal(full_o.trace, full_c.trace)
+    np.testing.assert_array_equal(resumed_o.trace, resumed_c.trace)
+    assert full_o.budget == full_c.budget
