@@ -280,3 +280,21 @@ def test_tidal_basin_keeps_amplitude_and_phase_across_time_steps(tmp_path):
         assert abs(phase_minutes) < 2.
     assert abs(metrics[0][0] - metrics[1][0]) < .002
     assert abs(metrics[0][1] - metrics[1][1]) < .1
+
+
+# ------------------------------------------------------ inventory rounding
+
+def test_transport_and_small_rain_have_one_inventory_rounding(tmp_path):
+    """Rain and the face transport join before the one F32 rounding of the
+    depth (tests/test_inventory_rounding.py:19-54)."""
+    from scenarios import two_cell_mesh
+    two_cell_mesh(tmp_path, connected=True)
+    mm = np.float32(1.4911491234670393e-5)
+    rain = write_rain(tmp_path, [[[mm, 0]]], from_origin(0, 10, 10, 10), [(0, 1)])
+    depth = np.array([0, .5, .4], np.float32)
+    seed = seed_checkpoint(tmp_path / 'seed.fdb', tmp_path / 'ne.txt', tmp_path / 'ns.txt', depth=depth)
+    r = run(domain(tmp_path, duration=1, restart=seed), ForceConfig(boundaries=[], rainfall=rain), 'oracle')
+    assert r.manifest['steps'] == 1
+    rain_rate = float(np.float32(float(mm) * .001))
+    ideal = float(depth[1]) - float(r.state.q[2]) * 10 / 100 + rain_rate
+    assert abs(float(r.state.depth[1]) - ideal) < .55 * float(np.spacing(np.float32(ideal)))
