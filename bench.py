@@ -57,6 +57,11 @@ def algorithmic_bytes(w):
     return b
 
 
+# DRAM bytes (read + write) of one fused step launch, from the ncu captures
+# summarised in profiles/ (k_step_tiled_<workload>.md).
+TRAFFIC_PER_LAUNCH = {'multires_quadtree': 160.490752e6 + 18.082304e6}
+
+
 def make_workload(name):
     from nhflood import workloads
     if name == 'plain_uniform_256':
@@ -452,7 +457,10 @@ def main():
                        'parallelism': f'replicas{world}'},
             'gpu_launches': launches,
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                         'frac': achieved / peak if achieved else None, 'traffic': None,
+                         'frac': achieved / peak if achieved else None,
+                         'traffic': TRAFFIC_PER_LAUNCH.get(w.name),
+                         'traffic_unit': 'bytes per step launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)',
+                         'algorithmic_bytes_per_launch': b_alg * w.cells,
                          'peak_kind': kind, 'algorithmic_bytes_per_cell_update': b_alg,
                          'scope': 'whole batch graph (fused step kernel + per-batch epilogue)'},
             'e2e': {'value': e2e, 'unit': METRIC, 'h2d_bytes_per_step': h2d // max(1, e2e_batches),
