@@ -140,7 +140,6 @@ template <bool kThetaOne, int kHang, int NT, int CPT>
 __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const unsigned n_tiles)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double sh_tree[NT];
     __shared__ unsigned long long sh_min[NT / 32];
     __shared__ uint32_t sh_cnt[3];
     __shared__ uint32_t sh_minbits;
@@ -589,7 +588,8 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
                 float val = term_value(t, B, terms.removed[kk], terms.floor_v[kk], terms.level[kk],
                                        terms.discharge[kk], terms.bi[kk], terms.kind[kk]);
                 if (!__syncthreads_or(val != 0.0f)) continue;
-                double sum = tree_halves<NT>((double)val, sh_tree);
+                // the tree's NT doubles live in the dead shared arrays (24 * E >= 8 * NT)
+                double sum = tree_halves<NT>((double)val, reinterpret_cast<double *>(smem_raw));
                 const int blk = blk0 + (tid >> 8);
                 if ((tid & 255) == 0 && blk < d.blocks && sum != 0.0)
                     acc_add(d.acc_sum + (size_t)blk * T + t, d.acc_comp + (size_t)blk * T + t, sum);

@@ -142,3 +142,30 @@ def test_multires_quadtree_bit_exact(tmp_path, cuda_available, path):
                                 list_depth_frames(tmp_path / 'cuda' / 'output')):
         np.testing.assert_array_equal(read_depth_frame(pa).view(np.uint32), read_depth_frame(pb).view(np.uint32))
     assert row_a == row_b
+
+
+@pytest.mark.parametrize('path', PATHS)
+def test_six_boundaries_use_the_wide_budget_bit_exact(tmp_path, cuda_available, path):
+    """4 + 6 x 6 = 40 budget terms (more than the 32-term mask of the fused
+    step): three level and three discharge boundaries on a 24 x 4 strip."""
+    from nhflood.input import ForceConfig
+    from nhflood.raster import from_origin
+    from scenarios import strip_grid_mesh, write_line, write_rain, write_series
+    results = []
+    for engine in ('oracle', cuda_engine(path)):
+        d = tmp_path / ('oracle' if engine == 'oracle' else 'cuda')
+        d.mkdir()
+        strip_grid_mesh(d, 24, 4, 10)
+        rain = write_rain(d, [[[20.]], [[0.]]], from_origin(0, 40, 240, 40), [(0, 150), (150, 300)])
+        boundaries = []
+        for k in range(3):
+            boundaries.append(dict(name=f'q{k}', kind='discharge',
+                                   line=write_line(d / f'q{k}.geojson', [[80 * k + 5, 0], [80 * k + 35, 0]]),
+                                   series=write_series(d / f'q{k}.csv', [(0, .5 + k), (300, .2)])))
+            boundaries.append(dict(name=f'h{k}', kind='level',
+                                   line=write_line(d / f'h{k}.geojson', [[80 * k + 5, 40], [80 * k + 35, 40]]),
+                                   series=write_series(d / f'h{k}.csv', [(0, .3 * k), (300, .1)])))
+        dc = domain(d, duration=300, yield_step=60)
+        results.append(run(dc, ForceConfig(boundaries=boundaries, rainfall=rain), engine))
+    assert_runs_identical(*results)
+    assert results[0].manifest["steps"] > 100 and sum(k.startswith("level:") for k in results[0].budget) == 3
