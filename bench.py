@@ -62,6 +62,22 @@ def algorithmic_bytes(w):
 TRAFFIC_PER_LAUNCH = {'multires_quadtree': 160.490752e6 + 18.082304e6}
 
 
+def combine_ranks(times, units, device, world):
+    """Whole-job figures over the replicas: the slowest rank's times (max)
+    and the units of all ranks (sum). times, units: equal-length lists of
+    this rank's seconds (or ms) and processed units; returns both lists
+    reduced over the process group (unchanged when world == 1)."""
+    if world <= 1:
+        return list(times), list(units)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x) for x in times], dtype=torch.float64, device=device)
+    u = torch.tensor([float(x) for x in units], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return t.tolist(), u.tolist()
+
+
 def make_workload(name):
     from nhflood import workloads
     if name == 'plain_uniform_256':
@@ -211,13 +227,8 @@ def bench_batched(args, rank, world, local):
         h2d += ens.h2d_bytes
     torch.cuda.synchronize(device)
     e2e_s = time.perf_counter() - t0
-    stats = torch.tensor([device_s, float(cell_updates), e2e_s, float(e2e_cells)], dtype=torch.float64, device=device)
-    if world > 1:
-        import torch.distributed as dist
-        mx, sm = stats.clone(), stats.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        device_s, e2e_s, cell_updates, e2e_cells = float(mx[0]), float(mx[2]), float(sm[1]), float(sm[3])
+    (device_s, e2e_s), (cell_updates, e2e_cells) = combine_ranks([device_s, e2e_s], [cell_updates, e2e_cells],
+                                                                 device, world)
     value = cell_updates / device_s
     plain = plain_cells / plain_s if plain_s else None
     if rank == 0:
@@ -431,14 +442,8 @@ def main():
         e2e_cells += run.finish(rows) * w.cells
     torch.cuda.synchronize(device)
     e2e_s = time.perf_counter() - t0
-    stats = torch.tensor([device_ms, float(cell_steps), e2e_s, float(e2e_cells)], dtype=torch.float64, device=device)
-    if world > 1:
-        mx = stats.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = stats.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        device_ms, e2e_s = float(mx[0]), float(mx[2])
-        cell_steps, e2e_cells = float(sm[1]), float(sm[3])
+    (device_ms, e2e_s), (cell_steps, e2e_cells) = combine_ranks([device_ms, e2e_s], [cell_steps, e2e_cells],
+                                                                device, world)
     value = cell_steps / (device_ms / 1e3) if device_ms > 0 else 0.0
     e2e = e2e_cells / e2e_s if e2e_s > 0 else 0.0
     if rank == 0:
