@@ -40,7 +40,31 @@ def needs_build() -> bool:
     return any(p.stat().st_mtime > stamp for p in deps)
 
 
+PREP_LIBRARY = LIBDIR / 'libnhfprep.so'
+
+
+def host_sources() -> list[Path]:
+    return sorted((CSRC / 'host').glob('*.cpp'))
+
+
+def build_host(verbose: bool = False, force: bool = False) -> Path:
+    """The host-only preprocessing library (g++, no CUDA): libnhfprep.so."""
+    deps = host_sources() + [INCLUDE / 'nhf_prep.h']
+    if not force and PREP_LIBRARY.exists() and all(p.stat().st_mtime <= PREP_LIBRARY.stat().st_mtime for p in deps):
+        return PREP_LIBRARY
+    LIBDIR.mkdir(exist_ok=True)
+    tmp = LIBDIR / f'.libnhfprep.{os.getpid()}.so'
+    cmd = [shutil.which('g++') or 'g++', '-O2', '-std=c++17', '-fPIC', '-shared', f'-I{INCLUDE}', '-o', str(tmp),
+           *map(str, host_sources())]
+    if verbose:
+        print(' '.join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, PREP_LIBRARY)
+    return PREP_LIBRARY
+
+
 def build(verbose: bool = False, force: bool = False) -> Path:
+    build_host(verbose, force)
     if not force and not needs_build():
         return LIBRARY
     LIBDIR.mkdir(exist_ok=True)

@@ -169,8 +169,68 @@ def _write_ns(path, t):
     ])
 
 
+_PREP = None
+
+
+def native_library():
+    """libnhfprep.so (csrc/host/nhf_prep.cpp, include/nhf_prep.h), or None
+    when it has not been built."""
+    global _PREP
+    if _PREP is None:
+        import ctypes
+        from .build import PREP_LIBRARY
+        if not PREP_LIBRARY.exists():
+            return None
+        lib = ctypes.CDLL(str(PREP_LIBRARY))
+        P, V, I64 = ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64
+        lib.nhp_prepare.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t,
+                                    ctypes.POINTER(P)]
+        lib.nhp_sizes.argtypes = [P, ctypes.POINTER(I64)]
+        lib.nhp_copy_cells.argtypes = [P] + [V] * 8
+        lib.nhp_copy_sides.argtypes = [P] + [V] * 7
+        lib.nhp_free.argtypes = [P]
+        lib.nhp_error.restype = ctypes.c_char_p
+        _PREP = lib
+    return _PREP
+
+
+def native_tables(ne_text: bytes, ns_text: bytes) -> tuple[dict, dict]:
+    """filter_ne_ns + build_ne_tables + build_ns_tables in C++: the same
+    tables, for meshes where the per-line Python passes are too slow."""
+    import ctypes
+    lib = native_library()
+    if lib is None:
+        raise RuntimeError('libnhfprep.so is not built (python -m nhflood.build)')
+    h = ctypes.c_void_p()
+    if lib.nhp_prepare(ne_text, len(ne_text), ns_text, len(ns_text), ctypes.byref(h)) != 0:
+        raise ValueError(f'NE/NS preprocessing failed: {lib.nhp_error().decode()}')
+    try:
+        sizes = (ctypes.c_int64 * 3)()
+        lib.nhp_sizes(h, sizes)
+        e, s, n = int(sizes[0]), int(sizes[1]), int(sizes[2])
+        ne = dict(index=np.zeros(e, np.uint32), x=np.zeros(e, np.float32), y=np.zeros(e, np.float32),
+                  z=np.zeros(e, np.float32), type=np.zeros(e, np.uint8), counts=np.zeros((e, 4), np.uint32),
+                  ptr=np.zeros((e, 4), np.uint32), isl=np.zeros(n, np.uint32))
+        ns = dict(index=np.zeros(s, np.uint32), length=np.zeros(s, np.float32), x=np.zeros(s, np.float32),
+                  y=np.zeros(s, np.float32), z=np.zeros(s, np.float32), attr=np.zeros(s, np.uint8),
+                  topo=np.zeros((s, 3), np.uint32))
+        lib.nhp_copy_cells(h, *(ne[k].ctypes.data for k in ('index', 'x', 'y', 'z', 'type', 'counts', 'ptr', 'isl')))
+        lib.nhp_copy_sides(h, *(ns[k].ctypes.data for k in ('index', 'length', 'x', 'y', 'z', 'attr', 'topo')))
+    finally:
+        lib.nhp_free(h)
+    return ne, ns
+
+
 def prepare_domain(cfg) -> None:
-    """prepare_domain (domain.py:590-606): filter, build ne/ns/boundary tables."""
+    """prepare_domain (domain.py:590-606): filter, build ne/ns/boundary tables.
+    Uses the C++ preprocessing when libnhfprep.so is built (the same tables),
+    else the Python restatement below."""
+    if native_library() is not None:
+        ne, ns = native_tables(Path(cfg.ne).read_bytes(), Path(cfg.ns).read_bytes())
+        _write_ne(cfg.ne_fdb, ne)
+        _write_ns(cfg.ns_fdb, ns)
+        fdb.save(cfg.boundary_fdb, [('U8Value', 'sbf', {'value': boundary_flags(ns['topo'].astype(np.int64))})])
+        return
     try:
         ne_lines = Path(cfg.ne).read_text(encoding='utf-8').splitlines(keepends=True)
         ns_lines = Path(cfg.ns).read_text(encoding='utf-8').splitlines(keepends=True)
