@@ -16,7 +16,7 @@ import math
 import numpy as np
 
 from .clock import COMPLETED, DONE, TICKS_PER_SECOND, HostClock, seconds_to_ticks, ticks_of, words
-from .model import StepParams
+from .model import STATE_F32, STATE_U32, StepParams
 
 FRAME = 900
 
@@ -108,6 +108,19 @@ class PlainRun:
         if abs(self.elapsed - self.next_frame) < 1e-9 or self.elapsed == self.w.duration:
             self.next_frame = min(self.next_frame + FRAME, float(self.w.duration))
         return completed
+
+    def adopt(self, other: 'PlainRun') -> None:
+        """Continue from another run of the same workload, on another engine:
+        its state arrays, clock and batch bookkeeping; the next CFL candidate
+        is recomputed from the adopted state (as the step itself computes it)."""
+        for name in STATE_F32 + STATE_U32:
+            self.engine.set(name, other.engine.get(name))
+        self.engine.set_clock(other.engine.get_clock())
+        self.clock.now_ticks = other.clock.now_ticks
+        self.elapsed, self.steps = other.elapsed, other.steps
+        self.next_output, self.next_frame = other.next_output, other.next_frame
+        self.rain_index = -1  # upload the rain rates with the next batch
+        self.engine.compute_cfl()
 
     def advance(self) -> int:
         """One synchronous batch through the public engine call."""

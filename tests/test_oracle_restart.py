@@ -84,3 +84,27 @@ def test_restart_after_requested_end_is_rejected_and_at_end_takes_no_steps(tmp_p
     assert same.manifest['completion_reason'] == 'checkpoint_at_end'
     assert same.budget == done.budget
     np.testing.assert_array_equal(same.state.depth, done.state.depth)
+
+
+def test_adopted_state_continues_like_the_original_run():
+    """PlainRun.adopt: a second engine that takes over a run's state, clock
+    and bookkeeping produces the original run's next batches bit for bit."""
+    from engine import OracleEngine
+    from nhflood.plain import PlainRun
+    from nhflood.workloads import plain_uniform_256
+    w = plain_uniform_256(n=32)
+    a = PlainRun(w, lambda x, p: OracleEngine(x, p))
+    while a.elapsed < 1300:
+        a.advance()
+    b = PlainRun(w, lambda x, p: OracleEngine(x, p))
+    b.adopt(a)
+    for _ in range(5):
+        ta, oa = a.begin()
+        tb, ob = b.begin()
+        np.testing.assert_array_equal(ta, tb)
+        ra, rb = a.engine.run_batch(ta, oa), b.engine.run_batch(tb, ob)
+        np.testing.assert_array_equal(ra, rb)
+        a.finish(ra)
+        b.finish(rb)
+    for name in ('depth', 'q', 'max_depth', 'peak_hi', 'peak_lo'):
+        np.testing.assert_array_equal(a.engine.get(name), b.engine.get(name))
