@@ -185,6 +185,10 @@ def bench_batched(args, rank, world, local):
     ens = EnsembleRun(ws, device=str(device), tile=args.tile, grid_blocks=args.grid)
     t_setup = time.perf_counter() - t0
     stream = ens.ensemble.stream()
+    # spin-up (untimed) a third into the members' runs, as for the plain form
+    spin_to = min(r.w.duration for r in ens.runs) / 3
+    while min(r.elapsed for r in ens.runs) < spin_to and not ens.done:
+        ens.advance()
     for _ in range(args.warmup):
         ens.advance()
     torch.cuda.synchronize(device)
@@ -255,6 +259,7 @@ def bench_batched(args, rank, world, local):
                        'cells': int(cells.sum()), 'cells_min': int(cells.min()), 'cells_max': int(cells.max()),
                        'time_steps_per_bench_step': ens.runs[0].params.batch_size,
                        'tile': ens.ensemble.tile, 'grid_blocks': ens.ensemble.grid, 'tiles': ens.ensemble.tiles,
+                       'spin_up_to_s': spin_to,
                        'l2': 'inputs larger than L2', 'parallelism': f'replicas{world}'},
             'plain_sequential': {'value': plain, 'unit': METRIC,
                                  'sample': f'{args.plain_batches} plain batches of each member, one member after another'},
