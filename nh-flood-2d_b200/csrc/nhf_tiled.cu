@@ -59,15 +59,6 @@ __device__ __forceinline__ void cp_async_wait_all()
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-// Programmatic dependent launch: a step (or pre-pass) kernel lets the next
-// launch in the stream start as soon as all of its blocks have started, and
-// waits for the previous launch to complete (with its memory visible) before
-// it reads anything that launch wrote: the control block and the state. The
-// next step's blocks thus stage their static index tables while the last
-// wave of the current step finishes.
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
 // ----------------------------------------------------------------- kernels
 
 template <int CPT>
@@ -160,7 +151,31 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
 
     if (tid == 0) { sh_cnt[0] = sh_cnt[1] = sh_cnt[2] = 0u; sh_minbits = __float_as_uint(1.0f); }
     if (tid < CPT * (NT / 256)) (&sh_mask[0][0])[tid] = 0u;
-    pdl_trigger();
+    const int active = c->active;
+    if (!active) {
+        // No physics this slot: the last block advances the slot and prepares the next.
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            unsigned ticket = atomicAdd(&c->done_blocks, 1u);
+            if (ticket == n_tiles - 1) {
+                c->done_blocks = 0;
+                finish_step(c);
+                if (c->slot < d.batch_size) prepare_step(d, c, cur_depth(d, c->parity), cur_q(d, c->parity));
+            }
+        }
+        return;
+    }
+    const int parity = c->parity;
+    const float dt = c->dt;
+    const int raining = c->raining;
+    const float *depth_in = parity ? d.depth_b : m.depth;
+    float *depth_out = parity ? m.depth : d.depth_b;
+    const float *q_in = parity ? d.q_b : m.q;
+    float *q_out = parity ? m.q : d.q_b;
+    const float *rt_in = parity ? d.rain_time_b : m.rain_time;
+    float *rt_out = parity ? m.rain_time : d.rain_time_b;
+
     const TilePlan &P = d.plan;
     const bool hanging = kHang == 1 || (kHang == 2 && m.hang_cells > 0);
     Tile tl;
@@ -207,33 +222,6 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
         cp_async4(reinterpret_cast<uint32_t *>(sh_fidx) + i, reinterpret_cast<const uint32_t *>(tl.fidx) + i);
     cp_async_wait_all();
     __syncthreads();
-    // Everything below reads what the previous launch wrote.
-    pdl_wait();
-    const int active = c->active;
-    if (!active) {
-        // No physics this slot: the last block advances the slot and prepares the next.
-        __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            unsigned ticket = atomicAdd(&c->done_blocks, 1u);
-            if (ticket == n_tiles - 1) {
-                c->done_blocks = 0;
-                finish_step(c);
-                if (c->slot < d.batch_size) prepare_step(d, c, cur_depth(d, c->parity), cur_q(d, c->parity));
-            }
-        }
-        return;
-    }
-    const int parity = c->parity;
-    const float dt = c->dt;
-    const int raining = c->raining;
-    const float *depth_in = parity ? d.depth_b : m.depth;
-    float *depth_out = parity ? m.depth : d.depth_b;
-    const float *q_in = parity ? d.q_b : m.q;
-    float *q_out = parity ? m.q : d.q_b;
-    const float *rt_in = parity ? d.rain_time_b : m.rain_time;
-    float *rt_out = parity ? m.rain_time : d.rain_time_b;
-
     // (b) Gathers: depth and bed of the tile and its rings, the per-cell
     // inputs of rings 0..2 (the rain pixel index parks in sh_rq), and q and
     // length of every local side.
@@ -1016,34 +1004,17 @@ void set_smem_all(size_t bytes)
     set_smem(k_step_ensemble<false, NT, CPT>, bytes);
 }
 
-// Launch with programmatic stream serialisation (see pdl_wait).
-template <typename... KArgs, typename... Args>
-void launch_pdl(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t s, Args... args)
-{
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)grid);
-    cfg.blockDim = dim3((unsigned)block);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kernel, args...);
-}
-
 template <int NT, int CPT>
 void launch_step(const Dev &d, size_t smem, cudaStream_t s)
 {
     const int grid = d.plan.n_tiles;
     const bool hanging = d.m.hang_cells > 0;
     if (d.theta_one) {
-        if (hanging) launch_pdl(k_step_tiled<true, true, NT, CPT>, grid, NT, smem, s, d);
-        else launch_pdl(k_step_tiled<true, false, NT, CPT>, grid, NT, smem, s, d);
+        if (hanging) k_step_tiled<true, true, NT, CPT><<<grid, NT, smem, s>>>(d);
+        else k_step_tiled<true, false, NT, CPT><<<grid, NT, smem, s>>>(d);
     } else {
-        if (hanging) launch_pdl(k_step_tiled<false, true, NT, CPT>, grid, NT, smem, s, d);
-        else launch_pdl(k_step_tiled<false, false, NT, CPT>, grid, NT, smem, s, d);
+        if (hanging) k_step_tiled<false, true, NT, CPT><<<grid, NT, smem, s>>>(d);
+        else k_step_tiled<false, false, NT, CPT><<<grid, NT, smem, s>>>(d);
     }
 }
 
@@ -1095,8 +1066,6 @@ __device__ __forceinline__ void pressure_slot(const Dev &d, int slot)
 
 __global__ void k_pressure_tiled(const __grid_constant__ Dev d)
 {
-    pdl_trigger();
-    pdl_wait();
     if (!d.ctl->active) return;
     int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot < d.m.hang_cells) pressure_slot(d, slot);
@@ -1127,8 +1096,6 @@ __device__ __forceinline__ void face_qn_cell(const Dev &d, int ei)
 
 __global__ void k_face_qn_tiled(const __grid_constant__ Dev d)
 {
-    pdl_trigger();
-    pdl_wait();
     if (!d.ctl->active) return;
     int ei = blockIdx.x * blockDim.x + threadIdx.x;
     if (ei < d.m.e_num) face_qn_cell(d, ei);
@@ -1164,8 +1131,6 @@ __global__ void k_ens_batch_start(const Dev *devs, const int2 *items)
 
 __global__ void k_ens_pressure(const Dev *devs, const int2 *items)
 {
-    pdl_trigger();
-    pdl_wait();
     const int2 w = items[blockIdx.x];
     const Dev &d = devs[w.x];
     if (!d.ctl->active) return;
@@ -1175,8 +1140,6 @@ __global__ void k_ens_pressure(const Dev *devs, const int2 *items)
 
 __global__ void k_ens_face_qn(const Dev *devs, const int2 *items)
 {
-    pdl_trigger();
-    pdl_wait();
     const int2 w = items[blockIdx.x];
     const Dev &d = devs[w.x];
     if (!d.ctl->active) return;
@@ -1337,8 +1300,8 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
 void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s)
 {
     const nhf_mesh &m = d.m;
-    if (m.hang_cells > 0) launch_pdl(k_pressure_tiled, (m.hang_cells + 255) / 256, 256, 0, s, d);
-    if (!d.theta_one) launch_pdl(k_face_qn_tiled, (m.e_num + 255) / 256, 256, 0, s, d);
+    if (m.hang_cells > 0) k_pressure_tiled<<<(m.hang_cells + 255) / 256, 256, 0, s>>>(d);
+    if (!d.theta_one) k_face_qn_tiled<<<(m.e_num + 255) / 256, 256, 0, s>>>(d);
     switch (d.plan.tile) {
     case 1024: launch_step<512, 2>(d, b.shared_bytes, s); break;
     case 512: launch_step<512, 1>(d, b.shared_bytes, s); break;
@@ -1384,14 +1347,14 @@ void ensemble_enqueue_batch_start(const EnsembleLaunch &e, cudaStream_t s)
 template <int NT, int CPT>
 void ensemble_launch(const EnsembleLaunch &e, cudaStream_t s)
 {
-    if (e.theta_one) launch_pdl(k_step_ensemble<true, NT, CPT>, e.grid, NT, e.smem, s, e.devs, e.step_items, e.n_step);
-    else launch_pdl(k_step_ensemble<false, NT, CPT>, e.grid, NT, e.smem, s, e.devs, e.step_items, e.n_step);
+    if (e.theta_one) k_step_ensemble<true, NT, CPT><<<e.grid, NT, e.smem, s>>>(e.devs, e.step_items, e.n_step);
+    else k_step_ensemble<false, NT, CPT><<<e.grid, NT, e.smem, s>>>(e.devs, e.step_items, e.n_step);
 }
 
 void ensemble_enqueue_step(const EnsembleLaunch &e, cudaStream_t s)
 {
-    if (e.n_hang) launch_pdl(k_ens_pressure, e.n_hang, 256, 0, s, e.devs, e.hang_items);
-    if (!e.theta_one && e.n_qn) launch_pdl(k_ens_face_qn, e.n_qn, 256, 0, s, e.devs, e.qn_items);
+    if (e.n_hang) k_ens_pressure<<<e.n_hang, 256, 0, s>>>(e.devs, e.hang_items);
+    if (!e.theta_one && e.n_qn) k_ens_face_qn<<<e.n_qn, 256, 0, s>>>(e.devs, e.qn_items);
     switch (e.tile) {
     case 1024: ensemble_launch<512, 2>(e, s); break;
     case 512: ensemble_launch<512, 1>(e, s); break;
