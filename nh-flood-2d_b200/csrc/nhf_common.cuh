@@ -36,10 +36,6 @@ struct TilePlan {
     // per tile: n_ext, n_r0, n_r01, n_r012, n_sides, n_owned, n_qf, r0_first_offset,
     // n_faces, cbase, sbase, then the pattern's ext, side, face_desc and face_idx offsets, 0
     const int4 *tile_head;     // [n_tiles][4]
-    const int32_t *tile_pattern, *tile_cbase, *tile_sbase;  // [n_tiles]
-    const int32_t *p_counts;   // [pattern][12]: n_ext, n_r0, n_r01, n_r012, n_sides, n_owned, n_qf,
-                               // r0_first_offset, n_faces, 0, 0, 0
-    const int32_t *p_offsets;  // [pattern][4]: ext, side, face_desc, face_idx
     const int32_t *ext_rel;    // relative cell ids by local slot (slot 0 = exterior sentinel)
     const int32_t *side_rel;   // relative side ids by local side
     const uint32_t *side_lohi; // local slots: lower | higher << 16

@@ -1252,8 +1252,7 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     if (srel.empty()) { srel.push_back(0); lohi.push_back(0); }
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
-    size_t o_tp = take(tp.size() * 4), o_tc = take(tc.size() * 4), o_ts = take(ts.size() * 4);
-    size_t o_cnt = take(counts.size() * 4), o_off = take(offsets.size() * 4), o_ext = take(ext.size() * 4);
+    size_t o_ext = take(ext.size() * 4);
     size_t o_srel = take(srel.size() * 4), o_lohi = take(lohi.size() * 4), o_fd = take(fdesc.size() * 4);
     size_t o_fi = take(fidx.size() * 2);
     size_t o_hd = take(head.size() * 4);
@@ -1263,9 +1262,7 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     auto up = [&](size_t o, const void *src, size_t n) {
         return cudaMemcpyAsync(b + o, src, n, cudaMemcpyHostToDevice, s) == cudaSuccess;
     };
-    bool ok = up(o_tp, tp.data(), tp.size() * 4) && up(o_tc, tc.data(), tc.size() * 4) &&
-              up(o_ts, ts.data(), ts.size() * 4) && up(o_cnt, counts.data(), counts.size() * 4) &&
-              up(o_off, offsets.data(), offsets.size() * 4) && up(o_ext, ext.data(), ext.size() * 4) &&
+    bool ok = up(o_ext, ext.data(), ext.size() * 4) &&
               up(o_srel, srel.data(), srel.size() * 4) && up(o_lohi, lohi.data(), lohi.size() * 4) &&
               up(o_fd, fdesc.data(), fdesc.size() * 4) && up(o_fi, fidx.data(), fidx.size() * 2) &&
               up(o_hd, head.data(), head.size() * 4) &&
@@ -1278,11 +1275,6 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     P.max_sides = max_sides;
     P.cells_per_thread = tile == 1024 ? 2 : 1;
     P.tile_head = (const int4 *)(b + o_hd);
-    P.tile_pattern = (const int32_t *)(b + o_tp);
-    P.tile_cbase = (const int32_t *)(b + o_tc);
-    P.tile_sbase = (const int32_t *)(b + o_ts);
-    P.p_counts = (const int32_t *)(b + o_cnt);
-    P.p_offsets = (const int32_t *)(b + o_off);
     P.ext_rel = (const int32_t *)(b + o_ext);
     P.side_rel = (const int32_t *)(b + o_srel);
     P.side_lohi = (const uint32_t *)(b + o_lohi);

@@ -41,3 +41,24 @@ def test_friction_power_and_horton_exp_round_like_the_exact_value():
     exact = np.exp(a.astype(np.float64)).astype(np.float32)
     diff = ulps(got, exact)
     assert diff.max() <= 1.0 and (diff == 0).mean() > 0.999
+
+
+def test_f64_build_of_the_step_follows_the_f32_step_on_a_benign_case():
+    """The F64 build (liboracle_f64.so, the precision study's reference) runs
+    the same step: on 600 s of rain on a gentle 32 x 32 grid (no flow yet,
+    water only accumulates) both builds take the same steps and agree to F32
+    rounding."""
+    import numpy as np
+    from engine import OracleEngine
+    from nhflood.plain import PlainRun
+    from nhflood.workloads import plain_uniform_256
+    w = plain_uniform_256(n=32)
+    w.duration = 600
+    runs = [PlainRun(w, lambda a, p, q=q: OracleEngine(a, p, precision=q)) for q in ('f32', 'f64')]
+    for r in runs:
+        while not r.done:
+            r.advance()
+    assert runs[0].steps == runs[1].steps == 600
+    h32, h64 = runs[0].engine.get('depth'), runs[1].engine.get('depth')
+    assert h64.dtype == np.float64 and h64.max() > 0.008
+    np.testing.assert_allclose(h32, h64, rtol=0, atol=1e-6)
