@@ -231,7 +231,6 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
         if (i) cp_async4(sh_h + i, depth_in + g);
         else sh_h[0] = m.depth[0];
         cp_async4(sh_z + i, m.bed + g);
-        sh_s[i] = 0.0f;  // donor_scale of the exterior sentinel stays 0
         if (i >= 1 && i <= tl.n_r012) {
             cp_async4(sh_area + i, m.area + g);
             cp_async4(sh_bi + i, m.boundary_id + g);
@@ -247,12 +246,9 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
     tl.lohi = sh_lohi;
     tl.fdesc = sh_fdesc;
     tl.fidx = sh_fidx;
+    if (tid == 0) sh_s[0] = 0.0f;  // donor_scale of the exterior sentinel (ring 3 is never a donor)
     cp_async_wait_all();
     __syncthreads();
-    for (int i = 1 + tid; i <= tl.n_r012; i += NT) {
-        const int pixel = __float_as_int(sh_rq[i]);
-        sh_rq[i] = raining ? d.rain_rates[pixel] : 0.0f;
-    }
 
     // P1: momentum (solver_compact.py:439-486) for every local side. A side
     // whose flow height is below min_h gets q = +0 whatever its other inputs
@@ -316,7 +312,9 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
                 kind = m.kind[bi];
                 if (kind == 1) discharge = d.values[bi] * m.weight[sh_g[i]];
             }
-            float rainq = sh_rq[i];
+            // rain rate from the staged pixel index, kept for the depth update
+            const float rainq = raining ? d.rain_rates[__float_as_int(sh_rq[i])] : 0.0f;
+            sh_rq[i] = rainq;
             float pipe = 0.0f;
             float positive = (maxf(pipe, 0.0f) + maxf(discharge, 0.0f)) * dt;
             float area = sh_area[i];
@@ -574,7 +572,9 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
                             acc_add(d.acc_sum + (size_t)blk * T + t, d.acc_comp + (size_t)blk * T + t, r);
                     }
                 }
-                __syncthreads();
+                // the staging area is reused only by a further chunk; after the
+                // last one the other warps go on while these finish
+                if (any || kk + 1 < CPT) __syncthreads();
             }
         }
     }
