@@ -304,17 +304,17 @@ def bench_served(args, rank, world, local):
         r.prepare()
     # warm-up: one small request through both paths (module loads, first graph)
     warm = [Request(-1, 0.0, _request_workload(dict(stream[0]['params'], width=1000.0, duration=60)))]
-    server = FloodServer(hbm_budget=args.hbm_budget, tile=args.tile or 512, device=str(device))
+    server = FloodServer(hbm_budget=args.hbm_budget, tile=args.tile or 256, device=str(device))
     serve(warm, server, realtime=False)
-    serve_sequential([Request(-1, 0.0, warm[0].workload)], tile=args.tile or 512, device=str(device), realtime=False)
-    server = FloodServer(hbm_budget=args.hbm_budget, tile=args.tile or 512, device=str(device))
+    serve_sequential([Request(-1, 0.0, warm[0].workload)], tile=args.tile or 256, device=str(device), realtime=False)
+    server = FloodServer(hbm_budget=args.hbm_budget, tile=args.tile or 256, device=str(device))
     with ClockSampler(local) as clocks:
         t0 = time.perf_counter()
         served = serve(reqs, server, realtime=True)
         served_wall = time.perf_counter() - t0
     server.close()
     t0 = time.perf_counter()
-    sequential = serve_sequential(reqs, tile=args.tile or 512, device=str(device), realtime=True)
+    sequential = serve_sequential(reqs, tile=args.tile or 256, device=str(device), realtime=True)
     seq_wall = time.perf_counter() - t0
     by_id = {c.id: c for c in sequential}
     max_err = 0.0
@@ -332,7 +332,7 @@ def bench_served(args, rank, world, local):
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'form': 'served',
             'config': {'workload': f'served_{len(reqs)}_requests', 'arrival_rate_per_s': 2.0,
                        'cells_total': int(cells.sum()), 'cells_min': int(cells.min()), 'cells_max': int(cells.max()),
-                       'hbm_budget_bytes': args.hbm_budget, 'tile': args.tile or 512, 'parallelism': f'replicas{world}',
+                       'hbm_budget_bytes': args.hbm_budget, 'tile': args.tile or 256, 'parallelism': f'replicas{world}',
                        'l2': 'inputs larger than L2 once several solves are resident'},
             'timing': 'wall clock of the whole session, arrivals replayed in real time',
             'latency': latency_summary(served),

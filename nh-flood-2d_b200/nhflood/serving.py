@@ -11,6 +11,10 @@ stream, so their upload and set-up overlap the batch; a solve that reaches
 its end time is retired at the end of the round with its final depth and
 max-depth (extrema) frames, and its memory goes back to the budget.
 
+Admitted solves are built (arrays, upload, tile plan) by a builder thread on
+its own stream, so the scheduling loop keeps launching rounds for the
+resident solves meanwhile; a finished build joins at the next round.
+
 Every solve runs the same arithmetic as the plain single run (the ensemble
 step is the plain step per member), so a result does not depend on what
 else was resident: alone and in the mix are bit-identical.
@@ -19,6 +23,7 @@ from __future__ import annotations
 
 import time
 from collections import deque
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -38,6 +43,19 @@ def device_bytes_estimate(arrays) -> int:
     scratch = 4 * (s + e + 4 * e + 2 * e + s) + 16 * ((e + 255) // 256) * arrays.terms
     plan = 24 * e + 64 * 1024
     return int(arrays.nbytes() + state + scratch + plan + (1 << 20))
+
+
+def device_bytes_bound(workload) -> int:
+    """An upper bound of device_bytes_estimate from the mesh sizes alone
+    (before the step arrays are built): hanging-edge tables counted as if
+    every side had one."""
+    m = workload.mesh
+    e, s, isl = m.e_num, m.s_num, len(m.isl_data)
+    terms = 4 + 6 * len(workload.forcing.boundaries)
+    inputs = 4 * (12 * e + 8 * e + isl) + 21 * s + 16 * e + 44 * s
+    state = 4 * (10 * e + s)
+    scratch = 4 * (s + e + 4 * e + 2 * e + s) + 16 * ((e + 255) // 256) * terms
+    return int(inputs + state + scratch + 24 * e + 64 * 1024 + (1 << 20))
 
 
 @dataclass
@@ -77,7 +95,7 @@ class Completed:
 
 
 class FloodServer:
-    def __init__(self, *, hbm_budget: float = 150e9, tile: int = 512, grid_blocks: int = 0,
+    def __init__(self, *, hbm_budget: float = 150e9, tile: int = 256, grid_blocks: int = 0,
                  batch_size: int = 32, device: str = 'cuda:0', clock=None):
         import torch
         self.torch = torch
@@ -86,6 +104,8 @@ class FloodServer:
         self.tile, self.grid_blocks, self.batch_size = tile, grid_blocks, batch_size
         self.side = torch.cuda.Stream(self.device)
         self.waiting: deque[Request] = deque()
+        self.building: deque = deque()  # (request, future of its PlainRun, bytes reserved)
+        self.builder = ThreadPoolExecutor(max_workers=1, thread_name_prefix='nhflood-build')
         self.active: list[tuple[Request, PlainRun, int, float]] = []  # request, run, bytes, admitted at
         self.used = 0
         self.peak_used = 0
@@ -100,32 +120,51 @@ class FloodServer:
 
     @property
     def busy(self) -> bool:
-        return bool(self.waiting or self.active)
+        return bool(self.waiting or self.building or self.active)
 
     def submit(self, request: Request) -> None:
         self.waiting.append(request)
 
     # -- admission and retirement ------------------------------------------
     def _admit(self) -> int:
-        admitted = 0
+        """Start building waiting requests, first come first served, while
+        their memory bound fits the budget next to what is resident or
+        being built."""
+        started = 0
         while self.waiting:
             req = self.waiting[0]
-            need = req.prepare()
+            need = device_bytes_bound(req.workload)
             if need > self.budget:
                 raise ValueError(f'request {req.id} needs {need} B, more than the whole budget')
             if self.used + need > self.budget:
                 break
             self.waiting.popleft()
-            with self.torch.cuda.stream(self.side):
-                run = PlainRun(req.workload, tiled_factory(self.tile, str(self.device)), batch_size=self.batch_size,
-                               arrays=req.arrays)
-            req.arrays = None  # the engine holds the device copy
-            self.active.append((req, run, need, self.now()))
             self.used += need
             self.peak_used = max(self.peak_used, self.used)
+            self.building.append((req, self.builder.submit(self._build, req), need))
+            started += 1
+        return started
+
+    def _build(self, req):
+        """Builder thread: the solve's arrays, upload and plan on the side stream."""
+        with self.torch.cuda.device(self.device), self.torch.cuda.stream(self.side):
+            run = PlainRun(req.workload, tiled_factory(self.tile, str(self.device)), batch_size=self.batch_size,
+                           arrays=req.arrays)
+        self.side.synchronize()
+        req.arrays = None  # the engine holds the device copy
+        return run
+
+    def _join_built(self, wait: bool) -> None:
+        """Finished builds join the resident set (in admission order); with
+        wait, block for the first one when nothing else can run."""
+        while self.building and (self.building[0][1].done() or wait):
+            req, future, bound = self.building.popleft()
+            run = future.result()
+            need = device_bytes_estimate(run.arrays)
+            self.used += need - bound
+            self.active.append((req, run, need, self.now()))
             self.dirty = True
-            admitted += 1
-        return admitted
+            wait = False
 
     def _retire(self) -> list[Completed]:
         done, keep = [], []
@@ -173,10 +212,14 @@ class FloodServer:
             for i, (_, run, _, _) in enumerate(self.active[:launched.members]):
                 run.finish(traces[i])
             self.rounds += 1
-        self.side.synchronize()
+        self._join_built(wait=launched is None)
         return self._retire()
 
     def close(self):
+        for _, future, _ in self.building:
+            future.result().close()
+        self.building.clear()
+        self.builder.shutdown(wait=True)
         if self.ensemble is not None:
             self.ensemble.close()
             self.ensemble = None
@@ -202,7 +245,7 @@ def serve(requests, server: FloodServer, realtime: bool = True) -> list[Complete
     return out
 
 
-def serve_sequential(requests, *, tile: int = 512, batch_size: int = 32, device: str = 'cuda:0',
+def serve_sequential(requests, *, tile: int = 256, batch_size: int = 32, device: str = 'cuda:0',
                      realtime: bool = True, clock=None) -> list[Completed]:
     """The plain form, one solve at a time in arrival order (the baseline of
     the served form): each request waits for the previous one to finish."""

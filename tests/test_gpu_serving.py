@@ -20,11 +20,11 @@ def requests():
 
 
 def test_served_results_equal_sequential_results(cuda_available):
-    from nhflood.serving import FloodServer, serve, serve_sequential
+    from nhflood.serving import FloodServer, device_bytes_bound, serve, serve_sequential
     reqs = requests()
     for r in reqs:
-        r.prepare()
-    needs = sorted(r.need for r in reqs)
+        assert device_bytes_bound(r.workload) >= r.prepare()
+    needs = sorted(device_bytes_bound(r.workload) for r in reqs)
     budget = needs[-1] + needs[-2] + 1  # at most the two largest together
     server = FloodServer(hbm_budget=budget, tile=256)
     resident = []
