@@ -166,6 +166,43 @@ void *nhf_stream(nhf_handle *h);
 /* Which step form the handle runs ("tiled(...)" or "multipass (reason)"). */
 const char *nhf_path(const nhf_handle *h);
 
+/* Gate controller (core/gate.py:35-206; the step graph's check_gates,
+ * clear/collect_gate_budget, measure_pond_inventory and finish_gate_bed
+ * passes, solver_compact.py:896-906, and the record_flux / record_cell hooks
+ * in tick, :523-524 and :595-604). Every array is a DEVICE pointer owned by
+ * the caller and alive until nhf_destroy; the controller words are read and
+ * restored by the caller directly (snapshot/restore, gate.py:195-215).
+ * While attached, every step checks the triggers and moves the gate beds at
+ * its start, records the post-limiter exchange volumes and the pond and
+ * gate-cell source terms, and moves the beds to the step end before the CFL.
+ * Terms (10 count + 8, the reference's order): per gate pond in/out, river
+ * in/out; overtopping in/out and the pond's six source terms (rain,
+ * infiltration, positivity, pipe, boundary, rounding); per gate the
+ * channel's six source terms. Gates need the multi-pass step (path 1). */
+typedef struct nhf_gate {
+    int32_t count;           /* gates */
+    int32_t n_targets;       /* gate cells */
+    int32_t n_flux;          /* recorded sides */
+    const int32_t *cell_gate;  /* [e_num] gate of each cell, -1 off gates */
+    const int32_t *pond;       /* [e_num] 1 on pond cells, 0 at the sentinel */
+    const float *closed;       /* [e_num] closed (initial) bed */
+    const int32_t *targets;    /* [n_targets] gate cells, gate by gate */
+    const int32_t *controls;   /* [count] control cell of each gate */
+    const int32_t *flux_sides; /* [n_flux] sides between gate and non-gate cells, or pond and non-pond cells */
+    uint32_t formal_tick[2];   /* clock words of formal time 0 (control starts there) */
+    float trigger_level, opening_seconds, open_elevation;
+    int32_t *commanded, *flow_seen, *opened;     /* [count] controller words */
+    uint32_t *command, *first_flow, *opened_at;  /* [count][2] clock words */
+} nhf_gate;
+int nhf_gate_attach(nhf_handle *h, const nhf_gate *gate);
+/* check_gates at run start (solver_compact.py:885-888): trigger check and
+ * bed motion at the current clock. */
+int nhf_gate_check(nhf_handle *h);
+int nhf_gate_terms(const nhf_handle *h);
+/* controller.budget.flush: this interval's totals [nhf_gate_terms] (host),
+ * FP64 per-block partials merged in block order; clears them. */
+int nhf_gate_flush(nhf_handle *h, double *totals);
+
 /* Ensemble (batched) form. The reference runs one domain per process
  * (solver_compact.py:179-1008); an ensemble advances many member handles
  * together, one fused step launch per slot for all of them, each member

@@ -43,6 +43,19 @@ struct TilePlan {
     const uint16_t *face_idx;  // local side indices in the reference's CSR order
 };
 
+// Gate controller (core/gate.py:35-206): the caller's tables and controller
+// words plus the library's budget partials [blocks][terms].
+struct GateDev {
+    int32_t count, n_targets, n_flux, terms, blocks;
+    const int32_t *cell_gate, *pond, *targets, *controls, *flux_sides;
+    const float *closed;
+    uint32_t formal_hi, formal_lo;
+    float trigger_level, opening_seconds, open_elevation;
+    int32_t *commanded, *flow_seen, *opened;
+    uint32_t *command, *first_flow, *opened_at;
+    double *acc_sum, *acc_comp;
+};
+
 struct Dev {
     nhf_mesh m;
     float g, neg_g, afa, sita, half_rest, seven_thirds, min_h, min_dt;

@@ -28,6 +28,10 @@ struct nhf_handle {
     cudaGraphNode_t begin_node = nullptr;
     cudaKernelNodeParams begin_params{};
     nhf::TiledBuild tb{};
+    nhf::GateDev gate{};
+    bool gate_on = false;
+    void *gate_mem = nullptr;   // gate budget partials
+    double *h_gacc = nullptr;   // pinned staging of the gate partials
     bool tiled = false;
     std::string path = "multipass";
     std::string err;

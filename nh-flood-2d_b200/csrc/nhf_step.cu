@@ -12,6 +12,11 @@
 //               FP64 per-block budget partials, wet count
 //   k_cfl       CFL packed (value, side) minimum; the last block commits the
 //               clock and writes the trace row
+// With a gate controller attached (core/gate.py) the step also runs
+//   k_gate_move trigger check and bed motion at the step start (after
+//               k_prepare) and bed motion to the step end (before k_cfl)
+//   k_gate_flux post-limiter exchange volumes of the recorded sides (after
+//               k_scale); k_cells adds the pond and gate-cell source terms
 // A batch of up to 64 steps plus the begin/trace copies is captured once into
 // a CUDA graph and replayed per batch. Every scalar the steps need (dt, clock
 // words, boundary values) lives in a device control block, so the graph is
@@ -276,8 +281,11 @@ __global__ void k_scale(Dev d)
 // ------------------------------------------------------------- cell update
 
 // tick cell loops 2 and 3 (solver_compact.py:525-610) for one 256-cell budget
-// block; the per-block budget partials have one writer.
-__global__ void __launch_bounds__(kBlock) k_cells(Dev d)
+// block; the per-block budget partials have one writer. kGate adds the gate
+// controller's record_cell, measure_inventory and rounding collection
+// (solver_compact.py:595-604; gate.py:151-193) for pond and gate cells.
+template <bool kGate>
+__global__ void __launch_bounds__(kBlock) k_cells(Dev d, GateDev g)
 {
     __shared__ double sh[kBlock];
     const nhf_mesh &m = d.m;
@@ -294,6 +302,8 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d)
     float t_discharge = 0.0f;
     int bi = -1, kind = -1;
     bool wet = false;
+    int goff = -1;
+    float gv[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     if (valid) {
         bi = m.boundary_id[ei];
         kind = bi >= 0 ? m.kind[bi] : -1;
@@ -357,6 +367,25 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d)
             depth = maxf(raw_depth, 0.0f);
         }
         m.depth[ei] = depth;
+        if (kGate) {
+            goff = g.pond[ei] == 1 ? 4 * g.count + 2
+                 : (g.cell_gate[ei] >= 0 ? 4 * g.count + 8 + 6 * g.cell_gate[ei] : -1);
+            if (goff >= 0) {
+                float applied_floor = floor_v, level_exchange = 0.0f;
+                if (kind == 0) {
+                    applied_floor = 0.0f;
+                    level_exchange = (depth - previous) * ea - (ql - qr + qb - qt) * dt - pipe * dt
+                                     - rain_depth * ea + removed * ea;
+                }
+                gv[0] = rain_depth * ea;
+                gv[1] = removed * ea;
+                gv[2] = applied_floor * ea;
+                gv[3] = pipe * dt;
+                gv[4] = (ssq - pipe) * dt + level_exchange;
+                float rounding = (depth - previous) - increment + removed - applied_floor;
+                gv[5] = rounding * ea - level_exchange;
+            }
+        }
         float h = maxf(depth, 0.01f);
         float u = 0.0f, v = 0.0f;
         if (depth >= d.min_h) {
@@ -387,6 +416,121 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d)
         if (!__syncthreads_or(val != 0.0f)) continue;
         double sum = block_tree((double)val, sh);
         if (threadIdx.x == 0) acc_add(acc_s + t, acc_c + t, sum);
+    }
+    if (kGate) {
+        // the pond group, then gate by gate: six terms each
+        for (int grp = -1; grp < g.count; ++grp) {
+            const int off = grp < 0 ? 4 * g.count + 2 : 4 * g.count + 8 + 6 * grp;
+            if (!__syncthreads_or(goff == off)) continue;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                float val = goff == off ? gv[k] : 0.0f;
+                if (!__syncthreads_or(val != 0.0f)) continue;
+                double sum = block_tree((double)val, sh);
+                if (threadIdx.x == 0) {
+                    size_t idx = (size_t)blk * g.terms + off + k;
+                    acc_add(g.acc_sum + idx, g.acc_comp + idx, sum);
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ gate control
+
+// since_command (gate.py:68-73): the command's clock age in F32 seconds.
+__device__ __forceinline__ float since_command(const GateDev &g, int gate, uint32_t hi, uint32_t lo)
+{
+    uint32_t borrow = lo < g.command[2 * gate + 1] ? 1u : 0u;
+    uint32_t high = hi - g.command[2 * gate] - borrow;
+    uint32_t low = lo - g.command[2 * gate + 1];
+    return __uint2float_rn(high) / 256.0f + __uint2float_rn(low) * 0x1p-40f;
+}
+
+// check (gate.py:88-99) and move (gate.py:75-86), one block: at_end = 0 is
+// check_gates at the step start (irreversible command once the control cell
+// is wet above the trigger, from formal time 0 on, then the beds at now);
+// at_end = 1 is finish_gate_bed (the beds at the step end).
+__global__ void __launch_bounds__(256) k_gate_move(Dev d, GateDev g, int at_end)
+{
+    const nhf_mesh &m = d.m;
+    const Ctl *c = d.ctl;
+    if (!c->active) return;
+    const uint32_t hi = at_end ? c->step_end[0] : c->now[0];
+    const uint32_t lo = at_end ? c->step_end[1] : c->now[1];
+    if (!at_end) {
+        const bool formal = hi > g.formal_hi || (hi == g.formal_hi && lo >= g.formal_lo);
+        for (int gate = threadIdx.x; formal && gate < g.count; gate += blockDim.x) {
+            int cell = g.controls[gate];
+            if (g.commanded[gate] == 0 && m.depth[cell] >= d.min_h && m.bed[cell] + m.depth[cell] > g.trigger_level) {
+                g.commanded[gate] = 1;
+                g.command[2 * gate] = hi; g.command[2 * gate + 1] = lo;
+            }
+        }
+        __syncthreads();
+    }
+    for (int slot = threadIdx.x; slot < g.n_targets; slot += blockDim.x) {
+        int cell = g.targets[slot];
+        int gate = g.cell_gate[cell];
+        if (g.commanded[gate] != 1) continue;
+        float fraction = minf(since_command(g, gate, hi, lo) / g.opening_seconds, 1.0f);
+        if (fraction >= 1.0f) {
+            m.bed[cell] = g.open_elevation;
+            if (atomicOr(&g.opened[gate], 1) == 0) {
+                g.opened_at[2 * gate] = hi; g.opened_at[2 * gate + 1] = lo;
+            }
+        } else {
+            float closed = g.closed[cell];
+            m.bed[cell] = closed + (g.open_elevation - closed) * fraction;
+        }
+    }
+}
+
+// record_flux (gate.py:118-140) on the post-limiter volume of each recorded
+// side, per 256 entries of the side list; the first nonzero gate-to-pond
+// volume latches the gate's first-flow time.
+__global__ void __launch_bounds__(kBlock) k_gate_flux(Dev d, GateDev g)
+{
+    __shared__ double sh[kBlock];
+    const nhf_mesh &m = d.m;
+    const Ctl *c = d.ctl;
+    if (!c->active) return;
+    const int p = blockIdx.x * kBlock + threadIdx.x;
+    int term = -1;
+    float v0 = 0.0f, v1 = 0.0f;
+    if (p < g.n_flux) {
+        int si = g.flux_sides[p];
+        int left = m.topology[3 * si + 1], right = m.topology[3 * si + 2];
+        float volume = m.q[si] * m.length[si] * c->dt;
+        int gl = g.cell_gate[left], gr = g.cell_gate[right];
+        int pl = g.pond[left], pr = g.pond[right];
+        int latch = -1;
+        float into = 0.0f;
+        if (gl >= 0 && gr < 0) {
+            if (pr == 1) { term = 4 * gl; into = volume; latch = gl; }
+            else { term = 4 * gl + 2; into = -volume; }
+        } else if (gr >= 0 && gl < 0) {
+            if (pl == 1) { term = 4 * gr; into = -volume; latch = gr; }
+            else { term = 4 * gr + 2; into = volume; }
+        } else if (pl != pr) {
+            term = 4 * g.count;
+            into = pr == 1 ? volume : -volume;
+        }
+        if (latch >= 0 && volume != 0.0f && atomicOr(&g.flow_seen[latch], 1) == 0) {
+            g.first_flow[2 * latch] = c->step_end[0]; g.first_flow[2 * latch + 1] = c->step_end[1];
+        }
+        v0 = maxf(into, 0.0f);
+        v1 = maxf(-into, 0.0f);
+    }
+    const int T = 4 * g.count + 2;
+    for (int t = 0; t < T; ++t) {
+        float val = term < 0 ? 0.0f : (t == term ? v0 : (t == term + 1 ? v1 : 0.0f));
+        if (!__syncthreads_or(val != 0.0f)) continue;
+        double sum = block_tree((double)val, sh);
+        if (threadIdx.x == 0) {
+            size_t idx = (size_t)blockIdx.x * g.terms + t;
+            acc_add(g.acc_sum + idx, g.acc_comp + idx, sum);
+        }
     }
 }
 
@@ -611,6 +755,7 @@ void enqueue_step(nhf_handle *h)
     const nhf_mesh &m = h->m;
     cudaStream_t s = h->s;
     k_prepare<<<1, 32, 0, s>>>(d);
+    if (h->gate_on) k_gate_move<<<1, 256, 0, s>>>(d, h->gate, 0);
     if (m.hang_cells > 0) k_pressure<<<grid_for(m.hang_cells, 256), 256, 0, s>>>(d);
     if (!d.theta_one) k_face_qn<<<grid_for(m.e_num, 256), 256, 0, s>>>(d);
     int gs = grid_for(m.s_num - 1, 256);
@@ -623,7 +768,13 @@ void enqueue_step(nhf_handle *h)
     }
     k_donor<<<grid_for(m.e_num - 1, 256), 256, 0, s>>>(d);
     k_scale<<<gs, 256, 0, s>>>(d);
-    k_cells<<<d.blocks, kBlock, 0, s>>>(d);
+    if (h->gate_on) {
+        if (h->gate.n_flux > 0) k_gate_flux<<<grid_for(h->gate.n_flux, kBlock), kBlock, 0, s>>>(d, h->gate);
+        k_cells<true><<<d.blocks, kBlock, 0, s>>>(d, h->gate);
+        k_gate_move<<<1, 256, 0, s>>>(d, h->gate, 1);
+    } else {
+        k_cells<false><<<d.blocks, kBlock, 0, s>>>(d, h->gate);
+    }
     int gc = grid_for(m.s_num - 1, 256);
     if (gc > 148 * 8) gc = 148 * 8;
     k_cfl<<<gc, 256, 0, s>>>(d, 1);
@@ -815,6 +966,8 @@ int nhf_destroy(nhf_handle *h)
     if (h->h_acc) cudaFreeHost(h->h_acc);
     if (h->d_ids) cudaFree(h->d_ids);
     if (h->d_samples) cudaFree(h->d_samples);
+    if (h->gate_mem) cudaFree(h->gate_mem);
+    if (h->h_gacc) cudaFreeHost(h->h_gacc);
     if (h->ev_in) cudaEventDestroy(h->ev_in);
     if (h->ev_out) cudaEventDestroy(h->ev_out);
     if (h->s) cudaStreamDestroy(h->s);
@@ -967,6 +1120,82 @@ int nhf_budget_flush(nhf_handle *h, double *totals)
         double s = 0.0, comp = 0.0;
         for (int b = 0; b < blocks; ++b) {
             double parts[2] = {h->h_acc[(size_t)b * T + t], h->h_acc[n + (size_t)b * T + t]};
+            for (int j = 0; j < 2; ++j) {
+                double p = parts[j];
+                double s2 = s + p;
+                if (fabs(s) >= fabs(p)) comp += (s - s2) + p; else comp += (p - s2) + s;
+                s = s2;
+            }
+        }
+        totals[t] = s + comp;
+    }
+    return leave(h);
+}
+
+int nhf_gate_attach(nhf_handle *h, const nhf_gate *gate)
+{
+    if (!h || !gate) return NHF_EINVAL;
+    if (h->tiled) return fail(h, NHF_EINVAL, "gate control runs on the multi-pass step (nhf_params.path = 1)");
+    if (h->gate_on) return fail(h, NHF_ESTATE, "a gate controller is already attached");
+    if (gate->count < 1 || gate->n_targets < 0 || gate->n_flux < 0)
+        return fail(h, NHF_EINVAL, "invalid gate sizes");
+    if (!gate->cell_gate || !gate->pond || !gate->closed || !gate->controls || !gate->commanded ||
+        !gate->command || !gate->flow_seen || !gate->first_flow || !gate->opened || !gate->opened_at ||
+        (gate->n_targets > 0 && !gate->targets) || (gate->n_flux > 0 && !gate->flux_sides))
+        return fail(h, NHF_EINVAL, "gate array missing");
+    if (!(gate->opening_seconds > 0.0f)) return fail(h, NHF_EINVAL, "opening_seconds must be positive");
+    GateDev &g = h->gate;
+    g.count = gate->count; g.n_targets = gate->n_targets; g.n_flux = gate->n_flux;
+    g.terms = 10 * gate->count + 8;
+    const int flux_blocks = grid_for(gate->n_flux, kBlock);
+    g.blocks = flux_blocks > h->dev.blocks ? flux_blocks : h->dev.blocks;
+    g.cell_gate = gate->cell_gate; g.pond = gate->pond; g.targets = gate->targets;
+    g.controls = gate->controls; g.flux_sides = gate->flux_sides; g.closed = gate->closed;
+    g.formal_hi = gate->formal_tick[0]; g.formal_lo = gate->formal_tick[1];
+    g.trigger_level = gate->trigger_level; g.opening_seconds = gate->opening_seconds;
+    g.open_elevation = gate->open_elevation;
+    g.commanded = gate->commanded; g.flow_seen = gate->flow_seen; g.opened = gate->opened;
+    g.command = gate->command; g.first_flow = gate->first_flow; g.opened_at = gate->opened_at;
+    const size_t n = (size_t)g.blocks * g.terms;
+    int rc = enter(h); if (rc) return rc;
+    CK(h, cudaMalloc(&h->gate_mem, 2 * n * sizeof(double)));
+    CK(h, cudaMemsetAsync(h->gate_mem, 0, 2 * n * sizeof(double), h->s));
+    CK(h, cudaMallocHost(&h->h_gacc, 2 * n * sizeof(double)));
+    g.acc_sum = (double *)h->gate_mem;
+    g.acc_comp = g.acc_sum + n;
+    h->gate_on = true;
+    // the step graph is rebuilt with the gate passes at the next batch
+    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+    if (h->graph_def) { cudaGraphDestroy(h->graph_def); h->graph_def = nullptr; }
+    h->begin_node = nullptr;
+    return leave(h);
+}
+
+int nhf_gate_check(nhf_handle *h)
+{
+    if (!h) return NHF_EINVAL;
+    if (!h->gate_on) return fail(h, NHF_ESTATE, "no gate controller attached");
+    int rc = enter(h); if (rc) return rc;
+    k_gate_move<<<1, 256, 0, h->s>>>(h->dev, h->gate, 0);
+    return leave(h);
+}
+
+int nhf_gate_terms(const nhf_handle *h) { return h && h->gate_on ? h->gate.terms : 0; }
+
+int nhf_gate_flush(nhf_handle *h, double *totals)
+{
+    if (!h || !totals) return NHF_EINVAL;
+    if (!h->gate_on) return fail(h, NHF_ESTATE, "no gate controller attached");
+    int rc = enter(h); if (rc) return rc;
+    const int T = h->gate.terms, blocks = h->gate.blocks;
+    const size_t n = (size_t)blocks * T;
+    CK(h, cudaMemcpyAsync(h->h_gacc, h->gate_mem, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaMemsetAsync(h->gate_mem, 0, 2 * n * sizeof(double), h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    for (int t = 0; t < T; ++t) {
+        double s = 0.0, comp = 0.0;
+        for (int b = 0; b < blocks; ++b) {
+            double parts[2] = {h->h_gacc[(size_t)b * T + t], h->h_gacc[n + (size_t)b * T + t]};
             for (int j = 0; j < 2; ++j) {
                 double p = parts[j];
                 double s2 = s + p;

@@ -23,6 +23,7 @@ import numpy as np
 
 from .clock import BAD_CFL, COMPLETED, DONE, TICKS_PER_SECOND, HostClock, seconds_to_ticks, ticks_of, words
 from .forcing import Forcing
+from .gate import GateController, GateLayout, append_gate_balance
 from .geometry import MeshGeometry, connected_still_water
 from .model import MIN_DT, StepParams, build_step_arrays
 from .output import (append_station_samples, read_checkpoint, resolve_station_cells, write_bed,
@@ -51,30 +52,50 @@ def default_engine(arrays, params):
 def evolve(domain_cfg, force_cfg, record, coupling, end_time, engine_factory=None, batch_size=32):
     if coupling is not None:
         raise NotImplementedError('SWMM pipe coupling is not part of this engine')
-    if force_cfg.gate is not None and force_cfg.gate.enabled:
-        raise NotImplementedError('Enabled gate controls are not part of this engine')
     mesh, side_flags = load_mesh(domain_cfg)
     geometry = MeshGeometry.from_mesh(mesh)
     forcing = Forcing.load(domain_cfg, force_cfg, geometry)
     return evolve_loaded(domain_cfg, record, end_time, mesh, side_flags, geometry, forcing,
-                         engine_factory=engine_factory, batch_size=batch_size)
+                         engine_factory=engine_factory, batch_size=batch_size, gate_cfg=force_cfg.gate)
 
 
 def evolve_loaded(domain_cfg, record, end_time, mesh, side_flags, geometry, forcing, *, engine_factory=None,
-                  batch_size=32, state=None):
+                  batch_size=32, state=None, gate_cfg=None):
     """The time loop on an already loaded mesh and forcing. ``state`` may be an
-    in-memory Checkpoint used instead of ``domain_cfg.restart_state``."""
+    in-memory Checkpoint used instead of ``domain_cfg.restart_state``;
+    ``gate_cfg`` is the force config's gate block (a layout is resolved and
+    validated whenever it is present, the controller runs when enabled)."""
     params = StepParams(afa=domain_cfg.afa, sita=domain_cfg.sita, min_h=domain_cfg.min_h, batch_size=batch_size)
     arrays = build_step_arrays(mesh, side_flags, geometry, forcing, domain_cfg.land_parameters, domain_cfg.sita)
+    if state is None and domain_cfg.restart_state:
+        state = read_checkpoint(domain_cfg.restart_state)
+    # the gate layout and closed bed come from the mesh bed (solver_compact.py:202-203, 297-299)
+    layout = (GateLayout.load(gate_cfg, geometry.bounds, mesh.land_type, mesh.topology, forcing.boundaries,
+                              arrays.bed) if gate_cfg is not None else None)
+    controller = None
+    if gate_cfg is not None and gate_cfg.enabled:
+        controller = GateController.build(gate_cfg, layout, arrays.bed, mesh.land_type, mesh.topology,
+                                          _clock_origin(domain_cfg, state))
+        arrays.gate = controller.tables
     engine = (engine_factory or default_engine)(arrays, params)
     try:
         record.device(engine.backend, engine.device_name)
-        return _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, batch_size, state)
+        return _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, batch_size, state,
+                    gate_cfg=gate_cfg, layout=layout, controller=controller)
     finally:
         engine.close()
 
 
-def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, batch_size, state=None):
+def _clock_origin(domain_cfg, state) -> float:
+    """Seconds of clock before formal time 0 (solver_compact.py:280-284)."""
+    meta = json.loads(state.metadata_json) if state else {}
+    if meta.get('run_state', False):
+        return meta['clock_origin_before_start_s']
+    return domain_cfg.warmup_duration
+
+
+def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, batch_size, state=None, *,
+         gate_cfg=None, layout=None, controller=None):
     e_num, s_num = mesh.e_num, mesh.s_num
     b_num = len(forcing.boundaries)
     afa, sita, min_h = domain_cfg.afa, domain_cfg.sita, domain_cfg.min_h
@@ -85,8 +106,7 @@ def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, 
         state = read_checkpoint(domain_cfg.restart_state)
     state_meta = json.loads(state.metadata_json) if state else {}
     continuation = bool(state_meta.get('run_state', False))
-    origin_before_start = (state_meta['clock_origin_before_start_s'] if continuation
-                           else domain_cfg.warmup_duration)
+    origin_before_start = _clock_origin(domain_cfg, state)
     initial_clock = ((state.clock_hi * 2 ** 32 + state.clock_lo) / 2 ** 40 if state else 0.)
     if state:
         end_tick = seconds_to_ticks(end_time + origin_before_start)
@@ -109,7 +129,7 @@ def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, 
     state_identity = {
         'ne_sha256': inputs.get(str(Path(domain_cfg.ne).resolve())),
         'ns_sha256': inputs.get(str(Path(domain_cfg.ns).resolve())),
-        'gate_config': 'null',
+        'gate_config': gate_cfg.model_dump_json() if gate_cfg is not None else 'null',
     }
     boundary_identity = [dict(name=b.name, kind=b.kind, selected_edges_sha256=hashlib.sha256(
         np.sort(b.side_ids).astype('<i8').tobytes()).hexdigest()) for b in forcing.boundaries]
@@ -132,6 +152,8 @@ def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, 
             engine.set(name, getattr(state, name))
         engine.set('peak_hi', state.first_time_hi)
         engine.set('peak_lo', state.first_time_lo)
+        if controller is not None and continuation:
+            engine.set_gate_state(controller.restore(state_meta['gate_controller']))
     bed_np = engine.get('bed')
     root = Path(domain_cfg.output_dir)
     record.data.update(bed_events=[], output={
@@ -152,7 +174,7 @@ def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, 
     previous_steps = state_meta['total_steps'] if continuation else 0
     previous_warmup_steps = state_meta['total_warmup_steps'] if continuation else 0
     discharge_peaks = np.zeros(b_num, dtype=np.float64)
-    record.data['gate_cell_count'] = 0
+    record.data['gate_cell_count'] = int(np.count_nonzero(layout.cell_gate >= 0)) if layout is not None else 0
     record.data['station_cells'] = station_cells
     coefficients = np.zeros((max(1, b_num), 2), dtype=np.float32)
     previous_coefficients = np.full_like(coefficients, np.nan)
@@ -204,11 +226,14 @@ def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, 
                         budget={'initial_storage_m3': budget.initial, 'rainfall_m3': float(budget.rain),
                                 'requested_discharge_m3': budget.discharge.tolist(),
                                 'device_totals': device_totals.tolist()})
+        if controller is not None:
+            metadata['gate_controller'] = controller.snapshot()
         tick_count = seconds_to_ticks(clock.host_now_seconds)
         peak_hi, peak_lo = engine.get('peak_hi'), engine.get('peak_lo')
         write_checkpoint(path, depth=depth_np, bed=engine.get('bed'), q=engine.get('q'),
                          rain_time=engine.get('rain_time'), infiltration=engine.get('infiltration'),
-                         clock_hi=tick_count >> 32, clock_lo=tick_count & 0xffffffff, gate_open=False,
+                         clock_hi=tick_count >> 32, clock_lo=tick_count & 0xffffffff,
+                         gate_open=controller.gate_open if controller is not None else False,
                          metadata_json=json.dumps(metadata), max_depth=engine.get('max_depth'),
                          first_time_hi=peak_hi, first_time_lo=peak_lo, max_speed=engine.get('max_speed'))
         s.last_checkpoint_wall = perf_counter()
@@ -222,6 +247,12 @@ def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, 
         depth_np = engine.get('depth')
         storage = float(np.sum(depth_np.astype(float) * area_f64, dtype=np.float64))
         row = budget.output(date, seconds, storage, phase)
+        if controller is not None:
+            controller.pull(engine)
+            record.data['gate_control'] = controller.report(depth_np, area_f64, seconds)
+            append_gate_balance(Path(domain_cfg.domain_dir) / 'gate_balance.csv', date, seconds,
+                                record.data['gate_control'])
+            record.write()
         if len(station_names):
             samples = engine.sample_stations(station_ids)
             append_station_samples(root / 'stations.csv', elapsed_seconds=seconds, time=date.isoformat(),
@@ -296,6 +327,10 @@ def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, 
                 targets[b.cells] = np.maximum(b.series.at(0.) - bed_np[b.cells].astype(float), 0.)
         engine.apply_initial_levels(targets)
     engine.set_active(1)
+    if controller is not None:
+        if controller.initial_storage is None:
+            controller.initialize_inventory(engine.get('depth'), area_f64)
+        engine.gate_check()
     engine.compute_cfl()
     engine.initial_diagnostics()
     if s.elapsed == 0. and end_time > 0.:
@@ -373,7 +408,7 @@ def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, 
                                   minimum_donor_scale=total_activity[2]),
             requested_discharge_peak_m3_s={b.name: float(discharge_peaks[i])
                                            for i, b in enumerate(forcing.boundaries) if b.kind == 'discharge'},
-            gate_open=False,
+            gate_open=bool(np.any(engine.gate_state()['commanded'])) if controller is not None else False,
             storage_depth_one_ulp_volume_m3=float(np.sum(np.abs(np.spacing(final_depth[1:])) * geometry.area[1:],
                                                          dtype=np.float64)))
         peak = engine.peak_memory()

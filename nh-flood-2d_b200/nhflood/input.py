@@ -45,8 +45,8 @@ class GatePointConfig(InputModel):
 
 
 class GateConfig(InputModel):
-    """Accepted for schema compatibility; the gate controller is not part of
-    this engine and an enabled gate is rejected when a run starts."""
+    """The gate controller block (input/force.py:38-56); resolved by
+    nhflood.gate.GateLayout, run on the device when enabled."""
     land_type: int = Field(ge=0, le=255)
     pond_land_type: int = Field(ge=0, le=255)
     enabled: bool

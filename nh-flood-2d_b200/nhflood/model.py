@@ -63,6 +63,7 @@ class StepArrays:
     slots: np.ndarray | None = None
     hcells: np.ndarray | None = None
     axes: np.ndarray | None = None
+    gate: object = None  # nhflood.gate.GateTables when a gate controller is enabled
     extra: dict = field(default_factory=dict)
 
     @property

@@ -33,6 +33,17 @@ class NhfParams(ctypes.Structure):
                 ('min_dt', c_float), ('batch_size', c_int32), ('path', c_int32)]
 
 
+_GATE_TABLES = ('cell_gate', 'pond', 'closed', 'targets', 'controls', 'flux_sides')
+_GATE_WORDS = ('commanded', 'flow_seen', 'opened', 'command', 'first_flow', 'opened_at')
+
+
+class NhfGate(ctypes.Structure):
+    _fields_ = ([('count', c_int32), ('n_targets', c_int32), ('n_flux', c_int32)]
+                + [(n, c_void_p) for n in _GATE_TABLES] + [('formal_tick', c_uint32 * 2)]
+                + [(n, c_float) for n in ('trigger_level', 'opening_seconds', 'open_elevation')]
+                + [(n, c_void_p) for n in _GATE_WORDS])
+
+
 _LIB = None
 
 
@@ -79,6 +90,10 @@ def library(path=None):
         'nhf_cfl_noalloc': (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_float, c_float,
                                       c_void_p, c_void_p, c_void_p]),
         'nhf_cfl_noalloc_error': (ctypes.c_char_p, []),
+        'nhf_gate_attach': (c_int32, [H, POINTER(NhfGate)]),
+        'nhf_gate_check': (c_int32, [H]),
+        'nhf_gate_terms': (c_int32, [H]),
+        'nhf_gate_flush': (c_int32, [H, POINTER(c_double)]),
         'nhf_ensemble_create': (c_int32, [POINTER(c_void_p), c_int32, c_int32, c_void_p, POINTER(c_void_p)]),
         'nhf_ensemble_destroy': (c_int32, [H]),
         'nhf_ensemble_last_error': (ctypes.c_char_p, [H]),
@@ -104,6 +119,7 @@ def exported_symbols() -> list[str]:
             'nhf_run_batch_async', 'nhf_read_trace', 'nhf_budget_flush', 'nhf_budget_terms', 'nhf_get_cfl',
             'nhf_limits', 'nhf_reset_limits', 'nhf_sample_stations', 'nhf_read_eq', 'nhf_read_gradients',
             'nhf_synchronize', 'nhf_stream', 'nhf_path', 'nhf_cfl_noalloc', 'nhf_cfl_noalloc_error',
+            'nhf_gate_attach', 'nhf_gate_check', 'nhf_gate_terms', 'nhf_gate_flush',
             'nhf_ensemble_create', 'nhf_ensemble_destroy', 'nhf_ensemble_last_error', 'nhf_ensemble_info',
             'nhf_ensemble_stream', 'nhf_ensemble_run_batch', 'nhf_ensemble_run_batch_async',
             'nhf_ensemble_read_trace']
@@ -178,8 +194,12 @@ class CudaEngine(Engine):
             tensor = self.t.get(name)
             setattr(mesh, name, tensor.data_ptr() if tensor is not None else None)
         self._mesh = mesh
-        p = NhfParams(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size,
-                      path_code(params.path))
+        path = path_code(params.path)
+        if arrays.gate is not None:
+            if path not in (0, 1):
+                raise ValueError('gate control runs on the multi-pass step; use path "auto" or "multipass"')
+            path = 1
+        p = NhfParams(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size, path)
         handle = c_void_p()
         with torch.cuda.device(dev):
             stream = torch.cuda.current_stream(dev).cuda_stream
@@ -190,6 +210,58 @@ class CudaEngine(Engine):
         self.terms = self.lib.nhf_budget_terms(self.h)
         self.path = self.lib.nhf_path(self.h).decode()
         self._trace = np.zeros((self.batch_size, NHF_TRACE_COLS), dtype=np.uint32)
+        self.gate = arrays.gate
+        if self.gate is not None:
+            self._attach_gate(self.gate)
+
+    def _attach_gate(self, tables):
+        """Device copies of the controller tables and words, attached to the
+        handle (nhf_gate_attach)."""
+        from .gate import STATE_FIELDS
+        torch, dev = self.torch, self.device
+        gate = NhfGate()
+        gate.count, gate.n_targets, gate.n_flux = tables.count, len(tables.targets), len(tables.flux_sides)
+        self.gt = {}
+        for name in _GATE_TABLES:
+            a = getattr(tables, name)
+            a = np.ascontiguousarray(a, dtype=np.float32 if name == 'closed' else np.int32)
+            t = torch.from_numpy(a if len(a) else np.zeros(1, a.dtype)).to(dev)
+            self.gt[name] = t
+            setattr(gate, name, t.data_ptr())
+        gate.formal_tick[0], gate.formal_tick[1] = tables.formal_tick >> 32, tables.formal_tick & 0xffffffff
+        gate.trigger_level, gate.opening_seconds = tables.trigger_level, tables.opening_seconds
+        gate.open_elevation = tables.open_elevation
+        self.gate_fields = STATE_FIELDS
+        for name, dtype, width in STATE_FIELDS:
+            t = torch.zeros((tables.count, width) if width > 1 else tables.count, dtype=torch.int32, device=dev)
+            self.gt[name] = t
+            setattr(gate, name, t.data_ptr())
+        self._gate = gate
+        self._check(self.lib.nhf_gate_attach(self.h, ctypes.byref(gate)), 'nhf_gate_attach')
+        self.gate_terms = self.lib.nhf_gate_terms(self.h)
+
+    def gate_check(self):
+        self._check(self.lib.nhf_gate_check(self.h), 'nhf_gate_check')
+
+    def gate_flush(self):
+        out = np.zeros(self.gate_terms, dtype=np.float64)
+        self._check(self.lib.nhf_gate_flush(self.h, out.ctypes.data_as(POINTER(c_double))), 'nhf_gate_flush')
+        return out
+
+    def gate_state(self) -> dict:
+        """The controller words (commanded, command ticks, first flow,
+        opened) as host arrays."""
+        out = {}
+        for name, dtype, _ in self.gate_fields:
+            out[name] = self.gt[name].cpu().numpy().view(dtype) if dtype == np.uint32 else \
+                self.gt[name].cpu().numpy().astype(dtype)
+        return out
+
+    def set_gate_state(self, state: dict) -> None:
+        for name, dtype, _ in self.gate_fields:
+            t = self.gt[name]
+            a = np.ascontiguousarray(np.asarray(state[name]).astype(dtype).reshape(tuple(t.shape)))
+            t.copy_(self.torch.from_numpy(a.view(np.int32)))
 
     # -- helpers ----------------------------------------------------------
     def _check(self, rc, what):

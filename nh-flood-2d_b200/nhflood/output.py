@@ -227,16 +227,37 @@ def read_manifest(path):
 
 
 class BedTimeline:
-    """Working bed at a frame time: bed.fdb plus recorded bed events
-    (output.py:299-343; gate opening records are not produced by this engine)."""
+    """Working bed at a frame time: bed.fdb plus recorded bed events, then the
+    gate beds re-derived from the manifest's ``gate_control`` block with the
+    device's F32 opening arithmetic (output.py:299-343)."""
 
     def __init__(self, output_root, manifest=None, expected_count=None):
         output_root = Path(output_root)
         manifest = read_manifest(output_root.parent / 'manifest.json') if manifest is None else manifest
         self.bed = read_bed(output_root / 'bed.fdb', expected_count)
         self.events = sorted(manifest.get('bed_events', []), key=lambda e: e['elapsed_seconds'])
+        self.gate_control = manifest.get('gate_control', {})
         self.cursor = 0
         self.seconds = float('-inf')
+
+    def _gate_beds(self, elapsed_seconds):
+        control = self.gate_control
+        f32 = np.float32
+        for gate in control.get('gates', []):
+            cells = np.asarray(gate['cell_ids'], dtype=np.int64)
+            closed = np.asarray(gate['closed_elevation'], dtype=f32)
+            fraction = f32(0.)
+            command = gate['command_seconds']
+            if command is not None and elapsed_seconds >= command:
+                hi, lo = gate['command_clock_ticks']
+                tick = round((elapsed_seconds + control['clock_origin_before_start_s']) * 2 ** 40)
+                age_ticks = max(tick - ((int(hi) << 32) | int(lo)), 0)
+                age = f32(age_ticks >> 32) / f32(256.) + f32(age_ticks & 0xffffffff) * f32(2. ** -40)
+                fraction = np.minimum(age / f32(control['opening_seconds']), f32(1.))
+            opened = f32(control['open_elevation'])
+            self.bed[cells] = closed + (opened - closed) * fraction
+            if fraction >= 1.:
+                self.bed[cells] = opened
 
     def at(self, elapsed_seconds):
         if elapsed_seconds < self.seconds:
@@ -250,6 +271,7 @@ class BedTimeline:
             self.bed[ids] = new_bed
             self.cursor += 1
         self.seconds = elapsed_seconds
+        self._gate_beds(elapsed_seconds)
         return self.bed
 
 

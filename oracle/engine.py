@@ -51,6 +51,17 @@ def _mesh_type(real):
     return OraMeshT
 
 
+_GATE_TABLES = ('cell_gate', 'pond', 'closed', 'targets', 'controls', 'flux_sides')
+_GATE_WORDS = ('commanded', 'flow_seen', 'opened', 'command', 'first_flow', 'opened_at')
+
+
+class OraGate(ctypes.Structure):
+    _fields_ = ([('count', c_int32), ('n_targets', c_int32), ('n_flux', c_int32)]
+                + [(n, c_void_p) for n in _GATE_TABLES] + [('formal_tick', c_uint32 * 2)]
+                + [(n, c_float) for n in ('trigger_level', 'opening_seconds', 'open_elevation')]
+                + [(n, c_void_p) for n in _GATE_WORDS])
+
+
 OraMesh = _mesh_type(c_float)
 _MESH = {'f32': OraMesh, 'f64': _mesh_type(c_double)}
 _REAL = {'f32': c_float, 'f64': c_double}
@@ -85,6 +96,8 @@ def library(precision: str = 'f32'):
             ('ora_pressure_difference', R, [H, c_int, c_int, c_int, R]),
             ('ora_ln', c_double, [c_double]), ('ora_exp', c_double, [c_double]),
             ('ora_powf', c_float, [c_float, c_float]), ('ora_expf', c_float, [c_float]),
+            ('ora_gate_attach', None, [H, POINTER(OraGate)]), ('ora_gate_check', None, [H]),
+            ('ora_gate_terms', c_int, [H]), ('ora_gate_flush', None, [H, POINTER(c_double)]),
         ]:
             fn = getattr(lib, name)
             fn.restype = res
@@ -151,6 +164,43 @@ class OracleEngine:
         self.h = self.lib.ora_create(ctypes.byref(m))
         self.terms = self.lib.ora_budget_terms(self.h)
         self._trace = np.zeros((self.batch_size, TRACE_COLS), np.uint32)
+        self.gate = getattr(arrays, 'gate', None)
+        if self.gate is not None:
+            self._attach_gate(self.gate)
+
+    def _attach_gate(self, t):
+        from nhflood.gate import STATE_FIELDS
+        g = OraGate()
+        g.count, g.n_targets, g.n_flux = t.count, len(t.targets), len(t.flux_sides)
+        for name in _GATE_TABLES:
+            dtype = self.real if name == 'closed' else np.int32
+            a = np.ascontiguousarray(getattr(t, name), dtype=dtype)
+            self.keep['gate_' + name] = a
+            setattr(g, name, a.ctypes.data)
+        g.formal_tick[0], g.formal_tick[1] = t.formal_tick >> 32, t.formal_tick & 0xffffffff
+        g.trigger_level, g.opening_seconds, g.open_elevation = t.trigger_level, t.opening_seconds, t.open_elevation
+        self.gate_words = {name: np.zeros((t.count, width) if width > 1 else t.count, dtype=dtype)
+                           for name, dtype, width in STATE_FIELDS}
+        for name in _GATE_WORDS:
+            setattr(g, name, self.gate_words[name].ctypes.data)
+        self._gate = g
+        self.lib.ora_gate_attach(self.h, ctypes.byref(g))
+        self.gate_terms = self.lib.ora_gate_terms(self.h)
+
+    def gate_check(self):
+        self.lib.ora_gate_check(self.h)
+
+    def gate_flush(self):
+        out = np.zeros(self.gate_terms, np.float64)
+        self.lib.ora_gate_flush(self.h, out.ctypes.data_as(POINTER(c_double)))
+        return out
+
+    def gate_state(self) -> dict:
+        return {name: a.copy() for name, a in self.gate_words.items()}
+
+    def set_gate_state(self, state: dict) -> None:
+        for name, a in self.gate_words.items():
+            a[...] = np.asarray(state[name]).astype(a.dtype).reshape(a.shape)
 
     def get(self, name):
         return self.state[name].copy()

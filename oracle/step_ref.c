@@ -14,6 +14,8 @@
  *   diagnostics    core/solver_compact.py:657-679
  *   pressure       core/pressure.py:65-129
  *   face_discharge, boundary_neighbor_sum  core/solver_compact.py:118-149
+ *   gate controller core/gate.py:68-206; its passes in the step graph
+ *                  core/solver_compact.py:896-906, hooks 523-524, 595-604
  * Pass structure and operation order follow the reference literally. Scalar
  * constants are F32 (Taichi default_fp); Python-only constant expressions
  * such as (1 - sita) / 2 are folded in F64 first, as Taichi folds them.
@@ -82,6 +84,10 @@ struct ora_ctx {
     real *diag;      /* [blocks*terms] per-step f32 values per cell collected per block */
     double *acc_sum, *acc_comp; /* [blocks*terms] */
     uint32_t *trace;  /* [batch][10] */
+    /* gate controller */
+    int gate_on, gterms, gblocks;
+    ora_gate gate;
+    double *gacc_sum, *gacc_comp; /* [gblocks*gterms] */
 };
 
 void ora_set_threads(int n)
@@ -130,6 +136,7 @@ void ora_destroy(ora_ctx *c)
     free(c->sdc); free(c->dh); free(c->eq); free(c->increment); free(c->rain_depth);
     free(c->donor_scale); free(c->cfl); free(c->flow_depth); free(c->face_qn); free(c->ssq);
     free(c->gradients); free(c->acc_sum); free(c->acc_comp); free(c->trace);
+    free(c->gacc_sum); free(c->gacc_comp);
     free(c);
 }
 
@@ -227,6 +234,177 @@ void ora_budget_flush(ora_ctx *c, double *totals)
     }
     memset(c->acc_sum, 0, sizeof(double) * (size_t)c->blocks * T);
     memset(c->acc_comp, 0, sizeof(double) * (size_t)c->blocks * T);
+}
+
+/* ---- gate controller (core/gate.py:68-206) ------------------------------ */
+
+void ora_gate_attach(ora_ctx *c, const ora_gate *gate)
+{
+    c->gate = *gate;
+    c->gate_on = 1;
+    c->gterms = 10 * gate->count + 8;
+    int flux_blocks = (gate->n_flux + BLOCK - 1) / BLOCK;
+    c->gblocks = flux_blocks > c->blocks ? flux_blocks : c->blocks;
+    free(c->gacc_sum); free(c->gacc_comp);
+    c->gacc_sum = (double *)calloc((size_t)c->gblocks * c->gterms, sizeof(double));
+    c->gacc_comp = (double *)calloc((size_t)c->gblocks * c->gterms, sizeof(double));
+}
+
+int ora_gate_terms(const ora_ctx *c) { return c->gate_on ? c->gterms : 0; }
+
+static void gate_acc_add(ora_ctx *c, int blk, int term, double p)
+{
+    size_t idx = (size_t)blk * c->gterms + term;
+    double sum = c->gacc_sum[idx];
+    double s = sum + p;
+    double bp = s - sum;
+    double err = (sum - (s - bp)) + (p - bp);
+    c->gacc_comp[idx] += err;
+    c->gacc_sum[idx] = s;
+}
+
+/* since_command (gate.py:68-73): clock age of the command in F32 seconds */
+static float since_command(const ora_gate *g, int gate, uint32_t hi, uint32_t lo)
+{
+    uint32_t borrow = lo < g->command[2 * gate + 1] ? 1u : 0u;
+    uint32_t high = hi - g->command[2 * gate] - borrow;
+    uint32_t low = lo - g->command[2 * gate + 1];
+    return (float)high / 256.0f + (float)low * 0x1p-40f;
+}
+
+/* move (gate.py:75-86): the working bed of every commanded gate at (hi, lo) */
+static void gate_move(ora_ctx *c, uint32_t hi, uint32_t lo)
+{
+    const ora_gate *g = &c->gate;
+    if (!c->active) return;
+    for (int slot = 0; slot < g->n_targets; ++slot) {
+        int cell = g->targets[slot];
+        int gate = g->cell_gate[cell];
+        if (g->commanded[gate] != 1) continue;
+        float fraction = minf(since_command(g, gate, hi, lo) / g->opening_seconds, 1.0f);
+        if (fraction >= 1.0f) {
+            c->m.bed[cell] = (real)g->open_elevation;
+            if (!g->opened[gate]) {
+                g->opened[gate] = 1;
+                g->opened_at[2 * gate] = hi; g->opened_at[2 * gate + 1] = lo;
+            }
+        } else {
+            real closed = g->closed[cell];
+            c->m.bed[cell] = closed + ((real)g->open_elevation - closed) * (real)fraction;
+        }
+    }
+}
+
+/* check (gate.py:88-99): irreversible command once the control cell is wet
+ * and its level exceeds the trigger, from formal time 0 on; then move */
+void ora_gate_check(ora_ctx *c)
+{
+    const ora_gate *g = &c->gate;
+    const ora_mesh *m = &c->m;
+    if (!c->gate_on || !c->active) return;
+    uint32_t hi = c->now[0], lo = c->now[1];
+    int formal = hi > g->formal_tick[0] || (hi == g->formal_tick[0] && lo >= g->formal_tick[1]);
+    for (int gate = 0; gate < g->count && formal; ++gate) {
+        int cell = g->controls[gate];
+        if (g->commanded[gate] == 0 && m->depth[cell] >= m->min_h
+            && m->bed[cell] + m->depth[cell] > (real)g->trigger_level) {
+            g->commanded[gate] = 1;
+            g->command[2 * gate] = hi; g->command[2 * gate + 1] = lo;
+        }
+    }
+    gate_move(c, hi, lo);
+}
+
+/* record_flux (gate.py:118-140) over the recorded sides after the limiter:
+ * term and value pairs of one side; at most two are nonzero. */
+static int gate_flux_terms(ora_ctx *c, int si, int terms[2], real values[2])
+{
+    const ora_gate *g = &c->gate;
+    const ora_mesh *m = &c->m;
+    int left = m->topology[3 * si + 1], right = m->topology[3 * si + 2];
+    real volume = m->q[si] * m->length[si] * c->dt;
+    int gl = g->cell_gate[left], gr = g->cell_gate[right];
+    int pl = g->pond[left], pr = g->pond[right];
+    int term = -1, latch = -1;
+    real into = R(0.0);
+    if (gl >= 0 && gr < 0) {
+        if (pr == 1) { term = 4 * gl; into = volume; latch = gl; }
+        else { term = 4 * gl + 2; into = -volume; }
+    } else if (gr >= 0 && gl < 0) {
+        if (pl == 1) { term = 4 * gr; into = -volume; latch = gr; }
+        else { term = 4 * gr + 2; into = volume; }
+    } else if (pl != pr) {
+        term = 4 * g->count;
+        into = pr == 1 ? volume : -volume;
+    }
+    if (latch >= 0 && volume != R(0.0) && !g->flow_seen[latch]) {
+        g->flow_seen[latch] = 1;
+        g->first_flow[2 * latch] = c->step_end[0]; g->first_flow[2 * latch + 1] = c->step_end[1];
+    }
+    terms[0] = term; terms[1] = term + 1;
+    values[0] = maxf(into, R(0.0));
+    values[1] = maxf(-into, R(0.0));
+    return term >= 0;
+}
+
+static void gate_record_fluxes(ora_ctx *c)
+{
+    const ora_gate *g = &c->gate;
+    int nblk = (g->n_flux + BLOCK - 1) / BLOCK;
+    int T = 4 * g->count + 2;  /* exchange terms */
+    real *vals = (real *)calloc((size_t)BLOCK * T, sizeof(real));
+    for (int blk = 0; blk < nblk; ++blk) {
+        memset(vals, 0, sizeof(real) * (size_t)BLOCK * T);
+        for (int i = 0; i < BLOCK; ++i) {
+            int p = blk * BLOCK + i;
+            if (p >= g->n_flux) break;
+            int terms[2]; real values[2];
+            if (!gate_flux_terms(c, g->flux_sides[p], terms, values)) continue;
+            vals[(size_t)i * T + terms[0]] = values[0];
+            vals[(size_t)i * T + terms[1]] = values[1];
+        }
+        double v[BLOCK];
+        for (int t = 0; t < T; ++t) {
+            int any = 0;
+            for (int i = 0; i < BLOCK; ++i) {
+                real val = vals[(size_t)i * T + t];
+                v[i] = (double)val;
+                any |= val != R(0.0);
+            }
+            if (any) gate_acc_add(c, blk, t, block_tree(v));
+        }
+    }
+    free(vals);
+}
+
+/* source_offset (gate.py:142-149): first of the six source terms of a pond
+ * or gate cell, -1 elsewhere */
+static int gate_source_offset(const ora_ctx *c, int cell)
+{
+    const ora_gate *g = &c->gate;
+    if (g->pond[cell] == 1) return 4 * g->count + 2;
+    if (g->cell_gate[cell] >= 0) return 4 * g->count + 8 + 6 * g->cell_gate[cell];
+    return -1;
+}
+
+void ora_gate_flush(ora_ctx *c, double *totals)
+{
+    int T = c->gterms;
+    for (int t = 0; t < T; ++t) {
+        double s = 0.0, comp = 0.0;
+        for (int blk = 0; blk < c->gblocks; ++blk) {
+            double parts[2] = {c->gacc_sum[(size_t)blk * T + t], c->gacc_comp[(size_t)blk * T + t]};
+            for (int j = 0; j < 2; ++j) {
+                double p = parts[j];
+                double n = s + p;
+                if (fabs(s) >= fabs(p)) comp += (s - n) + p; else comp += (p - n) + s;
+                s = n;
+            }
+        }
+        totals[t] = s + comp;
+    }
+    memset(c->gacc_sum, 0, sizeof(double) * (size_t)c->gblocks * T);
+    memset(c->gacc_comp, 0, sizeof(double) * (size_t)c->gblocks * T);
 }
 
 /* ---- setup kernels -------------------------------------------------------- */
@@ -637,6 +815,8 @@ static void tick(ora_ctx *c)
         m->q[si] *= c->donor_scale[donor];
     }
     c->limited_faces += limited_faces;
+    /* controller.record_flux on the post-limiter volumes (solver_compact.py:523-524) */
+    if (c->gate_on) gate_record_fluxes(c);
 
     /* cell fluxes, sources and depth update (solver_compact.py:525-610);
      * processed per 256-cell budget block. */
@@ -645,6 +825,9 @@ static void tick(ora_ctx *c)
 #pragma omp parallel for schedule(static) reduction(+ : wet)
     for (int blk = 0; blk < c->blocks; ++blk) {
         real *diag = (real *)calloc((size_t)BLOCK * T, sizeof(real));
+        real gvals[6 * BLOCK];
+        int goff[BLOCK];
+        for (int i = 0; i < BLOCK; ++i) goff[i] = -1;
         int e0 = blk * BLOCK;
         for (int i = 0; i < BLOCK; ++i) {
             int ei = e0 + i;
@@ -707,6 +890,24 @@ static void tick(ora_ctx *c)
                 dg[1] += floor_v * ea;
                 m->depth[ei] = maxf(raw_depth, R(0.0));
             }
+            /* controller.record_cell + measure_inventory + collect's rounding
+             * term (solver_compact.py:595-604; gate.py:151-193) */
+            if (c->gate_on && (goff[i] = gate_source_offset(c, ei)) >= 0) {
+                real applied_floor = floor_v, level_exchange = R(0.0);
+                if (bi >= 0 && m->kind[bi] == 0) {
+                    applied_floor = R(0.0);
+                    level_exchange = (m->depth[ei] - previous) * ea - (ql - qr + qb - qt) * dt - pipe * dt
+                                     - rain_depth * ea + removed * ea;
+                }
+                real *gv = gvals + 6 * i;
+                gv[0] = rain_depth * ea;
+                gv[1] = removed * ea;
+                gv[2] = applied_floor * ea;
+                gv[3] = pipe * dt;
+                gv[4] = (c->ssq[ei] - pipe) * dt + level_exchange;
+                real rounding = (m->depth[ei] - previous) - c->increment[ei] + removed - applied_floor;
+                gv[5] = rounding * ea - level_exchange;
+            }
             real u, v;
             velocity(c, ei, &u, &v);
             m->u[ei] = u; m->v[ei] = v;
@@ -728,6 +929,22 @@ static void tick(ora_ctx *c)
             }
             if (any) acc_add(c, (size_t)blk * T + t, block_tree(v));
         }
+        /* gate source terms: the pond group, then gate by gate */
+        for (int grp = -1; c->gate_on && grp < c->gate.count; ++grp) {
+            int off = grp < 0 ? 4 * c->gate.count + 2 : 4 * c->gate.count + 8 + 6 * grp;
+            int member = 0;
+            for (int i = 0; i < BLOCK; ++i) member |= goff[i] == off;
+            if (!member) continue;
+            for (int k = 0; k < 6; ++k) {
+                int any = 0;
+                for (int i = 0; i < BLOCK; ++i) {
+                    real val = goff[i] == off ? gvals[6 * i + k] : R(0.0);
+                    v[i] = (double)val;
+                    any |= val != R(0.0);
+                }
+                if (any) gate_acc_add(c, blk, off + k, block_tree(v));
+            }
+        }
         free(diag);
     }
     c->wet = wet;
@@ -741,8 +958,10 @@ void ora_run_batch(ora_ctx *c, const uint32_t target[2], const uint32_t origin[2
     c->slot = 0;
     for (int s = 0; s < c->m.batch_size; ++s) {
         prepare_step(c);
+        if (c->gate_on) ora_gate_check(c);
         if (c->active && c->m.hang_cells > 0) ora_update_pressure(c);
         tick(c);
+        if (c->gate_on) gate_move(c, c->step_end[0], c->step_end[1]);  /* finish_gate_bed */
         ora_compute_cfl(c);
         finish_step(c);
     }

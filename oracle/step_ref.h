@@ -107,6 +107,31 @@ void ora_read_gradients(const ora_ctx *c, ora_real *out /* [hang_cells*2] */);
 void ora_update_pressure(ora_ctx *c);
 ora_real ora_pressure_difference(const ora_ctx *c, int side, int lower, int higher, ora_real raw);
 
+/* Gate controller (core/gate.py:35-206). Tables and controller words are
+ * caller-owned and stay alive while attached. Exchange terms (gate/pond and
+ * gate/river volumes, overtopping) are accumulated per 256 entries of
+ * flux_sides; source terms (rain, infiltration, positivity, pipe, boundary,
+ * rounding of pond and gate cells) per 256 cells. Terms: 10 count + 8. */
+typedef struct {
+    int32_t count, n_targets, n_flux;
+    const int32_t *cell_gate;  /* [e_num] gate index of each cell, -1 off gates */
+    const int32_t *pond;       /* [e_num] 1 on pond cells, 0 at the sentinel */
+    const ora_real *closed;    /* [e_num] closed bed */
+    const int32_t *targets;    /* [n_targets] gate cells, gate by gate */
+    const int32_t *controls;   /* [count] control cell of each gate */
+    const int32_t *flux_sides; /* [n_flux] recorded sides in side order */
+    uint32_t formal_tick[2];   /* control starts at this clock (formal t = 0) */
+    float trigger_level, opening_seconds, open_elevation;
+    int32_t *commanded, *flow_seen, *opened; /* [count] */
+    uint32_t *command, *first_flow, *opened_at; /* [count*2] hi, lo */
+} ora_gate;
+void ora_gate_attach(ora_ctx *c, const ora_gate *gate);
+/* check + move at the current clock (the run-start check_gates call) */
+void ora_gate_check(ora_ctx *c);
+int ora_gate_terms(const ora_ctx *c);
+/* interval totals since the last flush, in term order; clears them */
+void ora_gate_flush(ora_ctx *c, double *totals);
+
 /* mathref.c */
 double ora_ln(double x);
 double ora_exp(double y);

@@ -128,7 +128,9 @@ def grid3_mesh(path: Path, bed=0.):
 
 def rectangles_mesh(path: Path, cells, bed, land_type=10):
     """Square cells (x0, x1, y0, y1); each face is split at the corners of its
-    neighbours; sides are numbered in sorted (orient, coordinate, a, b) order."""
+    neighbours; sides are numbered in sorted (orient, coordinate, a, b) order.
+    land_type is one class for every cell or a list with one per cell."""
+    types = list(land_type) if np.ndim(land_type) else [land_type] * len(cells)
     breaks = {1: defaultdict(set), 2: defaultdict(set)}
     for x0, x1, y0, y1 in cells:
         breaks[2][x0].update((y0, y1)); breaks[2][x1].update((y0, y1))
@@ -151,7 +153,7 @@ def rectangles_mesh(path: Path, cells, bed, land_type=10):
     for ei, ((x0, x1, y0, y1), per) in enumerate(zip(cells, faces), 1):
         ids = [sid[k] for keys in per for k in keys]
         ne.append(','.join(map(str, [ei, *(len(k) for k in per), *ids, (x0 + x1) / 2, (y0 + y1) / 2,
-                                     bed[ei], land_type])))
+                                     bed[ei], types[ei - 1]])))
     ns = []
     topo = np.zeros((len(sid) + 1, 3), dtype=np.int64)
     side_xy = np.zeros((len(sid) + 1, 2))
