@@ -340,3 +340,122 @@ def test_disabled_gate_runs_without_controller_and_keeps_identity(tmp_path):
     assert r.manifest['gate_cell_count'] == 1
     assert r.state.bed[2] == 10
     assert not r.state.gate_open
+
+
+def paired_section(path, *, hanging, regime):
+    """The same 8 m river-to-pond section with one whole pond face or two
+    split ones (tests/test_gate_extended.py:63-83)."""
+    cells, types = [(0, 8, 0, 8), (8, 16, 0, 8)], [1, 11]
+    if hanging:
+        cells += [(x, x + 4, y, y + 4) for x in (16, 20) for y in (0, 4)]
+        types += [10] * 4
+    else:
+        cells.append((16, 24, 0, 8))
+        types.append(10)
+    rest = len(cells) - 2
+    beds = [0., .1] + [0.] * rest
+    depths = [1.0001, .9] + [1.] * rest if regime == 'near_balance' else [2., .05] + [0.] * rest
+    return setup(path, cells=cells, types=types, bed=beds, depth=depths,
+                 gate=dict(gates=[dict(name='A', inside_point=(12, 2), control_point=(4, 2))], opening_seconds=.25,
+                           trigger_level=.5, open_elevation=0., pond_land_type=10))
+
+
+@pytest.mark.parametrize('regime', ['near_balance', 'dry_wet'])
+def test_uniform_and_hanging_section_agree_on_width_and_cumulative_flow(tmp_path, regime):
+    """tests/test_gate_extended.py:132-193: one shared 8 m face, whole or
+    split; the first step's exchange follows the head jump over the centre
+    distance (8 m, or 6 m to the split cells' centres), the second step
+    continues from the half-open bed."""
+    observations = []
+    for hanging in (False, True):
+        path = tmp_path / ('hanging' if hanging else 'uniform')
+        dc, force, topo, *_ = paired_section(path, hanging=hanging, regime=regime)
+        r = run(dc, force, .125)
+        gate, pond = gate_of(r), pond_of(r)
+        assert_control_volume(pond, scale=100.)
+        assert_control_volume(gate['channel_budget'], scale=100.)
+        interface = (topo[:, 1] == 2) & (topo[:, 2] > 2)
+        assert np.count_nonzero(interface) == (2 if hanging else 1)
+        lengths = np.full(np.count_nonzero(interface), 4. if hanging else 8.)
+        width_flow = float(np.dot(r.state.q[interface], lengths))
+        first_net = gate['pond_net_m3']
+        pond_cells = topo[interface, 2]
+        left_eta = float(r.state.bed[2]) + float(r.state.depth[2])
+        right_eta = r.state.bed[pond_cells].astype(float) + r.state.depth[pond_cells].astype(float)
+        face_depth = np.maximum(left_eta, right_eta) - np.maximum(float(r.state.bed[2]),
+                                                                  r.state.bed[pond_cells].astype(float))
+        distance = 6. if hanging else 8.
+        expected_q = r.state.q[interface].astype(float) - 9.81 * face_depth * (right_eta - left_eta) / distance * .125
+        nxt = run(dc, force, .25, output=path / 'next', restart=path / 'out/output/state_final.fdb')
+        np.testing.assert_allclose(nxt.state.q[interface], expected_q, rtol=3e-5, atol=2e-8)
+        second = gate_of(nxt)['pond_net_m3'] - first_net
+        assert second == pytest.approx(float(np.dot(expected_q, lengths)) * .125, rel=3e-5, abs=2e-8)
+        assert nxt.state.bed[2] == 0.
+        observations.append(dict(width_flow=width_flow, pond_net=gate['pond_net_m3'],
+                                 river_net=gate['channel_budget']['river_net_m3'], pond_storage=pond['storage_m3'],
+                                 channel_storage=gate['channel_budget']['storage_m3'], distance=distance))
+    uniform, hanging = observations
+    if regime == 'dry_wet':
+        for o in observations:
+            expected = 9.81 * .05 * .15 / o['distance'] * .125 * 8.
+            assert o['width_flow'] == pytest.approx(expected, rel=2e-5)
+            assert o['pond_net'] == pytest.approx(expected * .125, rel=2e-5)
+            assert o['pond_storage'] == pytest.approx(o['pond_net'], abs=2e-5)
+        assert hanging['width_flow'] / uniform['width_flow'] == pytest.approx(4 / 3, rel=2e-5)
+        assert hanging['river_net'] == pytest.approx(uniform['river_net'], rel=2e-5)
+    else:
+        keys = ('width_flow', 'pond_net', 'river_net', 'pond_storage', 'channel_storage')
+        np.testing.assert_allclose([uniform[k] for k in keys], [hanging[k] for k in keys], rtol=2e-3, atol=2e-4)
+
+
+@pytest.mark.parametrize('opening_seconds', [1800., 3600.])
+def test_formal_30000s_command_and_f32_opening_age(tmp_path, opening_seconds):
+    """tests/test_gate_extended.py:227-274: the trigger check and the F32
+    opening age at clock words 30,000 s in, by setting the clock directly."""
+    from engine import OracleEngine
+    from nhflood.forcing import Forcing
+    from nhflood.gate import GateController, GateLayout
+    from nhflood.geometry import MeshGeometry
+    from nhflood.model import StepParams, build_step_arrays
+    from nhflood.preprocess import load_mesh, preprocess
+    from nhflood.clock import seconds_to_ticks, words
+    cells = [(4, 8, 0, 4), (0, 4, 0, 4), (8, 12, 0, 4)]  # gate, control (river), pond
+    dc, force, *_ = setup(tmp_path, cells=cells, types=[11, 1, 10], bed=[8, 0, 0], depth=[0, 0, 0],
+                          gate=dict(trigger_level=1., opening_seconds=opening_seconds, open_elevation=0.,
+                                    gates=[dict(name='A', inside_point=(6., 2.), control_point=(2., 2.))]))
+    preprocess(dc, force)
+    mesh, flags = load_mesh(dc)
+    geometry = MeshGeometry.from_mesh(mesh)
+    forcing = Forcing.load(dc, force, geometry)
+    arrays = build_step_arrays(mesh, flags, geometry, forcing, dc.land_parameters, dc.sita)
+    layout = GateLayout.load(force.gate, geometry.bounds, mesh.land_type, mesh.topology, forcing.boundaries,
+                             arrays.bed)
+    assert layout.cell_gate.tolist() == [-1, 0, -1, -1] and layout.controls.tolist() == [2]
+    controller = GateController.build(force.gate, layout, arrays.bed, mesh.land_type, mesh.topology, 0.)
+    arrays.gate = controller.tables
+    eng = OracleEngine(arrays, StepParams(min_h=1e-5))
+    eng.initialize()
+    eng.set('bed', np.array([0, 8, 0, 0], np.float32))
+    fractional_age = np.float32(1.234567)
+    fractional_bed = np.float32(8. - 8. * np.float32(fractional_age / np.float32(opening_seconds)))
+    for seconds, expected in ((29999., None), (30000., 8.), (30001.234567, fractional_bed),
+                              (30000. + opening_seconds / 4, 6.), (30000. + opening_seconds / 2, 4.),
+                              (30000. + opening_seconds, 0.)):
+        if seconds == 30000.:
+            eng.set('depth', np.array([0, 0, 2, 0], np.float32))
+        eng.set_clock(words(seconds_to_ticks(seconds)))
+        eng.set_active(1)
+        eng.gate_check()
+        state = eng.gate_state()
+        assert state['commanded'][0] == int(expected is not None)
+        if expected is not None:
+            assert eng.get('bed')[1] == pytest.approx(expected, abs=2e-6)
+    controller.state = eng.gate_state()
+    controller.initialize_inventory(eng.get('depth'), np.array([0., 16., 16., 16.]))
+    report = controller.report(eng.get('depth'), np.array([0., 16., 16., 16.]), 30000. + opening_seconds)['gates'][0]
+    assert report['command_seconds'] == 30000.
+    assert report['scheduled_fully_open_seconds'] == 30000. + opening_seconds
+    assert report['fully_open_seconds'] == 30000. + opening_seconds
+    assert report['first_fully_open_sample_seconds'] == 30000. + opening_seconds
+    assert report['command_clock_ticks'] == words(seconds_to_ticks(30000.)).tolist()
+    eng.close()
