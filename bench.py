@@ -60,6 +60,8 @@ def algorithmic_bytes(w):
         b += 28
     if getattr(w.mesh, 'level', None) is not None:
         b += 12.0 * (w.mesh.s_num - 1) / w.cells + 20
+    if getattr(w, 'gate', None) is not None and w.gate.enabled:
+        b += 8  # the gate controller's per-cell gate index and pond flag
     return b
 
 
@@ -92,6 +94,8 @@ def make_workload(name):
         return workloads.dambreak(n=int(name.split('_')[1]))
     if name == 'multires_quadtree':
         return workloads.multires_quadtree()
+    if name.startswith('gated_polder_'):
+        return workloads.gated_polder(n=int(name.split('_')[2]))
     raise SystemExit(f'unknown workload {name}')
 
 
@@ -424,6 +428,9 @@ def main():
     launches = 0
     tiled = eng.path.startswith('tiled')
     pre = (1 if run.arrays.hang_cells else 0) + (0 if w.sita == 1.0 else 1)
+    gate = run.arrays.gate
+    # gate controller: bed motion at start and end, exchange volumes (multi-pass only)
+    pre += 0 if gate is None else 2 + (1 if len(gate.flux_sides) else 0)
     per_step_kernels = (1 if tiled else 6) + pre
     per_batch_kernels = 4 if tiled else 1  # begin (+ rain-time copy, state copy-back, velocity)
     recorded = 0

@@ -42,6 +42,8 @@ class PlainRun:
                 targets[b.cells] = np.maximum(b.series.at(0.) - bed[b.cells].astype(float), 0.)
         eng.apply_initial_levels(targets)
         eng.set_active(1)
+        if self.arrays.gate is not None:
+            eng.gate_check()  # check_gates before the first CFL (solver_compact.py:885-888)
         eng.compute_cfl()
         eng.initial_diagnostics()
         eng.reset_extrema()
@@ -115,6 +117,8 @@ class PlainRun:
         is recomputed from the adopted state (as the step itself computes it)."""
         for name in STATE_F32 + STATE_U32:
             self.engine.set(name, other.engine.get(name))
+        if self.arrays.gate is not None:
+            self.engine.set_gate_state(other.engine.gate_state())
         self.engine.set_clock(other.engine.get_clock())
         self.clock.now_ticks = other.clock.now_ticks
         self.elapsed, self.steps = other.elapsed, other.steps

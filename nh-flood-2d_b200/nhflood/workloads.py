@@ -54,6 +54,7 @@ class Workload:
     initial_depth: np.ndarray | None = None
     rain_raster: Raster | None = None
     meta: dict = field(default_factory=dict)
+    gate: object = None  # input.GateConfig: a gate controller block, or None
 
     @property
     def sbf(self):
@@ -85,8 +86,17 @@ class Workload:
                           zeros.copy(), depth.copy(), words, words.copy(), zeros.copy(), 0, 0, False, meta)
 
     def step_arrays(self):
+        """Step inputs; with an enabled gate block, the controller tables too
+        (the layout resolved from the mesh bed, control from t = 0)."""
         from .model import build_step_arrays
-        return build_step_arrays(self.mesh, self.sbf, self.geometry, self.forcing, self.land_parameters, self.sita)
+        arrays = build_step_arrays(self.mesh, self.sbf, self.geometry, self.forcing, self.land_parameters, self.sita)
+        if self.gate is not None and self.gate.enabled:
+            from .gate import GateController, GateLayout
+            layout = GateLayout.load(self.gate, self.geometry.bounds, self.mesh.land_type, self.mesh.topology,
+                                     self.forcing.boundaries, arrays.bed)
+            arrays.gate = GateController.build(self.gate, layout, arrays.bed, self.mesh.land_type,
+                                               self.mesh.topology, 0.).tables
+        return arrays
 
     def write_inputs(self, path) -> tuple[Path, Path]:
         """Write NE/NS text, forcing files and domain/force JSON; returns the JSON paths."""
@@ -287,6 +297,66 @@ def dambreak(n: int = 4096, dx: float = 1.0, seed: int = 3, duration: int = 1800
     land_parameters = {1: LandParameters(manning_n=0.03, infiltration='none')}
     return Workload(f'dambreak_{n}', mesh, geometry, forcing, land_parameters, duration=duration, yield_step=300,
                     initial_depth=depth, rain_raster=raster, meta={'lines': {'perimeter': lines}, 'seed': seed})
+
+
+def gated_polder(n: int = 1024, dx: float = 5.0, gates: int = 4, seed: int = 6, duration: int = 3600) -> Workload:
+    """River land draining south against a dike into a polder pond through
+    gates. n x n cells of dx metres: the pond (class 10, bed -2 m) fills the
+    southern eighth, a 4-row dike (class 3, 3 m above the land) closes it,
+    and `gates` openings of 4 x 16 cells (class 11, closed at the dike top,
+    open at -1 m) cut through it, each controlled by the land cell just
+    north of its middle. The land (class 1, 1 m fractal relief on a 0.001
+    slope towards the dike) starts with 1 m of water in the 40 rows above the
+    dike and takes 50 mm/h of rain for the first hour; the pond drains over
+    a free-outflow level boundary on the south edge. The trigger (level
+    above the highest control bed + 0.5 m) commands every gate at t = 0 and
+    they open over 600 s."""
+    from .input import GateConfig
+    rng = np.random.default_rng(seed)
+    width = n * dx
+    yc = (np.arange(n) + 0.5) * dx
+    noise = fractal_noise((n, n), 5, rng)
+    pond_rows, dike_rows = n // 8, 4
+    dike0 = pond_rows
+    land_bed = 1.0 * noise + 0.001 * (yc[:, None] - dike0 * dx)
+    bed = land_bed.copy()
+    land = np.ones((n, n), np.uint8)
+    bed[:pond_rows] = -2.0
+    land[:pond_rows] = 10
+    dike_top = float(land_bed[dike0 + dike_rows:dike0 + dike_rows + 8].max()) + 3.0
+    bed[dike0:dike0 + dike_rows] = dike_top
+    land[dike0:dike0 + dike_rows] = 3
+    centres = [int((k + 0.5) * n / gates) for k in range(gates)]
+    for c in centres:
+        land[dike0:dike0 + dike_rows, c - 8:c + 8] = 11
+    mesh = uniform_grid(n, n, dx, bed.astype(np.float32), land)
+    geometry = MeshGeometry.from_mesh(mesh)
+    rain, raster = _uniform_rain(geometry, width, width, np.array([0., 3600.]), np.array([3600., float(duration) + 3600.]),
+                                 [50.0, 0.0])
+    outflow = -102.0
+    south = [np.array([[0.0, 0.0], [width, 0.0]])]
+    claimed = np.zeros(mesh.e_num, bool)
+    boundary = select_boundary('south', 'level', south,
+                               TimeSeries(np.array([0., float(duration)]), np.array([outflow, outflow])),
+                               geometry, claimed)
+    forcing = Forcing.assemble([boundary], rain, duration)
+    depth = np.zeros(mesh.e_num, np.float32)
+    row = np.floor(mesh.y[1:] / dx).astype(np.int64)
+    depth[1:] = np.where((row >= dike0 + dike_rows) & (row < dike0 + dike_rows + 40), 1.0, 0.0)
+    control_row = dike0 + dike_rows
+    controls = [((c + 0.5) * dx, (control_row + 0.5) * dx) for c in centres]
+    trigger = float(max(bed[control_row, c] for c in centres)) + 0.5
+    gate = GateConfig(land_type=11, pond_land_type=10, enabled=True, trigger_level=trigger, opening_seconds=600.,
+                      open_elevation=-1.0,
+                      gates=[dict(name=f'G{k}', inside_point=((c + 0.5) * dx, (dike0 + 1.5) * dx),
+                                  control_point=controls[k]) for k, c in enumerate(centres)])
+    land_parameters = {1: LandParameters(manning_n=0.035, infiltration='none'),
+                       3: LandParameters(manning_n=0.05, infiltration='none'),
+                       10: LandParameters(manning_n=0.03, infiltration='none'),
+                       11: LandParameters(manning_n=0.02, infiltration='none')}
+    return Workload(f'gated_polder_{n}', mesh, geometry, forcing, land_parameters, duration=duration, yield_step=300,
+                    initial_depth=depth, rain_raster=raster, meta={'lines': {'south': south}, 'seed': seed},
+                    gate=gate)
 
 
 def simulate(workload: Workload, domain_dir, *, engine_factory=None, end_time=None, batch_size: int = 32):

@@ -93,3 +93,30 @@ def test_served_request_stream_has_the_configured_distribution():
     assert abs(w.forcing.rain.millimetres[0, 0] - reqs[0]['params']['uniform_rain'] * w.duration / 3600) < 1e-3
     a = w.step_arrays()
     assert device_bytes_estimate(a) > a.nbytes() + 40 * a.e_num
+
+
+def test_gated_polder_resolves_its_gates_and_opens_them_on_the_oracle():
+    """The gate benchmark workload: four gates of 4 x 16 cells through the
+    dike, every one commanded at t = 0 (control cells start 1 m deep, the
+    trigger is 0.5 m above the highest control bed) and fully open after
+    600 s; water reaches the pond through every gate."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / 'oracle'))
+    from engine import OracleEngine
+    from nhflood import workloads
+    from nhflood.plain import PlainRun
+    w = workloads.gated_polder(n=128, dx=40.0)
+    run = PlainRun(w, lambda a, p: OracleEngine(a, p))
+    gate = run.arrays.gate
+    assert gate.count == 4 and len(gate.targets) == 4 * 4 * 16
+    assert run.engine.gate_state()['commanded'].tolist() == [1, 1, 1, 1]
+    while run.elapsed < 700:
+        run.advance()
+    state = run.engine.gate_state()
+    assert state['opened'].tolist() == [1, 1, 1, 1] and state['flow_seen'].tolist() == [1, 1, 1, 1]
+    totals = run.engine.gate_flush()
+    assert all(totals[4 * g] > 0 for g in range(4))  # pond inflow through every gate
+    bed = run.engine.get('bed')
+    assert np.all(bed[gate.targets] == np.float32(-1.0))
+    run.close()
