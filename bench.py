@@ -204,7 +204,8 @@ def bench_batched(args, rank, world, local):
     cell_updates = 0
     recorded = 0
     hang = sum(1 for r in ens.runs if r.arrays.hang_cells)
-    per_batch_kernels = 5 + ens.runs[0].params.batch_size * (1 + (1 if hang else 0))
+    # per step: the ensemble step, its CFL pass, the hanging pre-pass if any member has hanging edges
+    per_batch_kernels = 5 + ens.runs[0].params.batch_size * (2 + (1 if hang else 0))
     with ClockSampler(local) as clocks:
         for k in range(args.steps):
             if ens.done:
@@ -217,9 +218,14 @@ def bench_batched(args, rank, world, local):
             recorded += 1
         torch.cuda.synchronize(device)
     device_s = sum(starts[i].elapsed_time(ends[i]) for i in range(recorded)) / 1e3
-    # the same scenarios, one after another, each with its own plain batch graph
+    # the same scenarios, one after another, each on a plain engine of its own
+    # (the plain form's own CFL choice) continuing from the member's state
+    from nhflood.ensemble import tiled_factory
+    from nhflood.plain import PlainRun
     plain_cells, plain_s = 0, 0.0
-    for r in ens.runs:
+    for member in ens.runs:
+        r = PlainRun(member.w, tiled_factory(ens.tile, str(device), cfl='auto'), batch_size=member.params.batch_size)
+        r.adopt(member)
         st = r.engine.stream()
         for _ in range(args.plain_batches):
             if r.done:
@@ -232,6 +238,7 @@ def bench_batched(args, rank, world, local):
             plain_cells += r.finish(r.engine.read_trace()) * r.w.cells
             b.synchronize()
             plain_s += a.elapsed_time(b) / 1e3
+        r.close()
     # end to end through the public call (host words in, host traces out)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
@@ -431,7 +438,8 @@ def main():
     gate = run.arrays.gate
     # gate controller: bed motion at start and end, exchange volumes (multi-pass only)
     pre += 0 if gate is None else 2 + (1 if len(gate.flux_sides) else 0)
-    per_step_kernels = (1 if tiled else 6) + pre
+    # fused step (+ its CFL pass on split plans) or the six multi-pass kernels
+    per_step_kernels = ((2 if 'cfl=pass' in eng.path else 1) if tiled else 6) + pre
     per_batch_kernels = 4 if tiled else 1  # begin (+ rain-time copy, state copy-back, velocity)
     recorded = 0
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=device)

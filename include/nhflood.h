@@ -99,6 +99,12 @@ typedef struct nhf_params {
                            multi-pass; 1: always the multi-pass step;
                            256, 512 or 1024: fused tiled step with that tile
                            size when the mesh allows it, else multi-pass */
+    int32_t cfl_mode;   /* fused step only. 0: the next step's CFL candidate
+                           in the step itself on meshes of less than two
+                           waves of tiles, else a separate pass after it;
+                           1: always in the step; 2: always a separate pass
+                           (ensemble members, whose launches span all
+                           members) */
 } nhf_params;
 
 typedef struct nhf_handle nhf_handle;

@@ -33,7 +33,8 @@ struct Ctl {
 // Tile plan of the fused step (built on the host by nhf_tiled.cu).
 struct TilePlan {
     int32_t n_tiles, tile, max_ext, max_sides, cells_per_thread;
-    // per tile: n_ext, n_r0, n_r01, n_r012, n_sides, n_owned, n_qf, r0_first_offset,
+    int32_t split;  // 1: two halo rings and a separate CFL pass; 0: three rings, CFL in the step
+    // per tile: n_ext, n_r0, n_r01, n_don, n_sides, n_owned, n_qf, r0_first_offset,
     // n_faces, cbase, sbase, then the pattern's ext, side, face_desc and face_idx offsets, 0
     const int4 *tile_head;     // [n_tiles][4]
     const int32_t *ext_rel;    // relative cell ids by local slot (slot 0 = exterior sentinel)
@@ -277,10 +278,12 @@ struct TiledBuild {
 // once). Returns 0 on success; a nonzero value with `why` set when the mesh
 // does not fit the tiled form (the caller then keeps the multi-pass form).
 // tile_request: 0 picks the tile size by mesh size; 256, 512 or 1024 asks
-// for that size only.
+// for that size only. cfl_mode: 0 separate CFL pass from two waves of tiles
+// on, 1 CFL always in the step, 2 always a separate pass.
 int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, size_t why_len,
-                int tile_request = 0);
-// Enqueue one fused step (plus the hanging/theta pre-passes when needed).
+                int tile_request = 0, int cfl_mode = 0);
+// Enqueue one fused step (plus the hanging/theta pre-passes and, for split
+// plans, the CFL pass).
 void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s);
 // Enqueue the batch epilogue: bring the state back into the caller's
 // buffers and refresh u, v.

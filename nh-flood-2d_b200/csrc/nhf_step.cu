@@ -868,11 +868,16 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     // Fused tiled step when the mesh allows it (params->path 0, or a tile size).
     if (params->path == 0 || params->path == 256 || params->path == 512 || params->path == 1024) {
         char why[256] = {0};
-        if (tiled_build(*mesh, h->s, &h->tb, why, sizeof(why), params->path) == 0) {
+        if (params->cfl_mode < 0 || params->cfl_mode > 2) {
+            rc = fail(nullptr, NHF_EINVAL, "cfl_mode must be 0, 1 or 2");
+            nhf_destroy(h);
+            return rc;
+        }
+        if (tiled_build(*mesh, h->s, &h->tb, why, sizeof(why), params->path, params->cfl_mode) == 0) {
             h->tiled = true;
-            char buf[128];
-            snprintf(buf, sizeof(buf), "tiled(tile=%d,patterns=%d,smem=%zu)", h->tb.plan.tile, h->tb.patterns,
-                     h->tb.shared_bytes);
+            char buf[160];
+            snprintf(buf, sizeof(buf), "tiled(tile=%d,patterns=%d,smem=%zu,cfl=%s)", h->tb.plan.tile,
+                     h->tb.patterns, h->tb.shared_bytes, h->tb.plan.split ? "pass" : "fused");
             h->path = buf;
         } else {
             h->path = std::string("multipass (") + why + ")";

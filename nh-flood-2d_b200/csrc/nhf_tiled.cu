@@ -1,20 +1,26 @@
-// Fused local-inertial step: one kernel launch per time step.
+// Fused local-inertial step: one kernel launch per time step (plus, on large
+// meshes, a separate CFL pass).
 //
 // Cells are split into tiles of T consecutive reference indices (T = 1024,
-// 512 or 256; a tile covers T/256 whole budget blocks). A 256-thread block
-// owns one tile and stages in shared memory the tile (ring 0) and three rings
-// of neighbours (graph distance 1..3), because one step of the reference's
-// passes (solver_compact.py:439-613) and its CFL (617-641) reach that far:
+// 512 or 256; a tile covers T/256 whole budget blocks). A block owns one
+// tile and stages in shared memory the tile (ring 0) and the rings of
+// neighbours (graph distance 1..3) that one step of the reference's passes
+// (solver_compact.py:439-613) and its CFL (617-641) reach:
 //   ring <= 3  water level and bed           -> momentum q* of faces(ring <= 2)
 //   ring <= 2  donor factor from those q*    -> final q of faces(ring <= 1)
 //   ring <= 1  depth update from final q     -> CFL of the sides the tile owns
+// That is the fused-CFL form. On meshes of several waves of tiles the plan
+// drops ring 3 and the ring-1 depth recompute, and the CFL candidate of the
+// next step is a separate grid-wide pass on the new state (k_cfl_tiled): the
+// halo work saved outweighs one more launch per step (TilePlan::split).
 // Every quantity is computed with the reference's operation order, so a cell
 // that several tiles recompute gets the same bits everywhere; each output
 // (depth, side q, extrema, budget block) has exactly one writer, its owner
 // tile. depth, q and rain_time are double-buffered so that halo reads never
 // see a neighbour's update of the same step. The last block to finish commits
-// the clock, writes the trace row and prepares the next step, so a batch is
-// one launch per step in a CUDA graph.
+// the clock and writes the trace row and (fused-CFL form) prepares the next
+// step; in the split form the CFL pass's last block prepares it. A batch is
+// one or two launches per step in one CUDA graph.
 //
 // The host planner below builds, per tile, the ring lists, the local side
 // list and a local face CSR, all relative to the tile's first cell and side.
@@ -68,7 +74,7 @@ struct CellTerms {
 };
 
 struct Tile {
-    int n_ext, n_r0, n_r01, n_r012, n_sides, n_owned, n_qf, r0off, n_faces;
+    int n_ext, n_r0, n_r01, n_don, n_sides, n_owned, n_qf, r0off, n_faces;
     int cbase, sbase;
     const int32_t *ext;
     const int32_t *srel;
@@ -161,7 +167,8 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
             if (ticket == n_tiles - 1) {
                 c->done_blocks = 0;
                 finish_step(c);
-                if (c->slot < d.batch_size) prepare_step(d, c, cur_depth(d, c->parity), cur_q(d, c->parity));
+                if (!d.plan.split && c->slot < d.batch_size)
+                    prepare_step(d, c, cur_depth(d, c->parity), cur_q(d, c->parity));
             }
         }
         return;
@@ -182,7 +189,7 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
     {
         const int4 *head = P.tile_head + 4 * t_index;
         const int4 h0 = head[0], h1 = head[1], h2 = head[2], h3 = head[3];
-        tl.n_ext = h0.x; tl.n_r0 = h0.y; tl.n_r01 = h0.z; tl.n_r012 = h0.w;
+        tl.n_ext = h0.x; tl.n_r0 = h0.y; tl.n_r01 = h0.z; tl.n_don = h0.w;
         tl.n_sides = h1.x; tl.n_owned = h1.y; tl.n_qf = h1.z; tl.r0off = h1.w;
         tl.n_faces = h2.x;
         tl.cbase = h2.y;
@@ -217,13 +224,13 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
         cp_async4(sh_srel + i, tl.srel + i);
         cp_async4(sh_lohi + i, tl.lohi + i);
     }
-    for (int i = tid; i <= tl.n_r012; i += NT) cp_async4(sh_fdesc + i, tl.fdesc + i);
+    for (int i = tid; i <= tl.n_don; i += NT) cp_async4(sh_fdesc + i, tl.fdesc + i);
     for (int i = tid; i < (tl.n_faces + 1) >> 1; i += NT)  // patterns keep an even length
         cp_async4(reinterpret_cast<uint32_t *>(sh_fidx) + i, reinterpret_cast<const uint32_t *>(tl.fidx) + i);
     cp_async_wait_all();
     __syncthreads();
     // (b) Gathers: depth and bed of the tile and its rings, the per-cell
-    // inputs of rings 0..2 (the rain pixel index parks in sh_rq), and q and
+    // inputs of the donor rings (the rain pixel index parks in sh_rq), and q and
     // length of every local side.
     for (int i = tid; i < tl.n_ext; i += NT) {
         const int g = i ? tl.cbase + sh_g[i] : 0;
@@ -231,7 +238,7 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
         if (i) cp_async4(sh_h + i, depth_in + g);
         else sh_h[0] = m.depth[0];
         cp_async4(sh_z + i, m.bed + g);
-        if (i >= 1 && i <= tl.n_r012) {
+        if (i >= 1 && i <= tl.n_don) {
             cp_async4(sh_area + i, m.area + g);
             cp_async4(sh_bi + i, m.boundary_id + g);
             cp_async4(sh_rq + i, m.rain_index + g);
@@ -300,11 +307,11 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
     }
     __syncthreads();
 
-    // P2: donor factor (solver_compact.py:491-514) for rings 0..2.
+    // P2: donor factor (solver_compact.py:491-514) for the donor rings.
     {
         uint32_t my_limited = 0;
         uint32_t my_min = __float_as_uint(1.0f);
-        for (int i = 1 + tid; i <= tl.n_r012; i += NT) {
+        for (int i = 1 + tid; i <= tl.n_don; i += NT) {
             const int bi = sh_bi[i];
             int kind = -1;
             float discharge = 0.0f;
@@ -489,7 +496,7 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
             if (mask) atomicOr(&sh_mask[kk][tid >> 8], mask);
         }
     }
-    // ring 1: the new depth only (for the CFL of owned sides)
+    // ring 1 (fused-CFL form): the new depth only, for the CFL of owned sides
     for (int i = tl.n_r0 + 1 + tid; i <= tl.n_r01; i += NT) {
         const int g = sh_g[i];
         const int bi = sh_bi[i];
@@ -597,17 +604,20 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
         }
     }
 
-    // P5: owned sides: final q out, CFL with the new depths.
+    // P5: owned sides: final q out; in the fused-CFL form also the CFL of the
+    // owned sides with the new depths (the split form's CFL pass follows).
+    const bool split = P.split != 0;
     unsigned long long best = kCflEmpty;
     // A side at the 0.01 m face-depth floor with q = 0 has the CFL value
     // afa * L / sqrt(g * 0.01); it is reused while L repeats.
     float dry_len = -1.0f, dry_cfl = 0.0f;
     for (int j = tid; j < tl.n_owned; j += NT) {
         const int gid = tl.sbase + tl.srel[j];
-        const uint32_t lh = tl.lohi[j];
-        const int a = (int)(lh & 0xffffu), b = (int)(lh >> 16);
         float qv = sh_q[j];
         q_out[gid] = qv;
+        if (split) continue;
+        const uint32_t lh = tl.lohi[j];
+        const int a = (int)(lh & 0xffffu), b = (int)(lh >> 16);
         if (a != 0 && b != 0) {
             float zl = sh_z[a], zh = sh_z[b];
             float head = maxf(zl + sh_s[a], zh + sh_s[b]);
@@ -626,15 +636,18 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
             best = key < best ? key : best;
         }
     }
-    best = warp_min_u64(best);
-    const int lane = tid & 31, warp = tid >> 5;
-    if (lane == 0) sh_min[warp] = best;
+    if (!split) {
+        best = warp_min_u64(best);
+        if ((tid & 31) == 0) sh_min[tid >> 5] = best;
+    }
     if (my_wet) atomicAdd(&sh_cnt[2], my_wet);
     __syncthreads();
     if (tid == 0) {
-        unsigned long long bmin = kCflEmpty;
-        for (int w = 0; w < NT / 32; ++w) bmin = sh_min[w] < bmin ? sh_min[w] : bmin;
-        if (bmin != kCflEmpty) atomicMin(&c->cfl_packed, bmin);
+        if (!split) {
+            unsigned long long bmin = kCflEmpty;
+            for (int w = 0; w < NT / 32; ++w) bmin = sh_min[w] < bmin ? sh_min[w] : bmin;
+            if (bmin != kCflEmpty) atomicMin(&c->cfl_packed, bmin);
+        }
         if (sh_cnt[0]) {
             atomicAdd(&c->limited_cells, sh_cnt[0]);
             atomicMin(&c->min_scale_bits, sh_minbits);
@@ -647,26 +660,96 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
     }
     __syncthreads();
     if (!sh_last || tid != 0) return;
-    // Last block: CFL result, trace row, clock commit, next step's preparation.
+    // Last block: (fused-CFL form: the CFL result,) trace row, clock commit,
+    // the new state becomes current (and the next step is prepared).
     __threadfence();
-    unsigned long long packed = atomicExch(&c->cfl_packed, kCflEmpty);
     c->done_blocks = 0;
-    if (packed == kCflEmpty) {
-        c->ndt = __uint_as_float(0x7f800000u);
-        c->cfl_arg = 0;
-    } else {
-        c->ndt = __uint_as_float((uint32_t)(packed >> 32));
-        c->cfl_arg = (int32_t)(packed & 0xffffffffu);
+    if (!split) {
+        unsigned long long packed = atomicExch(&c->cfl_packed, kCflEmpty);
+        if (packed == kCflEmpty) {
+            c->ndt = __uint_as_float(0x7f800000u);
+            c->cfl_arg = 0;
+        } else {
+            c->ndt = __uint_as_float((uint32_t)(packed >> 32));
+            c->cfl_arg = (int32_t)(packed & 0xffffffffu);
+        }
     }
     finish_step(c);
     c->parity = parity ^ 1;
-    if (c->slot < d.batch_size) prepare_step(d, c, depth_out, q_out);
+    if (!split && c->slot < d.batch_size) prepare_step(d, c, depth_out, q_out);
+}
+
+// CFL pass (solver_compact.py:617-641) over sides [first, end) with stride,
+// on the current (just updated) state; each block adds its minimum packed
+// key (cfl bits, side id) and the last of `blocks` blocks sets ndt /
+// cfl_arg (the lowest side id attains the minimum) and prepares the next
+// step (solver_compact.py:364-382).
+__device__ __forceinline__ void cfl_pass(const Dev &d, int first, int end, int stride, unsigned blocks)
+{
+    __shared__ unsigned long long sh[32];
+    __shared__ bool last;
+    const nhf_mesh &m = d.m;
+    Ctl *c = d.ctl;
+    const int active = c->active;
+    const float *depth = cur_depth(d, c->parity);
+    const float *q = cur_q(d, c->parity);
+    unsigned long long best = kCflEmpty;
+    if (active) {
+        for (int si = first + (int)threadIdx.x; si < end; si += stride) {
+            const int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
+            if (el != 0 && eh != 0) {
+                const float zl = m.bed[el], zh = m.bed[eh];
+                const float head = maxf(zl + depth[el], zh + depth[eh]);
+                const float h = maxf(head - maxf(maxf(zl, zh), kDh), 0.01f);
+                const float cfl = d.afa * m.length[si] / (sqrtf(d.g * h) + fabsf(q[si]) / h);
+                const unsigned long long key = ((unsigned long long)__float_as_uint(cfl) << 32) | (unsigned)si;
+                best = key < best ? key : best;
+            }
+        }
+    }
+    best = warp_min_u64(best);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sh[warp] = best;
+    __syncthreads();
+    if (warp == 0) {
+        best = lane < (int)(blockDim.x >> 5) ? sh[lane] : kCflEmpty;
+        best = warp_min_u64(best);
+        if (lane == 0) {
+            if (best != kCflEmpty) atomicMin(&c->cfl_packed, best);
+            __threadfence();
+            const unsigned ticket = atomicAdd(&c->done_blocks, 1u);
+            last = ticket == blocks - 1;
+        }
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    const unsigned long long packed = atomicExch(&c->cfl_packed, kCflEmpty);
+    c->done_blocks = 0;
+    if (active) {
+        if (packed == kCflEmpty) {
+            c->ndt = __uint_as_float(0x7f800000u);
+            c->cfl_arg = 0;
+        } else {
+            c->ndt = __uint_as_float((uint32_t)(packed >> 32));
+            c->cfl_arg = (int32_t)(packed & 0xffffffffu);
+        }
+    }
+    if (c->slot < d.batch_size) prepare_step(d, c, depth, q);
 }
 
 template <bool kThetaOne, bool kHanging, int NT, int CPT>
 __global__ void __launch_bounds__(NT, kMinBlocks<NT>) k_step_tiled(const __grid_constant__ Dev d)
 {
     step_tile<kThetaOne, kHanging ? 1 : 0, NT, CPT>(d, blockIdx.x, gridDim.x);
+}
+
+// CFL pass of one mesh after its fused step (grid-stride over the sides);
+// split plans only.
+__global__ void __launch_bounds__(256) k_cfl_tiled(const __grid_constant__ Dev d)
+{
+    if (!d.plan.split) return;
+    cfl_pass(d, 1 + (int)(blockIdx.x * blockDim.x), d.m.s_num, (int)(gridDim.x * blockDim.x), gridDim.x);
 }
 
 // Ensemble step: one launch advances every member mesh by one of its own
@@ -850,7 +933,7 @@ bool consistent(const HostMesh &hm, std::string &why)
 
 int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::vector<int32_t> &tile_pattern,
                std::vector<int32_t> &tile_cbase, std::vector<int32_t> &tile_sbase, int &max_ext, int &max_sides,
-               int &max_faces, std::string &why)
+               int &max_faces, int rings, std::string &why)
 {
     const int e = hm.e, s = hm.s;
     // cell adjacency through interior sides
@@ -887,7 +970,7 @@ int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::v
         for (int g = r0_first; g < r0_end; ++g) { stamp[g] = t; ring[g] = 0; slot[g] = (int)ext.size(); ext.push_back(g); }
         int ring_begin[5];
         ring_begin[0] = 1;
-        for (int r = 1; r <= 3; ++r) {
+        for (int r = 1; r <= rings; ++r) {
             ring_begin[r] = (int)ext.size();
             for (int i = ring_begin[r - 1]; i < ring_begin[r]; ++i) {
                 int cc = ext[i];
@@ -899,18 +982,23 @@ int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::v
             std::sort(ext.begin() + ring_begin[r], ext.end());
             for (int i = ring_begin[r]; i < (int)ext.size(); ++i) slot[ext[i]] = i;
         }
-        ring_begin[4] = (int)ext.size();
-        const int n_r0 = ring_begin[1] - 1, n_r01 = ring_begin[2] - 1, n_r012 = ring_begin[3] - 1;
-        // local sides: faces of rings 0..2
+        ring_begin[rings + 1] = (int)ext.size();
+        // donor rings: 0..rings-1; the final q reaches faces of rings
+        // 0..rings-2 (ring 1 too in the fused-CFL form, for its new depth)
+        const int n_r0 = ring_begin[1] - 1, n_don = ring_begin[rings] - 1;
+        const int n_r01 = rings == 3 ? ring_begin[2] - 1 : n_r0;
+        const int final_ring = rings - 2;
+        // local sides: faces of the donor rings (their momentum feeds the
+        // donor factors)
         sides.clear();
-        for (int i = 1; i <= n_r012; ++i) {
+        for (int i = 1; i <= n_don; ++i) {
             int cc = ext[i];
             for (int dd = 0; dd < 4; ++dd) {
                 int p = hm.fptr[4 * cc + dd], n = hm.fcnt[4 * cc + dd];
                 for (int j = 0; j < n; ++j) {
                     int sid = hm.isl[p + j];
                     if (sstamp[sid] != t) { sstamp[sid] = t; sflag[sid] = 0; sides.push_back(sid); }
-                    if (ring[cc] <= 1) sflag[sid] |= kFinal;
+                    if (ring[cc] <= final_ring) sflag[sid] |= kFinal;
                 }
             }
         }
@@ -934,7 +1022,7 @@ int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::v
         if ((int)ext.size() > 65535 || (int)sides.size() > 65535) { why = "tile halo too large"; return 1; }
         int sbase = sides.empty() ? 0 : *std::min_element(sides.begin(), sides.end());
         Pattern p;
-        p.counts = {(int)ext.size(), n_r0, n_r01, n_r012, (int)sides.size(), n_owned, n_qf, r0_first - cbase,
+        p.counts = {(int)ext.size(), n_r0, n_r01, n_don, (int)sides.size(), n_owned, n_qf, r0_first - cbase,
                     0, 0, 0, 0};
         p.ext.resize(ext.size());
         p.ext[0] = 0;
@@ -947,8 +1035,8 @@ int plan_tiles(const HostMesh &hm, int T, std::vector<Pattern> &patterns, std::v
             int lo = hm.topo[3 * sid + 1], hi = hm.topo[3 * sid + 2];
             p.lohi[i] = (uint32_t)slot[lo] | ((uint32_t)slot[hi] << 16);
         }
-        p.fdesc.assign(n_r012 + 1, 0u);
-        for (int i = 1; i <= n_r012; ++i) {
+        p.fdesc.assign(n_don + 1, 0u);
+        for (int i = 1; i <= n_don; ++i) {
             int cc = ext[i];
             if (p.fidx.size() > 65535) { why = "tile face table too large"; return 1; }
             uint32_t counts = 0;
@@ -1147,6 +1235,20 @@ __global__ void k_ens_face_qn(const Dev *devs, const int2 *items)
     for (int i = w.y * kEnsChunk + threadIdx.x; i < end; i += blockDim.x) face_qn_cell(d, i);
 }
 
+// CFL pass of every member: items are (member, chunk of kEnsChunk sides);
+// a member's last chunk block prepares that member's next step. Members with
+// a fused-CFL plan did both in their step and are skipped.
+__global__ void __launch_bounds__(256) k_ens_cfl(const Dev *devs, const int2 *items)
+{
+    const int2 w = items[blockIdx.x];
+    const Dev &d = devs[w.x];
+    if (!d.plan.split) return;
+    const int n = d.m.e_num > d.m.s_num ? d.m.e_num : d.m.s_num;
+    const unsigned chunks = (unsigned)((n + kEnsChunk - 1) / kEnsChunk);
+    const int first = max(1, w.y * kEnsChunk), end = min(d.m.s_num, (w.y + 1) * kEnsChunk);
+    cfl_pass(d, first, end, (int)blockDim.x, chunks);
+}
+
 // Batch end, part 1: the current state back into the caller's buffers.
 __global__ void k_ens_copy_back(const Dev *devs, const int2 *items)
 {
@@ -1183,7 +1285,8 @@ __global__ void k_ens_finish(const Dev *devs, uint32_t *trace, int batch)
 }
 }  // namespace
 
-int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, size_t why_len, int tile_request)
+int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, size_t why_len, int tile_request,
+                int cfl_mode)
 {
     std::string reason;
     auto bad = [&](const std::string &r) {
@@ -1210,8 +1313,16 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
             return bad("tile size must be 256, 512 or 1024");
         sizes = {tile_request};
     }
+    bool split = false;
     for (int T : sizes) {
-        if (plan_tiles(hm, T, patterns, tp, tc, ts, max_ext, max_sides, max_faces, reason)) return bad(reason);
+        // The separate CFL pass pays one launch per step for less halo work
+        // (no ring 3, no ring-1 depth recompute): worth it from two waves of
+        // resident blocks on.
+        const int resident = 148 * (T == 256 ? kMinBlocks<256> : kMinBlocks<512>);
+        const int n_tiles = (m.e_num + T - 1) / T;
+        split = cfl_mode == 2 || (cfl_mode == 0 && n_tiles >= 2 * resident);
+        if (plan_tiles(hm, T, patterns, tp, tc, ts, max_ext, max_sides, max_faces, split ? 2 : 3, reason))
+            return bad(reason);
         // The budget reduction stages one term of every thread (NT doubles)
         // in the 24 * max_ext bytes of shared arrays that are dead after the
         // depth update; meshes smaller than a tile need the padding.
@@ -1274,6 +1385,7 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     P.max_ext = max_ext;
     P.max_sides = max_sides;
     P.cells_per_thread = tile == 1024 ? 2 : 1;
+    P.split = split ? 1 : 0;
     P.tile_head = (const int4 *)(b + o_hd);
     P.ext_rel = (const int32_t *)(b + o_ext);
     P.side_rel = (const int32_t *)(b + o_srel);
@@ -1298,6 +1410,11 @@ void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s)
     case 1024: launch_step<512, 2>(d, b.shared_bytes, s); break;
     case 512: launch_step<512, 1>(d, b.shared_bytes, s); break;
     default: launch_step<256, 1>(d, b.shared_bytes, s); break;
+    }
+    if (b.plan.split) {
+        int gc = (m.s_num + 255) / 256;
+        if (gc > 148 * 8) gc = 148 * 8;
+        k_cfl_tiled<<<gc, 256, 0, s>>>(d);
     }
 }
 
@@ -1352,6 +1469,7 @@ void ensemble_enqueue_step(const EnsembleLaunch &e, cudaStream_t s)
     case 512: ensemble_launch<512, 1>(e, s); break;
     default: ensemble_launch<256, 1>(e, s); break;
     }
+    k_ens_cfl<<<e.n_cell, 256, 0, s>>>(e.devs, e.cell_items);
 }
 
 void ensemble_enqueue_batch_end(const EnsembleLaunch &e, cudaStream_t s)

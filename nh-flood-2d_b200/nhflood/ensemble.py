@@ -19,9 +19,13 @@ from .native import CudaEngine, CudaEnsemble
 from .plain import PlainRun
 
 
-def tiled_factory(tile: int, device: str = 'cuda:0'):
+def tiled_factory(tile: int, device: str = 'cuda:0', cfl: str = 'pass'):
+    """Engines on the fused step with this tile size. Ensemble members take
+    the separate CFL pass (one launch for all members per step); a plain run
+    may pass cfl='auto'."""
     def factory(arrays, params):
         params.path = f'tile{tile}'
+        params.cfl = cfl
         engine = CudaEngine(arrays, params, device=device)
         if not engine.path.startswith('tiled'):
             engine.close()

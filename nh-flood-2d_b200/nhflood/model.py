@@ -29,6 +29,10 @@ class StepParams:
     g: float = float(G)
     min_dt: float = float(np.float32(MIN_DT))
     path: str = 'auto'  # 'auto': fused tiled step when the mesh allows it; 'multipass'
+    # fused step: where the next step's CFL candidate is computed. 'auto': in
+    # the step on meshes of less than two waves of tiles, else in a separate
+    # pass; 'fused': always in the step; 'pass': always a separate pass
+    cfl: str = 'auto'
 
 
 @dataclass

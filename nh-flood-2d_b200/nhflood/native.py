@@ -30,7 +30,7 @@ class NhfMesh(ctypes.Structure):
 
 class NhfParams(ctypes.Structure):
     _fields_ = [('g', c_float), ('afa', c_float), ('sita', c_float), ('min_h', c_float),
-                ('min_dt', c_float), ('batch_size', c_int32), ('path', c_int32)]
+                ('min_dt', c_float), ('batch_size', c_int32), ('path', c_int32), ('cfl_mode', c_int32)]
 
 
 _GATE_TABLES = ('cell_gate', 'pond', 'closed', 'targets', 'controls', 'flux_sides')
@@ -199,7 +199,9 @@ class CudaEngine(Engine):
             if path not in (0, 1):
                 raise ValueError('gate control runs on the multi-pass step; use path "auto" or "multipass"')
             path = 1
-        p = NhfParams(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size, path)
+        cfl_mode = {'auto': 0, 'fused': 1, 'pass': 2}[params.cfl]
+        p = NhfParams(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size, path,
+                      cfl_mode)
         handle = c_void_p()
         with torch.cuda.device(dev):
             stream = torch.cuda.current_stream(dev).cuda_stream

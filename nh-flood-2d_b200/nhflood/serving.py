@@ -258,7 +258,7 @@ def serve_sequential(requests, *, tile: int = 256, batch_size: int = 32, device:
             if wait > 0:
                 time.sleep(wait)
         started = clock() - t0
-        run = PlainRun(req.workload, tiled_factory(tile, device), batch_size=batch_size)
+        run = PlainRun(req.workload, tiled_factory(tile, device, cfl='auto'), batch_size=batch_size)
         while not run.done:
             run.advance()
         out.append(Completed(req.id, req.arrival, started, clock() - t0, run.w.cells, run.steps,

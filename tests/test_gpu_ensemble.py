@@ -26,7 +26,7 @@ def members():
 def alone(w, tile):
     from nhflood.ensemble import tiled_factory
     from nhflood.plain import PlainRun
-    run = PlainRun(w, tiled_factory(tile))
+    run = PlainRun(w, tiled_factory(tile, cfl='fused'))  # the members run the separate CFL pass
     rows = []
     while not run.done:
         tw, ow = run.begin()

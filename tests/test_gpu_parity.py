@@ -47,16 +47,22 @@ CASES = {
 
 
 def cuda_engine(path):
+    """'auto': the fused step as chosen for the mesh (these small meshes
+    keep the CFL in the step); 'pass': the fused step with the separate CFL
+    pass; 'multipass': the reference's pass structure."""
     def factory(arrays, params):
         from nhflood.native import CudaEngine
-        params.path = path
+        params.path = 'multipass' if path == 'multipass' else 'auto'
+        params.cfl = 'pass' if path == 'pass' else 'auto'
         engine = CudaEngine(arrays, params)
-        assert engine.path.startswith('tiled' if path == 'auto' else 'multipass'), engine.path
+        assert engine.path.startswith('multipass' if path == 'multipass' else 'tiled'), engine.path
+        if path == 'pass':
+            assert 'cfl=pass' in engine.path, engine.path
         return engine
     return factory
 
 
-PATHS = ['auto', 'multipass']
+PATHS = ['auto', 'pass', 'multipass']
 
 
 @pytest.mark.parametrize('path', PATHS)
