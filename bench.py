@@ -67,7 +67,7 @@ def algorithmic_bytes(w):
 
 # DRAM bytes (read + write) of one fused step launch, from the ncu captures
 # summarised in profiles/ (k_step_tiled_<workload>.md).
-TRAFFIC_PER_LAUNCH = {'multires_quadtree': 160.490752e6 + 18.082304e6}
+TRAFFIC_PER_LAUNCH = {'multires_quadtree': 148.207616e6 + 18.244352e6}
 
 
 def combine_ranks(times, units, device, world):
@@ -190,7 +190,7 @@ def bench_batched(args, rank, world, local):
     t_setup = time.perf_counter() - t0
     stream = ens.ensemble.stream()
     # spin-up (untimed) a third into the members' runs, as for the plain form
-    spin_to = min(r.w.duration for r in ens.runs) / 3
+    spin_to = min(r.w.duration for r in ens.runs) / 3 if args.spin_up is None else args.spin_up
     while min(r.elapsed for r in ens.runs) < spin_to and not ens.done:
         ens.advance()
     for _ in range(args.warmup):
@@ -376,6 +376,8 @@ def main():
     ap.add_argument('--tile', type=int, default=None, help='batched: tile size (default: autotuned)')
     ap.add_argument('--grid', type=int, default=None, help='batched: 0 persistent, -1 block per tile')
     ap.add_argument('--plain-batches', type=int, default=2)
+    ap.add_argument('--spin-up', type=float, default=None,
+                    help='simulated seconds advanced (untimed) before the warm-up; default a third of the run')
     args = ap.parse_args()
 
     rank = int(os.environ.get('RANK', 0))
@@ -419,7 +421,8 @@ def main():
     stream = eng.stream()
     # spin-up (untimed): the timed batches start a third into the run, where
     # rain and flow have reached the domain, not on the initial dry state
-    while run.elapsed < w.duration / 3 and not run.done:
+    spin_to = w.duration / 3 if args.spin_up is None else args.spin_up
+    while run.elapsed < spin_to and not run.done:
         run.advance()
     spin_up_s = run.elapsed
     # warm-up batches (untimed)
@@ -502,7 +505,9 @@ def main():
                          'traffic_unit': 'bytes per step launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)',
                          'algorithmic_bytes_per_launch': b_alg * w.cells,
                          'peak_kind': kind, 'algorithmic_bytes_per_cell_update': b_alg,
-                         'scope': 'whole batch graph (fused step kernel + per-batch epilogue)'},
+                         'scope': ('whole batch graph (' + ('fused step kernel, its CFL pass' if 'cfl=pass' in eng.path
+                                   else 'fused step kernel' if tiled else 'multi-pass kernels')
+                                   + ', per-batch epilogue)')},
             'e2e': {'value': e2e, 'unit': METRIC, 'h2d_bytes_per_step': h2d // max(1, e2e_batches),
                     'd2h_bytes_per_step': d2h // max(1, e2e_batches)},
             'clocks': clocks.summary(),

@@ -175,3 +175,39 @@ def test_six_boundaries_use_the_wide_budget_bit_exact(tmp_path, cuda_available, 
         results.append(run(dc, ForceConfig(boundaries=boundaries, rainfall=rain), engine))
     assert_runs_identical(*results)
     assert results[0].manifest["steps"] > 100 and sum(k.startswith("level:") for k in results[0].budget) == 3
+
+
+@pytest.mark.parametrize('cfl', ['fused', 'pass'])
+def test_tile_1024_both_cfl_forms_bit_exact(cuda_available, cfl):
+    """The 1024-cell tiles (512 threads, two cells per thread) in both CFL
+    forms on the 65,536-cell configuration: 40 batches from t = 0, traces and
+    every state array identical to the oracle after each batch."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / 'oracle'))
+    from engine import OracleEngine
+    from nhflood.model import STATE_F32, STATE_U32
+    from nhflood.native import CudaEngine
+    from nhflood.plain import PlainRun
+    from nhflood.workloads import plain_uniform_256
+
+    def cuda(arrays, params):
+        params.path, params.cfl = 'tile1024', cfl
+        engine = CudaEngine(arrays, params)
+        assert engine.path.startswith('tiled(tile=1024') and f'cfl={cfl}' in engine.path, engine.path
+        return engine
+
+    w = plain_uniform_256()
+    runs = [PlainRun(w, lambda a, p: OracleEngine(a, p)), PlainRun(w, cuda)]
+    for _ in range(40):
+        rows = []
+        for r in runs:
+            tw, ow = r.begin()
+            rows.append(r.engine.run_batch(tw, ow))
+            r.finish(rows[-1])
+        np.testing.assert_array_equal(rows[0], rows[1])
+        for name in STATE_F32 + STATE_U32:
+            assert runs[0].engine.get(name).tobytes() == runs[1].engine.get(name).tobytes(), name
+    assert runs[1].elapsed > 0
+    for r in runs:
+        r.close()
