@@ -219,12 +219,12 @@ def bench_batched(args, rank, world, local):
         torch.cuda.synchronize(device)
     device_s = sum(starts[i].elapsed_time(ends[i]) for i in range(recorded)) / 1e3
     # the same scenarios, one after another, each on a plain engine of its own
-    # (the plain form's own CFL choice) continuing from the member's state
-    from nhflood.ensemble import tiled_factory
+    # (the plain form's own tile and CFL choice) continuing from the member's state
+    from nhflood.native import CudaEngine
     from nhflood.plain import PlainRun
     plain_cells, plain_s = 0, 0.0
     for member in ens.runs:
-        r = PlainRun(member.w, tiled_factory(ens.tile, str(device), cfl='auto'), batch_size=member.params.batch_size)
+        r = PlainRun(member.w, lambda a, p: CudaEngine(a, p, device=str(device)), batch_size=member.params.batch_size)
         r.adopt(member)
         st = r.engine.stream()
         for _ in range(args.plain_batches):
