@@ -253,7 +253,7 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
     tl.lohi = sh_lohi;
     tl.fdesc = sh_fdesc;
     tl.fidx = sh_fidx;
-    if (tid == 0) sh_s[0] = 0.0f;  // donor_scale of the exterior sentinel (ring 3 is never a donor)
+    if (tid == 0) sh_s[0] = 0.0f;  // donor_scale of the exterior sentinel (the outer ring is never a donor)
     cp_async_wait_all();
     __syncthreads();
 
@@ -357,7 +357,8 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
     }
     __syncthreads();
 
-    // P3: final discharge of faces(ring <= 1) (solver_compact.py:516-522).
+    // P3: final discharge of the final faces (rings 0..1, ring 0 in the split form)
+    // (solver_compact.py:516-522).
     {
         uint32_t my_faces = 0;
         for (int j = tid; j < tl.n_qf; j += NT) {
