@@ -11,7 +11,6 @@ checkpoints) are skipped: they are host I/O outside the step.
 from __future__ import annotations
 
 import bisect
-import math
 
 import numpy as np
 

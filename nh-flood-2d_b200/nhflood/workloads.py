@@ -28,7 +28,7 @@ from pathlib import Path
 
 import numpy as np
 
-from .forcing import Boundary, Forcing, RainField, TimeSeries, select_boundary
+from .forcing import Forcing, RainField, TimeSeries, select_boundary
 from .geometry import MeshGeometry
 from .input import DomainConfig, LandParameters
 from .output import Checkpoint

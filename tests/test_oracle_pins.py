@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from runner import run
-from scenarios import grid_cell, grid_horizontal, grid_vertical, two_cell_case
+from scenarios import two_cell_case
 
 ORACLE = 'oracle'
 

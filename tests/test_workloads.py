@@ -2,7 +2,6 @@
 its cell with the right orientation, every side listed by exactly its
 cells), 2:1 balance, hanging interfaces, and the forcing they carry."""
 import numpy as np
-import pytest
 
 from nhflood.geometry import MeshGeometry
 from nhflood.workloads import dambreak, multires_quadtree, plain_uniform_256, uniform_grid
