@@ -184,7 +184,9 @@ const char *nhf_path(const nhf_handle *h);
  * Terms (10 count + 8, the reference's order): per gate pond in/out, river
  * in/out; overtopping in/out and the pond's six source terms (rain,
  * infiltration, positivity, pipe, boundary, rounding); per gate the
- * channel's six source terms. Gates need the multi-pass step (path 1). */
+ * channel's six source terms. Gates run on the multi-pass step (path 1) or on
+ * the fused step with 256-cell tiles and the separate CFL pass (path 256,
+ * cfl_mode 2); the source terms then come from the fused depth update. */
 typedef struct nhf_gate {
     int32_t count;           /* gates */
     int32_t n_targets;       /* gate cells */

@@ -283,8 +283,12 @@ struct TiledBuild {
 int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, size_t why_len,
                 int tile_request = 0, int cfl_mode = 0);
 // Enqueue one fused step (plus the hanging/theta pre-passes and, for split
-// plans, the CFL pass).
-void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s);
+// plans, the CFL pass). With a gate controller (256-cell tiles, split plan)
+// only the pre-passes and the gate-enabled step: the caller then enqueues
+// the controller's passes and tiled_enqueue_cfl.
+void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s, const GateDev *gate = nullptr);
+// The separate CFL pass of a split plan (nothing otherwise).
+void tiled_enqueue_cfl(const Dev &d, const TiledBuild &b, cudaStream_t s);
 // Enqueue the batch epilogue: bring the state back into the caller's
 // buffers and refresh u, v.
 void tiled_enqueue_batch_end(const Dev &d, cudaStream_t s);

@@ -459,10 +459,11 @@ __global__ void __launch_bounds__(256) k_gate_move(Dev d, GateDev g, int at_end)
     const uint32_t hi = at_end ? c->step_end[0] : c->now[0];
     const uint32_t lo = at_end ? c->step_end[1] : c->now[1];
     if (!at_end) {
+        const float *depth = cur_depth(d, c->parity);
         const bool formal = hi > g.formal_hi || (hi == g.formal_hi && lo >= g.formal_lo);
         for (int gate = threadIdx.x; formal && gate < g.count; gate += blockDim.x) {
             int cell = g.controls[gate];
-            if (g.commanded[gate] == 0 && m.depth[cell] >= d.min_h && m.bed[cell] + m.depth[cell] > g.trigger_level) {
+            if (g.commanded[gate] == 0 && depth[cell] >= d.min_h && m.bed[cell] + depth[cell] > g.trigger_level) {
                 g.commanded[gate] = 1;
                 g.command[2 * gate] = hi; g.command[2 * gate + 1] = lo;
             }
@@ -501,7 +502,7 @@ __global__ void __launch_bounds__(kBlock) k_gate_flux(Dev d, GateDev g)
     if (p < g.n_flux) {
         int si = g.flux_sides[p];
         int left = m.topology[3 * si + 1], right = m.topology[3 * si + 2];
-        float volume = m.q[si] * m.length[si] * c->dt;
+        float volume = cur_q(d, c->parity)[si] * m.length[si] * c->dt;
         int gl = g.cell_gate[left], gr = g.cell_gate[right];
         int pl = g.pond[left], pr = g.pond[right];
         int latch = -1;
@@ -787,7 +788,20 @@ int build_graph(nhf_handle *h)
     k_begin<<<1, 256, 0, h->s>>>(h->dev, 0u, 0u, 0u, 0u, h->tiled ? 1 : 0);
     if (h->tiled) {
         tiled_enqueue_batch_start(h->dev, h->s);
-        for (int i = 0; i < h->p.batch_size; ++i) tiled_enqueue_step(h->dev, h->tb, h->s);
+        for (int i = 0; i < h->p.batch_size; ++i) {
+            if (h->gate_on) {
+                // check_gates, the step with the source terms, the exchange
+                // volumes, finish_gate_bed, then the CFL pass
+                k_gate_move<<<1, 256, 0, h->s>>>(h->dev, h->gate, 0);
+                tiled_enqueue_step(h->dev, h->tb, h->s, &h->gate);
+                if (h->gate.n_flux > 0)
+                    k_gate_flux<<<grid_for(h->gate.n_flux, kBlock), kBlock, 0, h->s>>>(h->dev, h->gate);
+                k_gate_move<<<1, 256, 0, h->s>>>(h->dev, h->gate, 1);
+                tiled_enqueue_cfl(h->dev, h->tb, h->s);
+            } else {
+                tiled_enqueue_step(h->dev, h->tb, h->s);
+            }
+        }
         tiled_enqueue_batch_end(h->dev, h->s);
     } else {
         for (int i = 0; i < h->p.batch_size; ++i) enqueue_step(h);
@@ -1140,7 +1154,9 @@ int nhf_budget_flush(nhf_handle *h, double *totals)
 int nhf_gate_attach(nhf_handle *h, const nhf_gate *gate)
 {
     if (!h || !gate) return NHF_EINVAL;
-    if (h->tiled) return fail(h, NHF_EINVAL, "gate control runs on the multi-pass step (nhf_params.path = 1)");
+    if (h->tiled && !(h->tb.plan.tile == 256 && h->tb.plan.split))
+        return fail(h, NHF_EINVAL, "gate control runs on the multi-pass step or on the fused step with 256-cell "
+                                   "tiles and the separate CFL pass (nhf_params.path = 1, or 256 with cfl_mode 2)");
     if (h->gate_on) return fail(h, NHF_ESTATE, "a gate controller is already attached");
     if (gate->count < 1 || gate->n_targets < 0 || gate->n_flux < 0)
         return fail(h, NHF_EINVAL, "invalid gate sizes");

@@ -142,9 +142,14 @@ __device__ __forceinline__ float term_value(int t, int B, float removed, float f
 
 // One fused step of tile t of the mesh described by d (n_tiles tiles).
 // kHang: 0 no hanging edges, 1 hanging edges, 2 decided by d at run time.
-template <bool kThetaOne, int kHang, int NT, int CPT>
-__device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const unsigned n_tiles)
+// kGate (256-cell tiles, separate CFL pass): the gate controller's source
+// terms of pond and gate cells (core/gate.py:151-193) from the depth update,
+// reduced per 256-cell block into gd's partials.
+template <bool kThetaOne, int kHang, int NT, int CPT, bool kGate = false>
+__device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const unsigned n_tiles,
+                                          const GateDev *gd = nullptr)
 {
+    static_assert(!kGate || (NT == 256 && CPT == 1), "gate terms need one 256-cell budget block per tile");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long sh_min[NT / 32];
     __shared__ uint32_t sh_cnt[3];
@@ -379,6 +384,8 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
     // block of the tile sits on one 256-thread half in thread order.
     CellTerms<CPT> terms;
     uint32_t my_wet = 0;
+    int g_off = -1;  // kGate: first source term of this pond or gate cell, -1 elsewhere
+    float g_v[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     const int T = d.terms;
     const int B = m.b_num;
     const uint32_t step_hi = c->step_end[0], step_lo = c->step_end[1];
@@ -486,6 +493,27 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
             m.peak_hi[g] = step_hi; m.peak_lo[g] = step_lo;
         }
         my_wet += depth >= d.min_h ? 1u : 0u;
+        if (kGate) {
+            // record_cell, measure_inventory and the rounding term
+            // (solver_compact.py:595-604; gate.py:151-193)
+            const int cg = gd->cell_gate[g];
+            g_off = gd->pond[g] == 1 ? 4 * gd->count + 2 : (cg >= 0 ? 4 * gd->count + 8 + 6 * cg : -1);
+            if (g_off >= 0) {
+                float applied_floor = floor_v, level_exchange = 0.0f;
+                if (kind == 0) {
+                    applied_floor = 0.0f;
+                    level_exchange = (depth - previous) * ea - (ql - qr + qb - qt) * dt - pipe * dt
+                                     - rain_depth * ea + removed * ea;
+                }
+                g_v[0] = rain_depth * ea;
+                g_v[1] = removed * ea;
+                g_v[2] = applied_floor * ea;
+                g_v[3] = pipe * dt;
+                g_v[4] = (ssq - pipe) * dt + level_exchange;
+                const float rounding = (depth - previous) - increment + removed - applied_floor;
+                g_v[5] = rounding * ea - level_exchange;
+            }
+        }
         if (T <= 32) {
             uint32_t mask = 0;
             if (terms.removed[kk] != 0.0f) mask |= 1u;
@@ -601,6 +629,27 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
                 const int blk = blk0 + (tid >> 8);
                 if ((tid & 255) == 0 && blk < d.blocks && sum != 0.0)
                     acc_add(d.acc_sum + (size_t)blk * T + t, d.acc_comp + (size_t)blk * T + t, sum);
+            }
+        }
+    }
+
+    if (kGate) {
+        // gate source terms: the pond group, then gate by gate, six terms
+        // each, the canonical 256-cell tree in the dead shared arrays
+        double *buf = reinterpret_cast<double *>(smem_raw);
+        const int blk = tl.cbase >> 8;
+        for (int grp = -1; grp < gd->count; ++grp) {
+            const int off = grp < 0 ? 4 * gd->count + 2 : 4 * gd->count + 8 + 6 * grp;
+            if (!__syncthreads_or(g_off == off)) continue;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const float val = g_off == off ? g_v[k] : 0.0f;
+                if (!__syncthreads_or(val != 0.0f)) continue;
+                const double sum = tree_halves<NT>((double)val, buf);
+                if (tid == 0) {
+                    const size_t idx = (size_t)blk * gd->terms + off + k;
+                    acc_add(gd->acc_sum + idx, gd->acc_comp + idx, sum);
+                }
             }
         }
     }
@@ -743,6 +792,16 @@ template <bool kThetaOne, bool kHanging, int NT, int CPT>
 __global__ void __launch_bounds__(NT, kMinBlocks<NT>) k_step_tiled(const __grid_constant__ Dev d)
 {
     step_tile<kThetaOne, kHanging ? 1 : 0, NT, CPT>(d, blockIdx.x, gridDim.x);
+}
+
+// The fused step with the gate controller's source terms (256-cell tiles,
+// split plans); the controller's bed motion and exchange volumes are
+// separate passes around it.
+template <bool kThetaOne, bool kHanging>
+__global__ void __launch_bounds__(256, 4) k_step_tiled_gate(const __grid_constant__ Dev d,
+                                                            const __grid_constant__ GateDev g)
+{
+    step_tile<kThetaOne, kHanging ? 1 : 0, 256, 1, true>(d, blockIdx.x, gridDim.x, &g);
 }
 
 // CFL pass of one mesh after its fused step (grid-stride over the sides);
@@ -1091,6 +1150,12 @@ void set_smem_all(size_t bytes)
     set_smem(k_step_tiled<false, true, NT, CPT>, bytes);
     set_smem(k_step_ensemble<true, NT, CPT>, bytes);
     set_smem(k_step_ensemble<false, NT, CPT>, bytes);
+    if (NT == 256 && CPT == 1) {
+        set_smem(k_step_tiled_gate<true, false>, bytes);
+        set_smem(k_step_tiled_gate<false, false>, bytes);
+        set_smem(k_step_tiled_gate<true, true>, bytes);
+        set_smem(k_step_tiled_gate<false, true>, bytes);
+    }
 }
 
 template <int NT, int CPT>
@@ -1402,18 +1467,36 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
     return 0;
 }
 
-void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s)
+void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s, const GateDev *gate)
 {
     const nhf_mesh &m = d.m;
     if (m.hang_cells > 0) k_pressure_tiled<<<(m.hang_cells + 255) / 256, 256, 0, s>>>(d);
     if (!d.theta_one) k_face_qn_tiled<<<(m.e_num + 255) / 256, 256, 0, s>>>(d);
+    if (gate) {  // 256-cell tiles, split plan (checked when the controller is attached)
+        const int grid = d.plan.n_tiles;
+        const size_t smem = b.shared_bytes;
+        const bool hanging = m.hang_cells > 0;
+        if (d.theta_one) {
+            if (hanging) k_step_tiled_gate<true, true><<<grid, 256, smem, s>>>(d, *gate);
+            else k_step_tiled_gate<true, false><<<grid, 256, smem, s>>>(d, *gate);
+        } else {
+            if (hanging) k_step_tiled_gate<false, true><<<grid, 256, smem, s>>>(d, *gate);
+            else k_step_tiled_gate<false, false><<<grid, 256, smem, s>>>(d, *gate);
+        }
+        return;  // the caller adds the controller's passes, then the CFL pass
+    }
     switch (d.plan.tile) {
     case 1024: launch_step<512, 2>(d, b.shared_bytes, s); break;
     case 512: launch_step<512, 1>(d, b.shared_bytes, s); break;
     default: launch_step<256, 1>(d, b.shared_bytes, s); break;
     }
+    tiled_enqueue_cfl(d, b, s);
+}
+
+void tiled_enqueue_cfl(const Dev &d, const TiledBuild &b, cudaStream_t s)
+{
     if (b.plan.split) {
-        int gc = (m.s_num + 255) / 256;
+        int gc = (d.m.s_num + 255) / 256;
         if (gc > 148 * 8) gc = 148 * 8;
         k_cfl_tiled<<<gc, 256, 0, s>>>(d);
     }

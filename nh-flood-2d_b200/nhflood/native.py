@@ -195,11 +195,14 @@ class CudaEngine(Engine):
             setattr(mesh, name, tensor.data_ptr() if tensor is not None else None)
         self._mesh = mesh
         path = path_code(params.path)
-        if arrays.gate is not None:
-            if path not in (0, 1):
-                raise ValueError('gate control runs on the multi-pass step; use path "auto" or "multipass"')
-            path = 1
         cfl_mode = {'auto': 0, 'fused': 1, 'pass': 2}[params.cfl]
+        if arrays.gate is not None:
+            # the controller runs on the fused step with 256-cell tiles and the
+            # separate CFL pass, or on the multi-pass step
+            if path not in (0, 1, 256) or (path != 1 and params.cfl == 'fused'):
+                raise ValueError('gate control needs path "auto", "tile256" or "multipass" and a separate CFL pass')
+            if path != 1:
+                path, cfl_mode = 256, 2
         p = NhfParams(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size, path,
                       cfl_mode)
         handle = c_void_p()

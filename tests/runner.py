@@ -23,7 +23,13 @@ def cuda_factory(arrays, params):
     return CudaEngine(arrays, params)
 
 
-FACTORIES = {'oracle': oracle_factory, 'cuda': cuda_factory}
+def cuda_multipass_factory(arrays, params):
+    from nhflood.native import CudaEngine
+    params.path = 'multipass'
+    return CudaEngine(arrays, params)
+
+
+FACTORIES = {'oracle': oracle_factory, 'cuda': cuda_factory, 'cuda_multipass': cuda_multipass_factory}
 
 
 @dataclass

@@ -1,5 +1,6 @@
-"""Gate controller on the B200: the CUDA step with the controller attached is
-bit-identical to the CPU restatement through the whole time loop (state,
+"""Gate controller on the B200: the CUDA step with the controller attached,
+on the fused step (256-cell tiles, separate CFL pass) and on the multi-pass
+step, is bit-identical to the CPU restatement through the whole time loop (state,
 trace, controller words and every exchange and source total of the
 ``gate_control`` report), on the reference's gate mechanism cases: bed
 motion and pond exchange, a short level pulse latching the command, seven
@@ -19,20 +20,25 @@ STATE = ('depth', 'bed', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_spe
          'first_time_lo')
 
 
+CUDA = ('cuda', 'cuda_multipass')
+
+
 def same(tmp_path, make, seconds, **kw):
     results = {}
-    for engine in ('oracle', 'cuda'):
+    for engine in ('oracle',) + CUDA:
         dc, force = make(tmp_path / engine)
         results[engine] = run(dc, force, seconds, engine=engine, **kw)
-    a, b = results['oracle'], results['cuda']
-    assert b.manifest['backend'] == 'cuda'
-    for name in STATE:
-        assert getattr(a.state, name).tobytes() == getattr(b.state, name).tobytes(), name
-    np.testing.assert_array_equal(a.trace, b.trace)
-    assert a.manifest['gate_control'] == b.manifest['gate_control']
-    assert a.state.gate_open == b.state.gate_open
-    assert a.manifest['mass_balance_final'] == b.manifest['mass_balance_final']
-    return a, b
+    a = results['oracle']
+    for engine in CUDA:
+        b = results[engine]
+        assert b.manifest['backend'] == 'cuda'
+        for name in STATE:
+            assert getattr(a.state, name).tobytes() == getattr(b.state, name).tobytes(), (engine, name)
+        np.testing.assert_array_equal(a.trace, b.trace)
+        assert a.manifest['gate_control'] == b.manifest['gate_control'], engine
+        assert a.state.gate_open == b.state.gate_open
+        assert a.manifest['mass_balance_final'] == b.manifest['mass_balance_final'], engine
+    return a, results['cuda']
 
 
 def test_bed_motion_and_pond_exchange(tmp_path):
@@ -114,24 +120,28 @@ def test_restart_during_opening_matches_the_oracle(tmp_path):
         dc, force, *_ = setup(path, boundaries=boundaries, depth=[1, 0, 0], bed=[0, 3, 0],
                               gate=dict(trigger_level=1.5, opening_seconds=2))
         return dc, force
-    for engine in ('oracle', 'cuda'):
+    for engine in ('oracle',) + CUDA:
         dc, force = make(tmp_path / engine)
         run(dc, force, 3, output=tmp_path / engine / 'part', engine=engine)
     results = {}
-    for engine in ('oracle', 'cuda'):
+    for engine in ('oracle',) + CUDA:
         dc, force = make(tmp_path / engine)
         results[engine] = run(dc, force, 6, output=tmp_path / engine / 'resumed', engine=engine,
                               restart=tmp_path / engine / 'part/output/state_final.fdb')
-    a, b = results['oracle'], results['cuda']
-    for name in STATE:
-        assert getattr(a.state, name).tobytes() == getattr(b.state, name).tobytes(), name
-    assert a.manifest['gate_control'] == b.manifest['gate_control']
+    a = results['oracle']
+    for engine in CUDA:
+        b = results[engine]
+        for name in STATE:
+            assert getattr(a.state, name).tobytes() == getattr(b.state, name).tobytes(), (engine, name)
+        assert a.manifest['gate_control'] == b.manifest['gate_control'], engine
 
 
-def test_gated_polder_matches_the_oracle_batch_by_batch():
+@pytest.mark.parametrize('path', ['auto', 'multipass'])
+def test_gated_polder_matches_the_oracle_batch_by_batch(path):
     """The polder workload at 128 x 128 (four gates, 256 gate cells, 384
-    recorded sides): 10 batches on both engines, state, controller words and
-    gate totals identical after every batch."""
+    recorded sides), on the fused and the multi-pass step: 10 batches on
+    both engines, state, controller words and gate totals identical after
+    every batch."""
     import sys
     from pathlib import Path
     sys.path.insert(0, str(Path(__file__).resolve().parents[1] / 'oracle'))
@@ -141,8 +151,15 @@ def test_gated_polder_matches_the_oracle_batch_by_batch():
     from nhflood.native import CudaEngine
     from nhflood.plain import PlainRun
     w = workloads.gated_polder(n=128, dx=40.0)
-    runs = [PlainRun(w, lambda a, p: OracleEngine(a, p)), PlainRun(w, lambda a, p: CudaEngine(a, p))]
-    assert runs[1].engine.path.startswith('multipass')
+    def cuda(a, p):
+        p.path = path
+        return CudaEngine(a, p)
+
+    runs = [PlainRun(w, lambda a, p: OracleEngine(a, p)), PlainRun(w, cuda)]
+    if path == 'auto':
+        assert runs[1].engine.path.startswith('tiled(tile=256') and 'cfl=pass' in runs[1].engine.path
+    else:
+        assert runs[1].engine.path.startswith('multipass')
     for _ in range(10):
         steps = [r.advance() for r in runs]
         assert steps[0] == steps[1]
