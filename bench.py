@@ -376,6 +376,7 @@ def main():
     ap.add_argument('--tile', type=int, default=None, help='batched: tile size (default: autotuned)')
     ap.add_argument('--grid', type=int, default=None, help='batched: 0 persistent, -1 block per tile')
     ap.add_argument('--plain-batches', type=int, default=2)
+    ap.add_argument('--path', default='auto', help="plain form's step: 'auto', 'multipass', 'tile256', 'tile512', 'tile1024'")
     ap.add_argument('--spin-up', type=float, default=None,
                     help='simulated seconds advanced (untimed) before the warm-up; default a third of the run')
     args = ap.parse_args()
@@ -416,7 +417,10 @@ def main():
     from nhflood.plain import PlainRun
 
     w = make_workload(args.workload)
-    run = PlainRun(w, lambda a, p: CudaEngine(a, p, device=str(device)))
+    def factory(a, p):
+        p.path = args.path
+        return CudaEngine(a, p, device=str(device))
+    run = PlainRun(w, factory)
     eng = run.engine
     stream = eng.stream()
     # spin-up (untimed): the timed batches start a third into the run, where
