@@ -223,7 +223,7 @@ def bench_batched(args, rank, world, local):
     from nhflood.native import CudaEngine
     from nhflood.plain import PlainRun
     plain_cells, plain_s = 0, 0.0
-    for member in ens.runs:
+    for member in ens.runs if args.plain_batches > 0 else ():
         r = PlainRun(member.w, lambda a, p: CudaEngine(a, p, device=str(device)), batch_size=member.params.batch_size)
         r.adopt(member)
         st = r.engine.stream()
