@@ -70,6 +70,21 @@ def algorithmic_bytes(w):
 TRAFFIC_PER_LAUNCH = {'multires_quadtree': 148.207616e6 + 18.244352e6}
 
 
+def launches_per_batch(run) -> int:
+    """Kernels one batch graph of a plain run launches: begin (+ rain-time
+    copy, state copy-back and velocity on the fused step), and per step the
+    fused step (+ its CFL pass on split plans) or the six multi-pass kernels,
+    the hanging-edge and theta pre-passes, and the gate controller's bed
+    motion (twice) and exchange volumes."""
+    eng = run.engine
+    tiled = eng.path.startswith('tiled')
+    pre = (1 if run.arrays.hang_cells else 0) + (0 if run.w.sita == 1.0 else 1)
+    gate = run.arrays.gate
+    pre += 0 if gate is None else 2 + (1 if len(gate.flux_sides) else 0)
+    per_step = ((2 if 'cfl=pass' in eng.path else 1) if tiled else 6) + pre
+    return (4 if tiled else 1) + run.params.batch_size * per_step
+
+
 def combine_ranks(times, units, device, world):
     """Whole-job figures over the replicas: the slowest rank's times (max)
     and the units of all ranks (sum). times, units: equal-length lists of
@@ -204,8 +219,10 @@ def bench_batched(args, rank, world, local):
     cell_updates = 0
     recorded = 0
     hang = sum(1 for r in ens.runs if r.arrays.hang_cells)
-    # per step: the ensemble step, its CFL pass, the hanging pre-pass if any member has hanging edges
-    per_batch_kernels = 5 + ens.runs[0].params.batch_size * (2 + (1 if hang else 0))
+    if ens.schedule == 'member graphs':  # every member's own batch graph
+        per_batch_kernels = sum(launches_per_batch(r) for r in ens.runs)
+    else:  # per step: the ensemble step, its CFL pass, the hanging pre-pass if any member has hanging edges
+        per_batch_kernels = 5 + ens.runs[0].params.batch_size * (2 + (1 if hang else 0))
     with ClockSampler(local) as clocks:
         for k in range(args.steps):
             if ens.done:
@@ -269,7 +286,8 @@ def bench_batched(args, rank, world, local):
             'config': {'workload': f'ensemble_{args.members}_quadtrees', 'members': len(ws),
                        'cells': int(cells.sum()), 'cells_min': int(cells.min()), 'cells_max': int(cells.max()),
                        'time_steps_per_bench_step': ens.runs[0].params.batch_size,
-                       'tile': ens.ensemble.tile, 'grid_blocks': ens.ensemble.grid, 'tiles': ens.ensemble.tiles,
+                       'schedule': ens.schedule, 'tile': ens.ensemble.tile or 'per member',
+                       'grid_blocks': ens.ensemble.grid, 'tiles': ens.ensemble.tiles,
                        'spin_up_to_s': spin_to,
                        'l2': 'inputs larger than L2', 'parallelism': f'replicas{world}'},
             'plain_sequential': {'value': plain, 'unit': METRIC,
@@ -441,13 +459,7 @@ def main():
     cell_steps = 0
     launches = 0
     tiled = eng.path.startswith('tiled')
-    pre = (1 if run.arrays.hang_cells else 0) + (0 if w.sita == 1.0 else 1)
-    gate = run.arrays.gate
-    # gate controller: bed motion at start and end, exchange volumes (multi-pass only)
-    pre += 0 if gate is None else 2 + (1 if len(gate.flux_sides) else 0)
-    # fused step (+ its CFL pass on split plans) or the six multi-pass kernels
-    per_step_kernels = ((2 if 'cfl=pass' in eng.path else 1) if tiled else 6) + pre
-    per_batch_kernels = 4 if tiled else 1  # begin (+ rain-time copy, state copy-back, velocity)
+    per_batch_launches = launches_per_batch(run)
     recorded = 0
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=device)
     with ClockSampler(local) as clocks:
@@ -464,7 +476,7 @@ def main():
             ends[k].record(stream)
             n = run.finish(eng.read_trace())
             cell_steps += n * w.cells
-            launches += per_batch_kernels + run.params.batch_size * per_step_kernels
+            launches += per_batch_launches
         torch.cuda.synchronize(device)
     timed = [starts[i].elapsed_time(ends[i]) for i in range(recorded)]
     device_ms = float(sum(timed))

@@ -215,14 +215,18 @@ int nhf_gate_flush(nhf_handle *h, double *totals);
  * (solver_compact.py:179-1008); an ensemble advances many member handles
  * together, one fused step launch per slot for all of them, each member
  * with its own clock, CFL dt, limiter statistics, budget and extrema.
- * Members must run the fused tiled step with one tile size (nhf_params.path
- * = that size), one batch size and one theta class (= 1 or < 1). A batch
+ * For the single-launch schedules members must run the fused tiled step
+ * with one tile size (nhf_params.path = that size, cfl_mode 2), one batch
+ * size and one theta class (= 1 or < 1). A batch
  * starts after the work queued so far on `stream` and on every member's
  * creation stream, and those streams wait for the batch. Everything else
  * about a member (forcing, clock, budget flush, stations, CFL read-back)
  * still goes through its own handle between batches. grid_blocks: 0 =
  * persistent grid (resident blocks per SM x SMs), -1 = one block per tile,
- * > 0 = that many blocks. */
+ * > 0 = that many blocks; -2 = member graphs: every member runs its own
+ * batch graph (its own step form, tile size and CFL placement) on its own
+ * stream, all members launched together; members then need to share only
+ * the batch size. */
 typedef struct nhf_ensemble nhf_ensemble;
 int nhf_ensemble_create(nhf_handle *const *members, int32_t n, int32_t grid_blocks, void *stream,
                         nhf_ensemble **out);

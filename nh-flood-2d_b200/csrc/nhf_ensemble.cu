@@ -1,11 +1,15 @@
-// Ensemble form of the C ABI: many member meshes (each an nhf_handle on the
-// fused tiled step, all with the same tile size and batch size) advance
-// together. One batch is one CUDA graph: the members' begin words in, for
-// every slot one pre-pass launch per hanging/theta need and ONE fused step
-// launch over the tiles of all members, the batch epilogue, and every
-// member's trace rows out. Each member keeps its own clock, dt (its own CFL
-// candidate), limiter statistics, budget partials and extrema, exactly as a
-// single-mesh batch does (solver_compact.py:918-985 per member).
+// Ensemble form of the C ABI: many member meshes advance together, each with
+// its own clock, dt (its own CFL candidate), limiter statistics, budget
+// partials and extrema, exactly as a single-mesh batch does
+// (solver_compact.py:918-985 per member). Two schedules:
+//  - one ensemble graph (members on the fused tiled step with one tile size
+//    and batch size): the members' begin words in, for every slot one
+//    pre-pass launch per hanging/theta need and ONE fused step launch over
+//    the tiles of all members, the batch epilogue, every member's trace out;
+//  - member graphs (grid_blocks = -2): every member runs its own batch graph
+//    (its own step form, tile size and CFL placement) on its own stream, all
+//    of them launched together, so that small members fill the GPU beside
+//    large ones while each keeps the single-mesh kernels.
 #include <cuda_runtime.h>
 
 #include <cstdarg>
@@ -31,6 +35,8 @@ struct nhf_ensemble {
     cudaGraph_t graph_def = nullptr;
     cudaGraphExec_t graph = nullptr;
     bool in_flight = false;
+    bool member_graphs = false;             // grid_blocks = -2
+    std::vector<cudaEvent_t> member_done;   // member-graph schedule: one per member
     std::string err;
 };
 
@@ -84,6 +90,61 @@ void append_chunks(std::vector<int2> &items, int member, int count)
     for (int c = 0; c * kEnsChunk < count; ++c) items.push_back(make_int2(member, c));
 }
 
+// The member-graph schedule: members may differ in step form and tile size,
+// not in batch size; their batch graphs are built here.
+int create_member_graphs(nhf_handle *const *members, int32_t n, void *stream, nhf_ensemble **out)
+{
+    const nhf_handle *h0 = members[0];
+    for (int i = 0; i < n; ++i) {
+        const nhf_handle *h = members[i];
+        if (!h) return efail(nullptr, NHF_EINVAL, "member %d is null", i);
+        if (h->p.batch_size != h0->p.batch_size) return efail(nullptr, NHF_EINVAL, "member %d has another batch size", i);
+        for (int j = 0; j < i; ++j)
+            if (members[j] == h) return efail(nullptr, NHF_EINVAL, "member %d is listed twice", i);
+    }
+    nhf_ensemble *e = new nhf_ensemble();
+    e->member_graphs = true;
+    e->members.assign(members, members + n);
+    e->user = (cudaStream_t)stream;
+    e->streams.push_back(e->user);
+    for (int i = 0; i < n; ++i) {
+        bool seen = false;
+        for (cudaStream_t st : e->streams) seen = seen || st == members[i]->user;
+        if (!seen) e->streams.push_back(members[i]->user);
+    }
+    int rc = NHF_OK;
+    auto bad = [&](int code, const char *what, cudaError_t err) {
+        rc = efail(nullptr, code, "%s failed: %s", what, cudaGetErrorString(err));
+        nhf_ensemble_destroy(e);
+        return rc;
+    };
+    cudaError_t err;
+    if ((err = cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking)) != cudaSuccess) return bad(NHF_ECUDA, "cudaStreamCreateWithFlags", err);
+    if ((err = cudaEventCreateWithFlags(&e->ev_in, cudaEventDisableTiming)) != cudaSuccess) return bad(NHF_ECUDA, "cudaEventCreateWithFlags", err);
+    if ((err = cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming)) != cudaSuccess) return bad(NHF_ECUDA, "cudaEventCreateWithFlags", err);
+    e->member_done.assign(n, nullptr);
+    int tiles = 0;
+    for (int i = 0; i < n; ++i) {
+        if ((err = cudaEventCreateWithFlags(&e->member_done[i], cudaEventDisableTiming)) != cudaSuccess)
+            return bad(NHF_ECUDA, "cudaEventCreateWithFlags", err);
+        int mrc = member_graph_prepare(members[i]);
+        if (mrc) {
+            rc = efail(nullptr, mrc, "member %d: %s", i, members[i]->err.c_str());
+            nhf_ensemble_destroy(e);
+            return rc;
+        }
+        tiles += members[i]->tiled ? members[i]->tb.plan.n_tiles : 0;
+    }
+    EnsembleLaunch &L = e->launch;
+    L.members = n;
+    L.batch = h0->p.batch_size;
+    L.tile = 0;     // per member
+    L.grid = -2;
+    L.n_step = tiles;
+    *out = e;
+    return NHF_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -101,6 +162,7 @@ int nhf_ensemble_destroy(nhf_ensemble *e)
     if (e->h_trace) cudaFreeHost(e->h_trace);
     if (e->ev_in) cudaEventDestroy(e->ev_in);
     if (e->ev_out) cudaEventDestroy(e->ev_out);
+    for (cudaEvent_t ev : e->member_done) cudaEventDestroy(ev);
     if (e->s) cudaStreamDestroy(e->s);
     delete e;
     return NHF_OK;
@@ -113,6 +175,8 @@ int nhf_ensemble_create(nhf_handle *const *members, int32_t n, int32_t grid_bloc
     *out = nullptr;
     const nhf_handle *h0 = members[0];
     if (!h0) return efail(nullptr, NHF_EINVAL, "member 0 is null");
+    if (grid_blocks < -2) return efail(nullptr, NHF_EINVAL, "grid_blocks must be -2, -1, 0 or positive");
+    if (grid_blocks == -2) return create_member_graphs(members, n, stream, out);
     const int tile = h0->tb.plan.tile;
     for (int i = 0; i < n; ++i) {
         const nhf_handle *h = members[i];
@@ -224,6 +288,25 @@ int nhf_ensemble_run_batch_async(nhf_ensemble *e, const uint32_t *targets, const
     // the pinned words of the previous batch may still be in use
     if (e->in_flight) ECK(e, cudaStreamSynchronize(e->s));
     const int n = e->launch.members;
+    if (e->member_graphs) {
+        // after all work queued on the caller streams, every member's own
+        // batch graph on its own stream; the ensemble stream joins them
+        for (cudaStream_t st : e->streams) {
+            ECK(e, cudaEventRecord(e->ev_in, st));
+            ECK(e, cudaStreamWaitEvent(e->s, e->ev_in, 0));
+        }
+        ECK(e, cudaEventRecord(e->ev_in, e->s));
+        for (int i = 0; i < n; ++i) {
+            int rc = member_graph_launch(e->members[i], targets + 2 * i, origins + 2 * i, e->ev_in, e->member_done[i]);
+            if (rc) return efail(e, rc, "member %d: %s", i, e->members[i]->err.c_str());
+        }
+        for (int i = 0; i < n; ++i) ECK(e, cudaStreamWaitEvent(e->s, e->member_done[i], 0));
+        e->in_flight = true;
+        ECK(e, cudaGetLastError());
+        ECK(e, cudaEventRecord(e->ev_out, e->s));
+        for (cudaStream_t st : e->streams) ECK(e, cudaStreamWaitEvent(st, e->ev_out, 0));
+        return NHF_OK;
+    }
     for (int i = 0; i < n; ++i) {
         e->h_words[4 * i] = targets[2 * i];
         e->h_words[4 * i + 1] = targets[2 * i + 1];
@@ -249,6 +332,12 @@ int nhf_ensemble_read_trace(nhf_ensemble *e, uint32_t *trace)
     if (!e || !trace) return NHF_EINVAL;
     ECK(e, cudaStreamSynchronize(e->s));
     e->in_flight = false;
+    if (e->member_graphs) {
+        const size_t rows = (size_t)NHF_TRACE_COLS * e->launch.batch;
+        for (int i = 0; i < e->launch.members; ++i)
+            memcpy(trace + rows * i, e->members[i]->h_trace, sizeof(uint32_t) * rows);
+        return NHF_OK;
+    }
     memcpy(trace, e->h_trace, sizeof(uint32_t) * NHF_TRACE_COLS * e->launch.batch * (size_t)e->launch.members);
     return NHF_OK;
 }

@@ -36,3 +36,11 @@ struct nhf_handle {
     std::string path = "multipass";
     std::string err;
 };
+
+namespace nhf {
+// The ensemble's member-graph schedule (nhf_step.cu): build a member's batch
+// graph, and launch it on the member's stream after `start`, recording `done`.
+int member_graph_prepare(nhf_handle *h);
+int member_graph_launch(nhf_handle *h, const uint32_t target[2], const uint32_t origin[2], cudaEvent_t start,
+                        cudaEvent_t done);
+}  // namespace nhf

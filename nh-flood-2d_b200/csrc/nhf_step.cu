@@ -835,6 +835,38 @@ int build_graph(nhf_handle *h)
 
 }  // namespace
 
+namespace nhf {
+
+// One member's own batch graph for the ensemble's member-graph schedule: the
+// member's stream waits for `start`, runs its batch towards `target` and
+// records `done`; the trace lands in the member's pinned trace buffer.
+int member_graph_prepare(nhf_handle *h)
+{
+    if (!h->graph) return build_graph(h);
+    return NHF_OK;
+}
+
+int member_graph_launch(nhf_handle *h, const uint32_t target[2], const uint32_t origin[2], cudaEvent_t start,
+                        cudaEvent_t done)
+{
+    int rc = member_graph_prepare(h);
+    if (rc) return rc;
+    CK(h, cudaStreamWaitEvent(h->s, start, 0));
+    Dev d = h->dev;
+    uint32_t w[4] = {target[0], target[1], origin[0], origin[1]};
+    int prepare_first = h->tiled ? 1 : 0;
+    void *args[6] = {&d, &w[0], &w[1], &w[2], &w[3], &prepare_first};
+    cudaKernelNodeParams kp = h->begin_params;
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    CK(h, cudaGraphExecKernelNodeSetParams(h->graph, h->begin_node, &kp));
+    CK(h, cudaGraphLaunch(h->graph, h->s));
+    CK(h, cudaEventRecord(done, h->s));
+    return NHF_OK;
+}
+
+}  // namespace nhf
+
 extern "C" {
 
 const char *nhf_version(void) { return "nhflood-b200 0.1 (sm_100a)"; }

@@ -1,15 +1,19 @@
 """Batched form: many scenarios of uneven mesh size advanced together.
 
 Each scenario is a ``PlainRun`` (its own engine, clock, forcing, budget,
-extrema: the reference's per-run state, solver_compact.py:179-1008) on the
-fused tiled step; ``CudaEnsemble`` runs one batch of every scenario as one
-CUDA graph with ONE fused step launch per slot for all of them. A scenario
-that has reached its end time keeps taking part with a target equal to its
-clock, which the device clock turns into an empty batch (status DONE), so
-scenarios of different durations share the graph.
+extrema: the reference's per-run state, solver_compact.py:179-1008);
+``CudaEnsemble`` runs one batch of every scenario per call. A scenario that
+has reached its end time keeps taking part with a target equal to its clock,
+which the device clock turns into an empty batch (status DONE), so scenarios
+of different durations share a batch.
 
-The tile size and the grid schedule (persistent blocks or one block per
-tile) come from ``nhflood.autotune`` unless given.
+Two schedules. Member graphs (the default): every scenario's engine makes the
+plain form's own choice of step form, tile size and CFL placement, and all
+scenarios' batch graphs are launched together on their own streams, so small
+scenarios fill the GPU beside large ones. One launch: every scenario on the
+fused step with one tile size, ONE step launch per slot for all of them; its
+tile size and grid (persistent blocks or one block per tile) come from
+``nhflood.autotune`` unless given.
 """
 from __future__ import annotations
 
@@ -34,17 +38,38 @@ def tiled_factory(tile: int, device: str = 'cuda:0', cfl: str = 'pass'):
     return factory
 
 
+MEMBER_GRAPHS = -2  # nhf_ensemble_create's grid_blocks for the member-graph schedule
+
+
+def plain_factory(device: str = 'cuda:0'):
+    """Engines with the plain form's own step choice."""
+    def factory(arrays, params):
+        return CudaEngine(arrays, params, device=device)
+    return factory
+
+
 class EnsembleRun:
+    """With neither tile nor grid_blocks (or grid_blocks = -2) the member
+    graphs; otherwise the one-launch schedule, the autotuner filling in what
+    is not given."""
+
     def __init__(self, workloads, *, tile: int | None = None, grid_blocks: int | None = None,
                  batch_size: int = 32, device: str = 'cuda:0', tuning_cache=None):
         self.workloads = list(workloads)
-        if tile is None or grid_blocks is None:
-            from .autotune import choose_schedule
-            schedule = choose_schedule(self.workloads, batch_size=batch_size, device=device, cache=tuning_cache)
-            tile = schedule.tile if tile is None else tile
-            grid_blocks = schedule.grid if grid_blocks is None else grid_blocks
+        if grid_blocks == MEMBER_GRAPHS or (tile is None and grid_blocks is None):
+            self.schedule = 'member graphs'
+            tile, grid_blocks = None, MEMBER_GRAPHS
+            factory = plain_factory(device)
+        else:
+            self.schedule = 'one launch'
+            if tile is None or grid_blocks is None:
+                from .autotune import choose_schedule
+                tuned = choose_schedule(self.workloads, batch_size=batch_size, device=device, cache=tuning_cache)
+                tile = tuned.tile if tile is None else tile
+                grid_blocks = tuned.grid if grid_blocks is None else grid_blocks
+            factory = tiled_factory(tile, device)
         self.tile, self.grid_blocks = tile, grid_blocks
-        self.runs = [PlainRun(w, tiled_factory(tile, device), batch_size=batch_size) for w in self.workloads]
+        self.runs = [PlainRun(w, factory, batch_size=batch_size) for w in self.workloads]
         self.ensemble = CudaEnsemble([r.engine for r in self.runs], grid_blocks)
         self.cells = np.array([w.cells for w in self.workloads], np.int64)
         self.h2d_bytes = 0

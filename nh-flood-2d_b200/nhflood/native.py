@@ -402,11 +402,12 @@ class CudaEngine(Engine):
 
 
 class CudaEnsemble:
-    """Member CudaEngines advanced together (nhf_ensemble_*): one fused step
-    launch per slot for all members, each with its own clock and dt. The
-    members must be on the fused tiled step with one tile size. Batches are
-    ordered after the current torch stream and the members' creation
-    streams."""
+    """Member CudaEngines advanced together (nhf_ensemble_*), each with its
+    own clock and dt: with grid_blocks = -2 every member's own batch graph,
+    all launched together on their own streams; otherwise one fused step
+    launch per slot for all members, which must then be on the fused tiled
+    step with one tile size. Batches are ordered after the current torch
+    stream and the members' creation streams."""
 
     def __init__(self, engines, grid_blocks: int = 0):
         if not engines:

@@ -28,7 +28,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .ensemble import tiled_factory
+from .ensemble import MEMBER_GRAPHS, plain_factory, tiled_factory
 from .plain import PlainRun
 
 
@@ -95,7 +95,7 @@ class Completed:
 
 
 class FloodServer:
-    def __init__(self, *, hbm_budget: float = 150e9, tile: int = 256, grid_blocks: int = 0,
+    def __init__(self, *, hbm_budget: float = 150e9, tile: int = 256, grid_blocks: int = -2,
                  batch_size: int = 32, device: str = 'cuda:0', clock=None):
         import torch
         self.torch = torch
@@ -148,8 +148,11 @@ class FloodServer:
     def _build(self, req):
         """Builder thread: the solve's arrays, upload and plan on the side stream."""
         with self.torch.cuda.device(self.device), self.torch.cuda.stream(self.side):
-            run = PlainRun(req.workload, tiled_factory(self.tile, str(self.device)), batch_size=self.batch_size,
-                           arrays=req.arrays)
+            # member graphs (grid_blocks -2): the plain form's own step choice;
+            # one launch: the fused step with the server's tile size
+            factory = (plain_factory(str(self.device)) if self.grid_blocks == MEMBER_GRAPHS
+                       else tiled_factory(self.tile, str(self.device)))
+            run = PlainRun(req.workload, factory, batch_size=self.batch_size, arrays=req.arrays)
         self.side.synchronize()
         req.arrays = None  # the engine holds the device copy
         return run

@@ -38,13 +38,14 @@ def alone(w, tile):
     return np.concatenate(rows), state, budget
 
 
-@pytest.mark.parametrize('grid', [0, -1, 3])
+@pytest.mark.parametrize('grid', [0, -1, 3, -2])
 def test_members_match_their_single_runs(cuda_available, grid):
+    """grid -2: the member graphs, each member on its own plain engine."""
     from nhflood.ensemble import EnsembleRun
     ws = members()
     expected = [alone(w, 256) for w in ws]
-    ens = EnsembleRun(ws, tile=256, grid_blocks=grid)
-    assert ens.ensemble.members == 4 and ens.ensemble.tile == 256
+    ens = EnsembleRun(ws, tile=None if grid == -2 else 256, grid_blocks=grid)
+    assert ens.ensemble.members == 4 and ens.ensemble.tile == (0 if grid == -2 else 256)
     rows = [[] for _ in ws]
     batches = 0
     while not ens.done:
