@@ -190,7 +190,8 @@ def cpu_baseline(workload, seconds_budget=15.0, threads=None, start=None):
 
 def bench_batched(args, rank, world, local):
     """Batched form: 64 seeded quadtree scenarios (about 40M cells) in one
-    ensemble, one fused step launch per slot for all of them, against the
+    ensemble (by default every scenario's own batch graph, all launched
+    together; --tile / --grid select the one-launch schedule), against the
     same scenarios stepped one after another with the plain form."""
     import torch
     from nhflood.ensemble import EnsembleRun
