@@ -74,13 +74,13 @@ class HostClock:
         """Advance the host clock over completed rows of a batch trace."""
         if not self.pending:
             raise RuntimeError('Call begin before reading a trace')
-        for row in rows:
-            status = int(row[3])
-            if status == COMPLETED:
-                self.now_ticks = ticks_of(row[1], row[2])
-            elif status in (BAD_CFL, BAD_DT, OVERSHOOT, DONE):
-                break
-            else:
-                raise RuntimeError(f'Unknown clock trace status {status}')
+        # rows complete up to the first other status, which ends the batch
+        status = np.asarray(rows)[:, 3]
+        stops = np.flatnonzero(status != COMPLETED)
+        n = int(stops[0]) if len(stops) else len(rows)
+        if n < len(rows) and int(status[n]) not in (BAD_CFL, BAD_DT, OVERSHOOT, DONE):
+            raise RuntimeError(f'Unknown clock trace status {int(status[n])}')
+        if n:
+            self.now_ticks = ticks_of(rows[n - 1][1], rows[n - 1][2])
         self.pending = False
         return rows

@@ -94,15 +94,14 @@ class PlainRun:
     def finish(self, rows) -> int:
         """Consume a batch trace; returns completed steps."""
         self.clock.read_trace(rows)
-        completed = 0
-        for row in rows:
-            status = int(row[3])
-            if status == DONE:
-                break
-            if status != COMPLETED:
-                raise RuntimeError(f'Device clock status {status} at {self.elapsed}s')
-            self.elapsed = ticks_of(row[1], row[2]) / TICKS_PER_SECOND
-            completed += 1
+        status = rows[:, 3]
+        stops = np.flatnonzero(status != COMPLETED)
+        completed = int(stops[0]) if len(stops) else len(rows)
+        if completed:
+            last = rows[completed - 1]
+            self.elapsed = ticks_of(last[1], last[2]) / TICKS_PER_SECOND
+        if completed < len(rows) and int(status[completed]) != DONE:
+            raise RuntimeError(f'Device clock status {int(status[completed])} at {self.elapsed}s')
         self.steps += completed
         if abs(self.elapsed - self.next_output) < 1e-9 or self.elapsed == self.w.duration:
             self.next_output = min(self.next_output + self.w.yield_step, float(self.w.duration))
