@@ -80,7 +80,8 @@ def launches_per_batch(run) -> int:
     tiled = eng.path.startswith('tiled')
     pre = (1 if run.arrays.hang_cells else 0) + (0 if run.w.sita == 1.0 else 1)
     gate = run.arrays.gate
-    pre += 0 if gate is None else 2 + (1 if len(gate.flux_sides) else 0)
+    if gate is not None:  # bed motion at the start and the end; exchange volumes (with the end motion when fused)
+        pre += 2 + (0 if tiled or not len(gate.flux_sides) else 1)
     per_step = ((2 if 'cfl=pass' in eng.path else 1) if tiled else 6) + pre
     return (4 if tiled else 1) + run.params.batch_size * per_step
 

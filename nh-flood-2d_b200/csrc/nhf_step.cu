@@ -447,10 +447,32 @@ __device__ __forceinline__ float since_command(const GateDev &g, int gate, uint3
     return __uint2float_rn(high) / 256.0f + __uint2float_rn(low) * 0x1p-40f;
 }
 
-// check (gate.py:88-99) and move (gate.py:75-86), one block: at_end = 0 is
-// check_gates at the step start (irreversible command once the control cell
-// is wet above the trigger, from formal time 0 on, then the beds at now);
-// at_end = 1 is finish_gate_bed (the beds at the step end).
+// move (gate.py:75-86): the threads of one block set the working bed of
+// every commanded gate cell to its opening fraction at (hi, lo).
+__device__ __forceinline__ void gate_move_beds(const Dev &d, const GateDev &g, uint32_t hi, uint32_t lo)
+{
+    const nhf_mesh &m = d.m;
+    for (int slot = threadIdx.x; slot < g.n_targets; slot += blockDim.x) {
+        int cell = g.targets[slot];
+        int gate = g.cell_gate[cell];
+        if (g.commanded[gate] != 1) continue;
+        float fraction = minf(since_command(g, gate, hi, lo) / g.opening_seconds, 1.0f);
+        if (fraction >= 1.0f) {
+            m.bed[cell] = g.open_elevation;
+            if (atomicOr(&g.opened[gate], 1) == 0) {
+                g.opened_at[2 * gate] = hi; g.opened_at[2 * gate + 1] = lo;
+            }
+        } else {
+            float closed = g.closed[cell];
+            m.bed[cell] = closed + (g.open_elevation - closed) * fraction;
+        }
+    }
+}
+
+// check (gate.py:88-99) and move, one block: at_end = 0 is check_gates at
+// the step start (irreversible command once the control cell is wet above
+// the trigger, from formal time 0 on, then the beds at now); at_end = 1 is
+// finish_gate_bed (the beds at the step end).
 __global__ void __launch_bounds__(256) k_gate_move(Dev d, GateDev g, int at_end)
 {
     const nhf_mesh &m = d.m;
@@ -470,27 +492,15 @@ __global__ void __launch_bounds__(256) k_gate_move(Dev d, GateDev g, int at_end)
         }
         __syncthreads();
     }
-    for (int slot = threadIdx.x; slot < g.n_targets; slot += blockDim.x) {
-        int cell = g.targets[slot];
-        int gate = g.cell_gate[cell];
-        if (g.commanded[gate] != 1) continue;
-        float fraction = minf(since_command(g, gate, hi, lo) / g.opening_seconds, 1.0f);
-        if (fraction >= 1.0f) {
-            m.bed[cell] = g.open_elevation;
-            if (atomicOr(&g.opened[gate], 1) == 0) {
-                g.opened_at[2 * gate] = hi; g.opened_at[2 * gate + 1] = lo;
-            }
-        } else {
-            float closed = g.closed[cell];
-            m.bed[cell] = closed + (g.open_elevation - closed) * fraction;
-        }
-    }
+    gate_move_beds(d, g, hi, lo);
 }
 
 // record_flux (gate.py:118-140) on the post-limiter volume of each recorded
 // side, per 256 entries of the side list; the first nonzero gate-to-pond
 // volume latches the gate's first-flow time.
-__global__ void __launch_bounds__(kBlock) k_gate_flux(Dev d, GateDev g)
+// move_end (fused step): block 0 then also does finish_gate_bed, which the
+// volumes do not read.
+__global__ void __launch_bounds__(kBlock) k_gate_flux(Dev d, GateDev g, int move_end)
 {
     __shared__ double sh[kBlock];
     const nhf_mesh &m = d.m;
@@ -533,6 +543,7 @@ __global__ void __launch_bounds__(kBlock) k_gate_flux(Dev d, GateDev g)
             acc_add(g.acc_sum + idx, g.acc_comp + idx, sum);
         }
     }
+    if (move_end && blockIdx.x == 0) gate_move_beds(d, g, c->step_end[0], c->step_end[1]);
 }
 
 // --------------------------------------------------------------------- CFL
@@ -770,7 +781,7 @@ void enqueue_step(nhf_handle *h)
     k_donor<<<grid_for(m.e_num - 1, 256), 256, 0, s>>>(d);
     k_scale<<<gs, 256, 0, s>>>(d);
     if (h->gate_on) {
-        if (h->gate.n_flux > 0) k_gate_flux<<<grid_for(h->gate.n_flux, kBlock), kBlock, 0, s>>>(d, h->gate);
+        if (h->gate.n_flux > 0) k_gate_flux<<<grid_for(h->gate.n_flux, kBlock), kBlock, 0, s>>>(d, h->gate, 0);
         k_cells<true><<<d.blocks, kBlock, 0, s>>>(d, h->gate);
         k_gate_move<<<1, 256, 0, s>>>(d, h->gate, 1);
     } else {
@@ -794,9 +805,11 @@ int build_graph(nhf_handle *h)
                 // volumes, finish_gate_bed, then the CFL pass
                 k_gate_move<<<1, 256, 0, h->s>>>(h->dev, h->gate, 0);
                 tiled_enqueue_step(h->dev, h->tb, h->s, &h->gate);
+                // the exchange volumes and finish_gate_bed in one launch
                 if (h->gate.n_flux > 0)
-                    k_gate_flux<<<grid_for(h->gate.n_flux, kBlock), kBlock, 0, h->s>>>(h->dev, h->gate);
-                k_gate_move<<<1, 256, 0, h->s>>>(h->dev, h->gate, 1);
+                    k_gate_flux<<<grid_for(h->gate.n_flux, kBlock), kBlock, 0, h->s>>>(h->dev, h->gate, 1);
+                else
+                    k_gate_move<<<1, 256, 0, h->s>>>(h->dev, h->gate, 1);
                 tiled_enqueue_cfl(h->dev, h->tb, h->s);
             } else {
                 tiled_enqueue_step(h->dev, h->tb, h->s);
