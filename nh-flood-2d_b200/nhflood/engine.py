@@ -29,7 +29,7 @@ from .model import MIN_DT, StepParams, build_step_arrays
 from .output import (append_station_samples, read_checkpoint, resolve_station_cells, write_bed,
                      write_checkpoint, write_depth_frame, write_extrema)
 from .preprocess import load_mesh
-from .run_record import WaterBudget
+from .run_record import WaterBudget, finite_totals
 
 CHECKPOINT_INTERVAL_S = 30 * 60
 FRAME_INTERVAL_S = 900
@@ -242,7 +242,7 @@ def _run(domain_cfg, record, end_time, mesh, geometry, forcing, arrays, engine, 
         nonlocal device_totals
         date = domain_cfg.start + timedelta(seconds=seconds)
         s.outputs += 1
-        device_totals = device_totals + engine.budget_flush()
+        device_totals = device_totals + finite_totals(engine.budget_flush())
         budget.set_device_terms(device_totals)
         depth_np = engine.get('depth')
         storage = float(np.sum(depth_np.astype(float) * area_f64, dtype=np.float64))

@@ -27,6 +27,7 @@ from pathlib import Path
 import numpy as np
 
 from .clock import seconds_to_ticks
+from .run_record import finite_totals
 
 FIRST_FLOW_DEFINITION = ('End of first completed step with nonzero post-limiter gate-to-pond subedge volume '
                          'in either direction')
@@ -221,7 +222,7 @@ class GateController:
     def pull(self, engine) -> None:
         """Fold the device's interval totals into the cumulative ones and copy
         the controller words back."""
-        self.totals = self.totals + engine.gate_flush()
+        self.totals = self.totals + finite_totals(engine.gate_flush())
         self.state = engine.gate_state()
 
     def initialize_inventory(self, depth, area) -> None:

@@ -111,6 +111,16 @@ class RunRecord:
         self.write()
 
 
+def finite_totals(totals):
+    """DeviceBudget.flush's check (device_budget.py:71-73): an infinite or NaN
+    F32 term in any step poisons the interval's FP64 totals, and the run
+    stops with the reference's error."""
+    totals = np.asarray(totals)
+    if not np.all(np.isfinite(totals)):
+        raise FloatingPointError('Nonfinite F32 device budget diagnostic')
+    return totals
+
+
 class WaterBudget:
     """mass_balance.csv rows from device terms and host F64 forcing totals."""
 

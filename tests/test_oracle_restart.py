@@ -108,3 +108,25 @@ def test_adopted_state_continues_like_the_original_run():
         b.finish(rb)
     for name in ('depth', 'q', 'max_depth', 'peak_hi', 'peak_lo'):
         np.testing.assert_array_equal(a.engine.get(name), b.engine.get(name))
+
+
+def test_nonfinite_budget_term_stops_the_run(tmp_path):
+    """device_budget.py:71-73: a non-finite F32 budget term raises at the next
+    output's flush (here an engine whose flush reports NaN)."""
+    from runner import oracle_factory
+
+    def poisoned(arrays, params):
+        engine = oracle_factory(arrays, params)
+        clean = engine.budget_flush
+
+        def flush():
+            totals = clean()
+            totals[0] = float('nan')
+            return totals
+        engine.budget_flush = flush
+        return engine
+
+    src = tmp_path / 'inputs'
+    rain = inputs(src)
+    with pytest.raises(FloatingPointError, match='Nonfinite F32 device budget diagnostic'):
+        solve(src, rain, tmp_path / 'run', 5, engine=poisoned)
