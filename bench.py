@@ -74,16 +74,21 @@ def launches_per_batch(run) -> int:
     """Kernels one batch graph of a plain run launches: begin (+ rain-time
     copy, state copy-back and velocity on the fused step), and per step the
     fused step (+ its CFL pass on split plans) or the six multi-pass kernels,
-    the hanging-edge and theta pre-passes, and the gate controller's bed
-    motion (twice) and exchange volumes."""
+    the hanging-edge and theta pre-passes, and the gate controller's
+    passes."""
     eng = run.engine
     tiled = eng.path.startswith('tiled')
     pre = (1 if run.arrays.hang_cells else 0) + (0 if run.w.sita == 1.0 else 1)
     gate = run.arrays.gate
-    if gate is not None:  # bed motion at the start and the end; exchange volumes (with the end motion when fused)
-        pre += 2 + (0 if tiled or not len(gate.flux_sides) else 1)
+    once = 0
+    if gate is not None:
+        if tiled:  # exchange volumes with the end motion; start motion in the CFL pass (own launch at batch start)
+            pre += 1
+            once += 1
+        else:  # bed motion at the start and the end, exchange volumes
+            pre += 2 + (1 if len(gate.flux_sides) else 0)
     per_step = ((2 if 'cfl=pass' in eng.path else 1) if tiled else 6) + pre
-    return (4 if tiled else 1) + run.params.batch_size * per_step
+    return (4 if tiled else 1) + once + run.params.batch_size * per_step
 
 
 def combine_ranks(times, units, device, world):

@@ -265,6 +265,54 @@ __device__ __forceinline__ float boundary_neighbor_sum(float q, float left, floa
     return result;
 }
 
+// since_command (gate.py:68-73): the command's clock age in F32 seconds.
+__device__ __forceinline__ float since_command(const GateDev &g, int gate, uint32_t hi, uint32_t lo)
+{
+    uint32_t borrow = lo < g.command[2 * gate + 1] ? 1u : 0u;
+    uint32_t high = hi - g.command[2 * gate] - borrow;
+    uint32_t low = lo - g.command[2 * gate + 1];
+    return __uint2float_rn(high) / 256.0f + __uint2float_rn(low) * 0x1p-40f;
+}
+
+// move (gate.py:75-86): the threads of one block set the working bed of
+// every commanded gate cell to its opening fraction at (hi, lo).
+__device__ __forceinline__ void gate_move_beds(const Dev &d, const GateDev &g, uint32_t hi, uint32_t lo)
+{
+    const nhf_mesh &m = d.m;
+    for (int slot = threadIdx.x; slot < g.n_targets; slot += blockDim.x) {
+        int cell = g.targets[slot];
+        int gate = g.cell_gate[cell];
+        if (g.commanded[gate] != 1) continue;
+        float fraction = minf(since_command(g, gate, hi, lo) / g.opening_seconds, 1.0f);
+        if (fraction >= 1.0f) {
+            m.bed[cell] = g.open_elevation;
+            if (atomicOr(&g.opened[gate], 1) == 0) {
+                g.opened_at[2 * gate] = hi; g.opened_at[2 * gate + 1] = lo;
+            }
+        } else {
+            float closed = g.closed[cell];
+            m.bed[cell] = closed + (g.open_elevation - closed) * fraction;
+        }
+    }
+}
+
+// check (gate.py:88-99), the threads of one block over the gates: from
+// formal time 0 on, an irreversible command once the control cell is wet
+// and its level is strictly above the trigger.
+__device__ __forceinline__ void gate_check(const Dev &d, const GateDev &g, uint32_t hi, uint32_t lo)
+{
+    const nhf_mesh &m = d.m;
+    const float *depth = cur_depth(d, d.ctl->parity);
+    const bool formal = hi > g.formal_hi || (hi == g.formal_hi && lo >= g.formal_lo);
+    for (int gate = threadIdx.x; formal && gate < g.count; gate += blockDim.x) {
+        int cell = g.controls[gate];
+        if (g.commanded[gate] == 0 && depth[cell] >= d.min_h && m.bed[cell] + depth[cell] > g.trigger_level) {
+            g.commanded[gate] = 1;
+            g.command[2 * gate] = hi; g.command[2 * gate + 1] = lo;
+        }
+    }
+}
+
 // ---------------------------------------------------------------- host side
 
 struct TiledBuild {
@@ -287,8 +335,9 @@ int tiled_build(const nhf_mesh &m, cudaStream_t s, TiledBuild *out, char *why, s
 // only the pre-passes and the gate-enabled step: the caller then enqueues
 // the controller's passes and tiled_enqueue_cfl.
 void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s, const GateDev *gate = nullptr);
-// The separate CFL pass of a split plan (nothing otherwise).
-void tiled_enqueue_cfl(const Dev &d, const TiledBuild &b, cudaStream_t s);
+// The separate CFL pass of a split plan (nothing otherwise); with a gate
+// controller its last block also runs the next step's check_gates.
+void tiled_enqueue_cfl(const Dev &d, const TiledBuild &b, cudaStream_t s, const GateDev *gate = nullptr);
 // Enqueue the batch epilogue: bring the state back into the caller's
 // buffers and refresh u, v.
 void tiled_enqueue_batch_end(const Dev &d, cudaStream_t s);

@@ -438,58 +438,18 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d, GateDev g)
 
 // ------------------------------------------------------------ gate control
 
-// since_command (gate.py:68-73): the command's clock age in F32 seconds.
-__device__ __forceinline__ float since_command(const GateDev &g, int gate, uint32_t hi, uint32_t lo)
-{
-    uint32_t borrow = lo < g.command[2 * gate + 1] ? 1u : 0u;
-    uint32_t high = hi - g.command[2 * gate] - borrow;
-    uint32_t low = lo - g.command[2 * gate + 1];
-    return __uint2float_rn(high) / 256.0f + __uint2float_rn(low) * 0x1p-40f;
-}
-
-// move (gate.py:75-86): the threads of one block set the working bed of
-// every commanded gate cell to its opening fraction at (hi, lo).
-__device__ __forceinline__ void gate_move_beds(const Dev &d, const GateDev &g, uint32_t hi, uint32_t lo)
-{
-    const nhf_mesh &m = d.m;
-    for (int slot = threadIdx.x; slot < g.n_targets; slot += blockDim.x) {
-        int cell = g.targets[slot];
-        int gate = g.cell_gate[cell];
-        if (g.commanded[gate] != 1) continue;
-        float fraction = minf(since_command(g, gate, hi, lo) / g.opening_seconds, 1.0f);
-        if (fraction >= 1.0f) {
-            m.bed[cell] = g.open_elevation;
-            if (atomicOr(&g.opened[gate], 1) == 0) {
-                g.opened_at[2 * gate] = hi; g.opened_at[2 * gate + 1] = lo;
-            }
-        } else {
-            float closed = g.closed[cell];
-            m.bed[cell] = closed + (g.open_elevation - closed) * fraction;
-        }
-    }
-}
-
 // check (gate.py:88-99) and move, one block: at_end = 0 is check_gates at
 // the step start (irreversible command once the control cell is wet above
 // the trigger, from formal time 0 on, then the beds at now); at_end = 1 is
 // finish_gate_bed (the beds at the step end).
 __global__ void __launch_bounds__(256) k_gate_move(Dev d, GateDev g, int at_end)
 {
-    const nhf_mesh &m = d.m;
     const Ctl *c = d.ctl;
     if (!c->active) return;
     const uint32_t hi = at_end ? c->step_end[0] : c->now[0];
     const uint32_t lo = at_end ? c->step_end[1] : c->now[1];
     if (!at_end) {
-        const float *depth = cur_depth(d, c->parity);
-        const bool formal = hi > g.formal_hi || (hi == g.formal_hi && lo >= g.formal_lo);
-        for (int gate = threadIdx.x; formal && gate < g.count; gate += blockDim.x) {
-            int cell = g.controls[gate];
-            if (g.commanded[gate] == 0 && depth[cell] >= d.min_h && m.bed[cell] + depth[cell] > g.trigger_level) {
-                g.commanded[gate] = 1;
-                g.command[2 * gate] = hi; g.command[2 * gate + 1] = lo;
-            }
-        }
+        gate_check(d, g, hi, lo);
         __syncthreads();
     }
     gate_move_beds(d, g, hi, lo);
@@ -801,16 +761,17 @@ int build_graph(nhf_handle *h)
         tiled_enqueue_batch_start(h->dev, h->s);
         for (int i = 0; i < h->p.batch_size; ++i) {
             if (h->gate_on) {
-                // check_gates, the step with the source terms, the exchange
-                // volumes, finish_gate_bed, then the CFL pass
-                k_gate_move<<<1, 256, 0, h->s>>>(h->dev, h->gate, 0);
+                // check_gates (here for the batch's first step; the CFL pass
+                // runs it for the next ones), the step with the source terms,
+                // the exchange volumes with finish_gate_bed, the CFL pass
+                if (i == 0) k_gate_move<<<1, 256, 0, h->s>>>(h->dev, h->gate, 0);
                 tiled_enqueue_step(h->dev, h->tb, h->s, &h->gate);
                 // the exchange volumes and finish_gate_bed in one launch
                 if (h->gate.n_flux > 0)
                     k_gate_flux<<<grid_for(h->gate.n_flux, kBlock), kBlock, 0, h->s>>>(h->dev, h->gate, 1);
                 else
                     k_gate_move<<<1, 256, 0, h->s>>>(h->dev, h->gate, 1);
-                tiled_enqueue_cfl(h->dev, h->tb, h->s);
+                tiled_enqueue_cfl(h->dev, h->tb, h->s, &h->gate);
             } else {
                 tiled_enqueue_step(h->dev, h->tb, h->s);
             }

@@ -734,10 +734,12 @@ __device__ __forceinline__ void step_tile(const Dev &d, const int t_index, const
 // key (cfl bits, side id) and the last of `blocks` blocks sets ndt /
 // cfl_arg (the lowest side id attains the minimum) and prepares the next
 // step (solver_compact.py:364-382).
-__device__ __forceinline__ void cfl_pass(const Dev &d, int first, int end, int stride, unsigned blocks)
+__device__ __forceinline__ void cfl_pass(const Dev &d, int first, int end, int stride, unsigned blocks,
+                                         const GateDev *gd = nullptr)
 {
     __shared__ unsigned long long sh[32];
     __shared__ bool last;
+    __shared__ int prepared;
     const nhf_mesh &m = d.m;
     Ctl *c = d.ctl;
     const int active = c->active;
@@ -772,20 +774,32 @@ __device__ __forceinline__ void cfl_pass(const Dev &d, int first, int end, int s
         }
     }
     __syncthreads();
-    if (!last || threadIdx.x != 0) return;
-    __threadfence();
-    const unsigned long long packed = atomicExch(&c->cfl_packed, kCflEmpty);
-    c->done_blocks = 0;
-    if (active) {
-        if (packed == kCflEmpty) {
-            c->ndt = __uint_as_float(0x7f800000u);
-            c->cfl_arg = 0;
-        } else {
-            c->ndt = __uint_as_float((uint32_t)(packed >> 32));
-            c->cfl_arg = (int32_t)(packed & 0xffffffffu);
+    if (!last) return;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned long long packed = atomicExch(&c->cfl_packed, kCflEmpty);
+        c->done_blocks = 0;
+        if (active) {
+            if (packed == kCflEmpty) {
+                c->ndt = __uint_as_float(0x7f800000u);
+                c->cfl_arg = 0;
+            } else {
+                c->ndt = __uint_as_float((uint32_t)(packed >> 32));
+                c->cfl_arg = (int32_t)(packed & 0xffffffffu);
+            }
         }
+        prepared = c->slot < d.batch_size;
+        if (prepared) prepare_step(d, c, depth, q);
     }
-    if (c->slot < d.batch_size) prepare_step(d, c, depth, q);
+    if (!gd) return;
+    // gate runs: the next step's check_gates (trigger check and beds at its
+    // start) by this block, once that step is prepared in this batch
+    __syncthreads();
+    if (!prepared || !c->active) return;
+    const uint32_t hi = c->now[0], lo = c->now[1];
+    gate_check(d, *gd, hi, lo);
+    __syncthreads();
+    gate_move_beds(d, *gd, hi, lo);
 }
 
 template <bool kThetaOne, bool kHanging, int NT, int CPT>
@@ -810,6 +824,12 @@ __global__ void __launch_bounds__(256) k_cfl_tiled(const __grid_constant__ Dev d
 {
     if (!d.plan.split) return;
     cfl_pass(d, 1 + (int)(blockIdx.x * blockDim.x), d.m.s_num, (int)(gridDim.x * blockDim.x), gridDim.x);
+}
+
+// CFL pass of a gate run (split plan): also the next step's check_gates.
+__global__ void __launch_bounds__(256) k_cfl_tiled_gate(const __grid_constant__ Dev d, const __grid_constant__ GateDev g)
+{
+    cfl_pass(d, 1 + (int)(blockIdx.x * blockDim.x), d.m.s_num, (int)(gridDim.x * blockDim.x), gridDim.x, &g);
 }
 
 // Ensemble step: one launch advances every member mesh by one of its own
@@ -1493,12 +1513,13 @@ void tiled_enqueue_step(const Dev &d, const TiledBuild &b, cudaStream_t s, const
     tiled_enqueue_cfl(d, b, s);
 }
 
-void tiled_enqueue_cfl(const Dev &d, const TiledBuild &b, cudaStream_t s)
+void tiled_enqueue_cfl(const Dev &d, const TiledBuild &b, cudaStream_t s, const GateDev *gate)
 {
     if (b.plan.split) {
         int gc = (d.m.s_num + 255) / 256;
         if (gc > 148 * 8) gc = 148 * 8;
-        k_cfl_tiled<<<gc, 256, 0, s>>>(d);
+        if (gate) k_cfl_tiled_gate<<<gc, 256, 0, s>>>(d, *gate);
+        else k_cfl_tiled<<<gc, 256, 0, s>>>(d);
     }
 }
 

@@ -23,8 +23,9 @@ def fake_run(path, *, hang=0, sita=1.0, gate_flux=None, batch=32):
     ('tiled(tile=256,patterns=4159,smem=32852,cfl=pass)', 0, 0.7, None, 4 + 32 * (2 + 1)),
     ('multipass', 0, 1.0, None, 1 + 32 * 6),
     ('multipass', 5, 0.7, None, 1 + 32 * (6 + 2)),
-    # gate runs: bed motion at the start, exchange volumes with the end motion (fused) ...
-    ('tiled(tile=256,patterns=124,smem=28168,cfl=pass)', 0, 1.0, 2400, 4 + 32 * (2 + 2)),
+    # gate runs: exchange volumes with the end motion, the start motion in the
+    # CFL pass and once at the batch start (fused) ...
+    ('tiled(tile=256,patterns=124,smem=28168,cfl=pass)', 0, 1.0, 2400, 4 + 1 + 32 * (2 + 1)),
     # ... or bed motion, exchange volumes, bed motion (multi-pass)
     ('multipass', 0, 1.0, 2400, 1 + 32 * (6 + 3)),
     ('multipass', 0, 1.0, 0, 1 + 32 * (6 + 2)),
