@@ -1,4 +1,6 @@
-"""Autotuner for the fused step's tile size and grid schedule.
+"""Autotuner for the one-launch ensemble schedule: the fused step's tile
+size and grid (the member-graph schedule, the default, needs no tuning:
+each member keeps the plain form's own choice).
 
 Candidates: tile sizes 256, 512 and 1024 cells (256- or 512-thread blocks)
 crossed with two grid schedules of the step kernel: persistent (resident
