@@ -44,3 +44,26 @@ def test_algorithmic_bytes_by_workload_kind():
     q = workloads.multires_quadtree(width=2000.0)
     s_over_n = (q.mesh.s_num - 1) / q.cells
     assert bench.algorithmic_bytes(q) == pytest.approx(52 + 4 + 28 + 12 * s_over_n + 20)
+
+
+def test_source_hash_is_relocatable_and_ignores_non_sources(tmp_path):
+    """The run record's source identity (the reference's test_run_record.py
+    property): sorted relative paths, lengths and bytes of the sources only,
+    the same after a copy, changed by a rename or an edit."""
+    import shutil
+    from nhflood.run_record import source_tree_sha256
+    src = tmp_path / 'src'
+    (src / 'pkg').mkdir(parents=True)
+    (src / 'pkg' / 'z.py').write_bytes(b'z=1\n')
+    (src / 'a.cu').write_bytes(b'// a\n')
+    (src / 'notes.txt').write_text('irrelevant')
+    first = source_tree_sha256(src)
+    copied = tmp_path / 'copy'
+    shutil.copytree(src, copied)
+    assert source_tree_sha256(copied) == first
+    (copied / 'notes.txt').write_text('changed')
+    assert source_tree_sha256(copied) == first
+    (copied / 'a.cu').rename(copied / 'b.cu')
+    assert source_tree_sha256(copied) != first
+    (src / 'pkg' / 'z.py').write_bytes(b'z=2\n')
+    assert source_tree_sha256(src) != first

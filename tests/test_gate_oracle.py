@@ -459,3 +459,30 @@ def test_formal_30000s_command_and_f32_opening_age(tmp_path, opening_seconds):
     assert report['first_fully_open_sample_seconds'] == 30000. + opening_seconds
     assert report['command_clock_ticks'] == words(seconds_to_ticks(30000.)).tolist()
     eng.close()
+
+
+def test_disabled_and_never_triggered_gates_leave_the_step_bitwise_unchanged(tmp_path):
+    """tests/test_gate_compatibility.py's invariant: the controller changes
+    nothing of the hydraulics until a gate is commanded; a disabled block, an
+    enabled block whose trigger is never reached, and no gate block give
+    identical states and traces."""
+    import json as _json
+    from nhflood.input import ForceConfig
+    results = {}
+    for name, gate in (('none', None), ('disabled', dict(enabled=False)), ('idle', dict(trigger_level=1000.))):
+        dc, force, *_ = setup(tmp_path / name, depth=[2, 2, 1], rain=50, gate=gate or {})
+        if gate is None:
+            force = ForceConfig(boundaries=force.boundaries, rainfall=force.rainfall, gate=None)
+            seed = read_checkpoint(dc.restart_state)
+            meta = _json.loads(seed.metadata_json)
+            meta['gate_config'] = 'null'
+            seed.metadata_json = _json.dumps(meta)
+            write_checkpoint(dc.restart_state, **vars(seed))
+        results[name] = run(dc, force, 3)
+    base = results['none']
+    for name in ('disabled', 'idle'):
+        r = results[name]
+        np.testing.assert_array_equal(base.trace, r.trace)
+        for field in ('depth', 'bed', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_speed'):
+            assert getattr(base.state, field).tobytes() == getattr(r.state, field).tobytes(), (name, field)
+    assert gate_of(results['idle'])['command_seconds'] is None
