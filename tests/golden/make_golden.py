@@ -1,0 +1,405 @@
+"""Generate golden vectors for the host-side inputs of the step by running
+the reference's own NumPy/pydantic code.
+
+Three parts of nh-flood-2d run without Taichi, rasterio or fastdb4py:
+  * preprocess/hydraulics.py – map_land_parameters (side Manning n, cell
+    Horton parameters), open_boundary_face_fractions (θ < 1 boundary faces),
+    connected_still_water (the warm-up fill);
+  * preprocess/gate.py – GateLayout.load (gate components, control cells,
+    validation);
+  * input/domain.py, input/force.py – the config schema and absolute_time.
+This script imports those modules unchanged from a reference checkout,
+feeds them seeded synthetic meshes and configs, and writes what they return
+(or the error they raise) to host_golden.json and host_golden.npz next to
+it. tests/test_golden_host.py replays every case through nhflood.
+
+    python tests/golden/make_golden.py [--reference PATH]
+
+The reference's preprocess/__init__.py imports its Taichi domain pass, so
+the package object is registered without running that file; the two
+modules themselves are imported as they are. The meshes are 2:1 quadtrees
+built here (a 2 m base grid with random cells split into four 1 m cells).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import sys
+import types
+from collections import defaultdict
+from pathlib import Path
+from types import SimpleNamespace as NS
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+
+def load_reference(root: Path):
+    src = root / 'src'
+    sys.path.insert(0, str(src))
+    importlib.import_module('nh_flood_2d')
+    package = types.ModuleType('nh_flood_2d.preprocess')
+    package.__path__ = [str(src / 'nh_flood_2d' / 'preprocess')]
+    sys.modules['nh_flood_2d.preprocess'] = package
+    return NS(hydraulics=importlib.import_module('nh_flood_2d.preprocess.hydraulics'),
+              gate=importlib.import_module('nh_flood_2d.preprocess.gate'),
+              input=importlib.import_module('nh_flood_2d.input'),
+              force=importlib.import_module('nh_flood_2d.input.force'))
+
+
+# ---------------------------------------------------------------- meshes
+
+def quadtree(rng, nx, ny, split_fraction):
+    """Cells (x0, x1, y0, y1) of a 2 m grid with some cells split in four;
+    sides split at every neighbour corner; face CSR per direction
+    (0 west, 1 east, 2 south, 3 north)."""
+    cells = []
+    for j in range(ny):
+        for i in range(nx):
+            x0, y0 = 2 * i, 2 * j
+            if rng.random() < split_fraction:
+                cells += [(x0 + a, x0 + a + 1, y0 + b, y0 + b + 1) for b in (0, 1) for a in (0, 1)]
+            else:
+                cells.append((x0, x0 + 2, y0, y0 + 2))
+    breaks = {1: defaultdict(set), 2: defaultdict(set)}
+    for x0, x1, y0, y1 in cells:
+        breaks[2][x0].update((y0, y1)); breaks[2][x1].update((y0, y1))
+        breaks[1][y0].update((x0, x1)); breaks[1][y1].update((x0, x1))
+    owner = defaultdict(dict)
+    faces = []
+    for cell, (x0, x1, y0, y1) in enumerate(cells, 1):
+        per = []
+        for orient, coord, a, b, role in ((2, x0, y0, y1, 'hi'), (2, x1, y0, y1, 'lo'),
+                                          (1, y0, x0, x1, 'hi'), (1, y1, x0, x1, 'lo')):
+            points = sorted(p for p in breaks[orient][coord] if a <= p <= b)
+            keys = [(orient, coord, u, w) for u, w in zip(points, points[1:])]
+            for key in keys:
+                owner[key][role] = cell
+            per.append(keys)
+        faces.append(per)
+    side_id = {key: i for i, key in enumerate(sorted(owner), 1)}
+    topology = np.zeros((len(side_id) + 1, 3), dtype=np.int32)
+    length = np.zeros(len(side_id) + 1, dtype=np.float32)
+    for key, i in side_id.items():
+        orient, _, u, w = key
+        topology[i] = (orient, owner[key].get('lo', 0), owner[key].get('hi', 0))
+        length[i] = w - u
+    n = len(cells) + 1
+    face_ptr = np.zeros((n, 4), dtype=np.int32)
+    face_count = np.zeros((n, 4), dtype=np.int32)
+    flat = []
+    for cell, per in enumerate(faces, 1):
+        for d, keys in enumerate(per):
+            face_ptr[cell, d] = len(flat)
+            face_count[cell, d] = len(keys)
+            flat += [side_id[k] for k in keys]
+    bounds = np.zeros((n, 4), dtype=np.float64)
+    bounds[1:] = [(x0, y0, x1, y1) for x0, x1, y0, y1 in cells]
+    area = np.zeros(n, dtype=np.float64)
+    area[1:] = (bounds[1:, 2] - bounds[1:, 0]) * (bounds[1:, 3] - bounds[1:, 1])
+    return dict(topology=topology, length=length, face_ptr=face_ptr, face_count=face_count,
+                flat=np.array(flat, dtype=np.int32), bounds=bounds, area=area)
+
+
+def exterior_cells(mesh, side):
+    """Cells on one outer edge ('west', 'east', 'south', 'north'), id order."""
+    b = mesh['bounds']
+    column = {'west': 0, 'south': 1, 'east': 2, 'north': 3}[side]
+    value = b[1:, column].min() if side in ('west', 'south') else b[1:, column].max()
+    cells = np.flatnonzero(b[:, column] == value)
+    return cells[cells != 0].astype(np.int64)
+
+
+def smooth_bed(rng, mesh, relief):
+    centre_x = (mesh['bounds'][:, 0] + mesh['bounds'][:, 2]) / 2
+    centre_y = (mesh['bounds'][:, 1] + mesh['bounds'][:, 3]) / 2
+    bed = np.zeros(len(centre_x))
+    for _ in range(4):
+        kx, ky, phase = rng.uniform(.05, .4), rng.uniform(.05, .4), rng.uniform(0, 2 * np.pi)
+        bed += rng.uniform(.2, 1) * np.sin(kx * centre_x + ky * centre_y + phase)
+    bed = relief * bed / np.abs(bed).max() + rng.normal(0, relief / 20, bed.shape)
+    bed[0] = 0
+    return bed.astype(np.float32)
+
+
+# ---------------------------------------------------------------- cases
+
+def decimal(rng, low, high, digits):
+    return float(round(rng.uniform(low, high), digits))
+
+
+def land_cases(ref, rng, mesh, arrays):
+    out = []
+    n = len(mesh['bounds'])
+    for case in range(8):
+        classes = sorted(rng.choice([0, 1, 3, 7, 10, 11, 42, 200, 255], size=rng.integers(1, 6), replace=False))
+        types_ = rng.choice(classes, size=n).astype(np.uint8)
+        table = {}
+        for c in classes:
+            if case == 7 and c == classes[-1]:
+                continue  # a class without parameters: rejected
+            if rng.random() < .5:
+                f0 = decimal(rng, 0, 120, 3)
+                table[str(int(c))] = dict(manning_n=decimal(rng, 0, .2, 5), infiltration=dict(
+                    f0_mm_h=f0, fc_mm_h=decimal(rng, 0, f0, 3), k_per_h=decimal(rng, 0, 8, 4)))
+            else:
+                table[str(int(c))] = dict(manning_n=decimal(rng, 0, .2, 5), infiltration='none')
+        parsed = {int(k): ref.input.domain.LandParameters.model_validate(v) for k, v in table.items()}
+        arrays[f'land{case}_types'] = types_
+        try:
+            side_n, f0, fc, k = ref.hydraulics.map_land_parameters(parsed, types_, mesh['topology'])
+        except ValueError as error:
+            out.append(dict(table=table, error=str(error)))
+            continue
+        for name, value in (('side_n', side_n), ('f0', f0), ('fc', fc), ('k', k)):
+            arrays[f'land{case}_{name}'] = value
+        out.append(dict(table=table, error=None))
+    return out
+
+
+def face_fraction_cases(ref, rng, mesh, arrays):
+    topology = mesh['topology']
+    exterior = np.flatnonzero(((topology[:, 1] == 0) ^ (topology[:, 2] == 0)))
+    out = []
+    for case in range(4):
+        selected = np.zeros(len(topology), dtype=bool)
+        selected[rng.choice(exterior, size=max(1, int(len(exterior) * (case + 1) / 6)), replace=False)] = True
+        result = ref.hydraulics.open_boundary_face_fractions(selected, mesh['length'], topology, mesh['face_ptr'],
+                                                             mesh['face_count'], mesh['flat'])
+        arrays[f'faces{case}_selected'] = selected
+        arrays[f'faces{case}_result'] = result
+        out.append(case)
+    return out
+
+
+def level_boundary(name, cells, level):
+    return NS(name=name, kind='level', cells=np.asarray(cells, dtype=np.int64), series=NS(at=lambda t, v=level: v))
+
+
+def still_water_cases(ref, rng, mesh, arrays):
+    topology = mesh['topology']
+    out = []
+    for case in range(16):
+        bed = smooth_bed(rng, mesh, relief=3.0)
+        crest = np.full(len(topology), -999.0, dtype=np.float32)
+        ridge = rng.choice(len(topology), size=len(topology) // 12, replace=False)
+        crest[ridge] = rng.uniform(-1, 4, ridge.size).astype(np.float32)
+        closed = (rng.random(len(topology)) < .04).astype(np.uint8)
+        edges = rng.permutation(['west', 'east', 'south', 'north'])[:1 if case % 2 else rng.integers(2, 5)]
+        specs = []
+        for i, edge in enumerate(edges):
+            cells = exterior_cells(mesh, edge)
+            cells = cells[rng.random(cells.size) < .6] if cells.size > 2 else cells
+            # shared decimal levels make one body per level; a level that is
+            # not an F32 value checks the F64 comparison
+            level = [0.5, 0.5, 1.1, -0.3][i] if case % 3 == 0 else decimal(rng, -1.5, 2.5, 2)
+            specs.append(dict(name=f'{edge}_{i}', kind='level', cells=cells.tolist(), level=level))
+        if case % 4 == 1:
+            specs.append(dict(name='inflow', kind='discharge', cells=exterior_cells(mesh, 'north').tolist(),
+                              level=9.0))
+        boundaries = [level_boundary(s['name'], s['cells'], s['level']) if s['kind'] == 'level'
+                      else NS(name=s['name'], kind='discharge', cells=np.asarray(s['cells']),
+                              series=NS(at=lambda t: 9.0)) for s in specs]
+        arrays[f'still{case}_bed'] = bed
+        arrays[f'still{case}_crest'] = crest
+        arrays[f'still{case}_closed'] = closed
+        try:
+            depth, meta = ref.hydraulics.connected_still_water(bed, crest, closed, topology, boundaries, mesh['area'])
+        except ValueError as error:
+            out.append(dict(boundaries=specs, error=str(error)))
+            continue
+        arrays[f'still{case}_depth'] = depth
+        out.append(dict(boundaries=specs, error=None, meta=meta))
+    return out
+
+
+def gate_mesh(rng):
+    """A 2 m grid, 14 x 6: river (1) west of x = 10, pond (11) east of it, two
+    gate strips (10) in the column x = 10-12 and one gate cell at (9, 7)."""
+    mesh = quadtree(rng, 14, 6, 0.0)
+    centre_x = (mesh['bounds'][:, 0] + mesh['bounds'][:, 2]) / 2
+    centre_y = (mesh['bounds'][:, 1] + mesh['bounds'][:, 3]) / 2
+    types_ = np.where(centre_x < 10, 1, 11).astype(np.uint8)
+    # the lower and upper strip, with a pond cell between them, and the gate cell at (9, 7)
+    types_[(centre_x > 10) & (centre_x < 12) & (centre_y < 6)] = 10
+    types_[(centre_x > 10) & (centre_x < 12) & (centre_y > 8)] = 10
+    types_[(centre_x > 8) & (centre_x < 10) & (centre_y > 6) & (centre_y < 8)] = 10
+    types_[0] = 0
+    return mesh, types_, centre_x, centre_y
+
+
+def gate_cases(ref, rng, arrays):
+    mesh, types_, cx, cy = gate_mesh(rng)
+    arrays['gate_bounds'] = mesh['bounds']
+    arrays['gate_topology'] = mesh['topology']
+    arrays['gate_types'] = types_
+    bed = np.where(types_ == 10, 2.0, 0.5).astype(np.float32)
+    bed[0] = 0
+    arrays['gate_bed'] = bed
+    strip_low = (11.0, 3.0)      # inside the lower strip
+    strip_high = (11.0, 10.0)    # inside the upper strip
+    island = (9.0, 7.0)          # a gate cell between river and the pond cell between the strips
+    river = (3.0, 3.0)
+    pond = (20.0, 6.0)
+    corner = (10.0, 6.0)         # a corner shared by four cells: first id wins
+    base = [('north', strip_high, river), ('south', strip_low, pond), ('island', island, river)]
+    variants = [
+        dict(gates=base),
+        dict(gates=base, open_elevation=2.0),
+        dict(gates=base, open_elevation=float(np.nextafter(np.float32(2.0), np.float32(3.0)))),
+        dict(gates=base[:2]),
+        dict(gates=[base[0], ('south', strip_low, pond), ('again', (11.0, 1.0), river)]),
+        dict(gates=[base[0], ('south', strip_low, strip_high), base[2]]),
+        dict(gates=[base[0], ('south', river, pond), base[2]]),
+        dict(gates=[base[0], ('south', (99.0, 3.0), pond), base[2]]),
+        dict(gates=[base[0], ('south', strip_low, corner), base[2]]),
+        dict(gates=base, pond_land_type=12),
+        dict(gates=base, overlap=True),
+        dict(gates=base, level_on='gate'),
+        dict(gates=base, level_on='river'),
+        dict(gates=[base[0], base[1], ('island', (8.0, 6.0), river)]),
+        dict(gates=[base[0], base[1], ('island', island, (12.0, 8.0))]),
+    ]
+    out = []
+    for i, v in enumerate(variants):
+        land_types = types_.copy()
+        if v.get('overlap'):
+            land_types[land_types == 10] = 11
+        pond_type = v.get('pond_land_type', 11)
+        config = NS(land_type=10, pond_land_type=pond_type, open_elevation=v.get('open_elevation', 1.0),
+                    gates=[NS(name=n, inside_point=p, control_point=q) for n, p, q in v['gates']])
+        boundaries = []
+        if v.get('level_on') == 'gate':
+            boundaries.append(NS(kind='level', cells=np.flatnonzero(land_types == 10)[:1]))
+        elif v.get('level_on') == 'river':
+            boundaries.append(NS(kind='level', cells=np.flatnonzero(land_types == 1)[:3]))
+        spec = dict(land_type=10, pond_land_type=pond_type, open_elevation=config.open_elevation,
+                    gates=[dict(name=n, inside_point=list(p), control_point=list(q)) for n, p, q in v['gates']],
+                    overlap=bool(v.get('overlap')), level_cells=[b.cells.tolist() for b in boundaries])
+        try:
+            layout = ref.gate.GateLayout.load(config, NS(bounds=mesh['bounds']), land_types, mesh['topology'],
+                                              boundaries, bed)
+        except ValueError as error:
+            out.append(dict(spec, error=str(error)))
+            continue
+        out.append(dict(spec, error=None, cell_gate=layout.cell_gate.tolist(), controls=layout.controls.tolist(),
+                        cells=[c.tolist() for c in layout.cells]))
+    return out
+
+
+# ---------------------------------------------------------------- configs
+
+DOMAIN = dict(ne='NE', ns='NS', epsg_code=2326, domain_dir='OUT', start='2023-09-07T16:00:00+08:00',
+              duration=3600, warmup_duration=0,
+              land_parameters={'10': dict(manning_n=0.03, infiltration='none')})
+FORCE = dict(boundaries=[dict(name='river', kind='discharge', line='line.geojson', series='q.csv')],
+             rainfall=dict(raster='rain.tif', intervals='rain.csv'))
+GATE = dict(land_type=10, pond_land_type=11, enabled=True, trigger_level=1.5, opening_seconds=600,
+            open_elevation=0.5, gates=[dict(name='g1', inside_point=[1, 2], control_point=[3, 4])])
+
+DOMAIN_CHANGES = [
+    {}, {'afa': 0}, {'afa': 1}, {'afa': 1.01}, {'sita': -0.1}, {'sita': 0.7}, {'sita': 1.5}, {'min_h': 0},
+    {'min_h': 1e-3}, {'start': '2023-09-07T16:00:00'}, {'start': 1694054400}, {'start': '2023-09-07T08:00:00Z'},
+    {'duration': 0}, {'duration': 16777215}, {'duration': 16777215, 'warmup_duration': 1},
+    {'warmup_duration': -1}, {'warmup_duration': 600}, {'land_parameters': {}},
+    {'land_parameters': {'256': dict(manning_n=0.03, infiltration='none')}},
+    {'land_parameters': {'-1': dict(manning_n=0.03, infiltration='none')}},
+    {'land_parameters': {'0': dict(manning_n=0.0, infiltration='none')}},
+    {'land_parameters': {'10': dict(manning_n=-0.01, infiltration='none')}},
+    {'land_parameters': {'10': dict(manning_n=0.03, infiltration=dict(f0_mm_h=5, fc_mm_h=10, k_per_h=2))}},
+    {'land_parameters': {'10': dict(manning_n=0.03, infiltration=dict(f0_mm_h=60, fc_mm_h=10, k_per_h=4))}},
+    {'land_parameters': {'10': dict(manning_n=0.03, infiltration=dict(f0_mm_h=60, fc_mm_h=10))}},
+    {'land_parameters': {'10': dict(manning_n=0.03, infiltration='horton')}},
+    {'land_parameters': {'10': dict(manning_n=0.03)}},
+    {'land_parameters': {'10': dict(manning_n=0.03, infiltration='none', extra=1)}},
+    {'manning': {'10': 0.03}}, {'yield_step': 0}, {'yield_step': 60}, {'yield_step': 300.5},
+    {'yield_step': 300.0}, {'stations': {'a': [1, 2]}}, {'stations': {'a': [1]}}, {'stations': {'a': [1, 2, 3]}},
+    {'restart_state': 'state.fdb'}, {'observation_dir': 'obs'}, {'ne': 'MISSING'}, {'epsg_code': '2326'},
+    {'epsg_code': 2326.5}, {'duration': '3600'},
+]
+FORCE_CHANGES = [
+    {}, {'boundaries': []},
+    {'boundaries': [FORCE['boundaries'][0], dict(FORCE['boundaries'][0])]},
+    {'boundaries': [dict(FORCE['boundaries'][0], kind='flow')]},
+    {'boundaries': [dict(FORCE['boundaries'][0], name='')]},
+    {'boundaries': [dict(FORCE['boundaries'][0], kind='level'), dict(FORCE['boundaries'][0], name='sea')]},
+    {'rainfall': dict(raster='rain.tif')}, {'gate': None}, {'gate': GATE},
+    {'gate': dict(GATE, pond_land_type=10)}, {'gate': dict(GATE, opening_seconds=0)},
+    {'gate': dict(GATE, gates=[])}, {'gate': dict(GATE, land_type=256)},
+    {'gate': dict(GATE, gates=[GATE['gates'][0], GATE['gates'][0]])},
+    {'gate': dict(GATE, gates=[dict(GATE['gates'][0], inside_point=[1])])},
+    {'gate': dict(GATE, extra=True)}, {'gate': {k: v for k, v in GATE.items() if k != 'enabled'}},
+    {'pipes': []},
+]
+TIMES = ['2023-09-07T08:00:00Z', '2023-09-07T16:00:00+08:00', '2023-09-07T08:00:00', '2023-09-07',
+         '2023-09-07T08:00:00.123456-03:30', '2023-09-07 08:00:00+00:00', '2023-02-29T00:00:00Z']
+
+
+def validate(model, text):
+    from pydantic import ValidationError
+    try:
+        value = model.model_validate_json(text)
+    except ValidationError as error:
+        return dict(accepted=False, errors=sorted([[str(p) for p in e['loc']] for e in error.errors()]))
+    return dict(accepted=True, dump=value.model_dump(mode='json'))
+
+
+def config_cases(ref, work: Path):
+    (work / 'NE').write_text('mesh\n')
+    (work / 'NS').write_text('mesh\n')
+
+    def place(d):
+        return {k: (str(work / v) if k in ('ne', 'ns', 'domain_dir') and isinstance(v, str) else v)
+                for k, v in d.items()}
+
+    def unplace(value):
+        if isinstance(value, dict):
+            return {k: unplace(v) for k, v in value.items()}
+        if isinstance(value, str) and value.startswith(str(work) + '/'):
+            return value[len(str(work)) + 1:]
+        return value
+
+    out = []
+    for change in DOMAIN_CHANGES:
+        config = {**DOMAIN, **change}
+        result = validate(ref.input.DomainConfig, json.dumps(place(config)))
+        out.append(dict(kind='domain', config=config, **unplace(result)))
+    for change in FORCE_CHANGES:
+        config = {**FORCE, **change}
+        result = validate(ref.input.ForceConfig, json.dumps(config))
+        out.append(dict(kind='force', config=config, **result))
+    times = []
+    for text in TIMES:
+        try:
+            times.append(dict(text=text, value=ref.force.absolute_time(text).isoformat()))
+        except ValueError as error:
+            times.append(dict(text=text, error=str(error)))
+    return out, times
+
+
+def main():
+    import tempfile
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument('--reference', type=Path, default=Path('/root/reference'))
+    args = parser.parse_args()
+    ref = load_reference(args.reference)
+    rng = np.random.default_rng(20261204)
+    arrays = {}
+    mesh = quadtree(rng, 12, 9, 0.3)
+    for key in ('topology', 'length', 'face_ptr', 'face_count', 'flat', 'bounds', 'area'):
+        arrays[f'mesh_{key}'] = mesh[key]
+    golden = dict(land=land_cases(ref, rng, mesh, arrays), faces=face_fraction_cases(ref, rng, mesh, arrays),
+                  still=still_water_cases(ref, rng, mesh, arrays), gate=gate_cases(ref, rng, arrays))
+    with tempfile.TemporaryDirectory() as work:
+        golden['configs'], golden['times'] = config_cases(ref, Path(work))
+    (HERE / 'host_golden.json').write_text(json.dumps(golden, indent=1) + '\n')
+    np.savez_compressed(HERE / 'host_golden.npz', **arrays)
+    summary = {k: (sum(c.get('error') is not None for c in v if isinstance(c, dict)), len(v))
+               for k, v in golden.items()}
+    print('cases (errors, total):', summary)
+
+
+if __name__ == '__main__':
+    main()
