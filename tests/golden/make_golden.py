@@ -23,17 +23,47 @@ built here (a 2 m base grid with random cells split into four 1 m cells).
 from __future__ import annotations
 
 import argparse
+import ast
+import csv
 import importlib
 import json
+import math
 import sys
 import types
 from collections import defaultdict
+from dataclasses import dataclass
+from datetime import datetime, timedelta, timezone
 from pathlib import Path
 from types import SimpleNamespace as NS
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
+
+
+def definitions(path: Path, names, namespace, inside=None) -> dict:
+    """Compile the named top-level definitions of one reference file (or the
+    named methods of its class ``inside``) from its unchanged source, and run
+    them in ``namespace``. The rest of the file, which needs Taichi,
+    rasterio or fastdb4py, is not run."""
+    tree = ast.parse(path.read_text(), filename=str(path))
+    body = tree.body
+    if inside is not None:
+        body = next(n for n in body if isinstance(n, ast.ClassDef) and n.name == inside).body
+    keep = []
+    for node in body:
+        if isinstance(node, (ast.FunctionDef, ast.ClassDef)) and node.name in names:
+            keep.append(node)
+        elif isinstance(node, ast.Assign) and all(isinstance(t, ast.Name) and t.id in names for t in node.targets):
+            keep.append(node)
+    found = {getattr(n, 'name', None) or n.targets[0].id for n in keep}
+    if found != set(names):
+        raise LookupError(f'{path}: missing {sorted(set(names) - found)}')
+    for node in keep:
+        if inside is not None:
+            node.decorator_list = []
+    exec(compile(ast.Module(keep, type_ignores=[]), str(path), 'exec'), namespace)
+    return namespace
 
 
 def load_reference(root: Path):
@@ -43,10 +73,19 @@ def load_reference(root: Path):
     package = types.ModuleType('nh_flood_2d.preprocess')
     package.__path__ = [str(src / 'nh_flood_2d' / 'preprocess')]
     sys.modules['nh_flood_2d.preprocess'] = package
-    return NS(hydraulics=importlib.import_module('nh_flood_2d.preprocess.hydraulics'),
-              gate=importlib.import_module('nh_flood_2d.preprocess.gate'),
-              input=importlib.import_module('nh_flood_2d.input'),
-              force=importlib.import_module('nh_flood_2d.input.force'))
+    ref = NS(hydraulics=importlib.import_module('nh_flood_2d.preprocess.hydraulics'),
+             gate=importlib.import_module('nh_flood_2d.preprocess.gate'),
+             input=importlib.import_module('nh_flood_2d.input'),
+             force=importlib.import_module('nh_flood_2d.input.force'))
+    pkg = src / 'nh_flood_2d'
+    ref.clock = NS(**definitions(pkg / 'core/clock.py', ['_TICKS_PER_SECOND', '_MAX_TICKS', '_seconds_to_ticks',
+                                                         '_words'], dict(math=math, np=np)))
+    ref.series = NS(**definitions(pkg / 'preprocess/force.py', ['TimeSeries', 'RainField'],
+                                  dict(np=np, csv=csv, dataclass=dataclass, absolute_time=ref.force.absolute_time)))
+    ref.budget = NS(**definitions(pkg / 'core/run_record.py', ['WaterBudget'], dict(np=np, csv=csv)))
+    ref.balance = NS(**definitions(pkg / 'core/gate.py', ['append_gate_balance'], dict(csv=csv, Path=Path)))
+    ref.report = definitions(pkg / 'core/gate.py', ['report'], dict(np=np), inside='GateController')['report']
+    return ref
 
 
 # ---------------------------------------------------------------- meshes
@@ -289,6 +328,169 @@ def gate_cases(ref, rng, arrays):
     return out
 
 
+# ---------------------------------------------------------------- clock, series, rain
+
+def tick_cases(ref, rng):
+    values = [0.0, -0.0, 1.0, 0.5, 2.0 ** -41, 3 * 2.0 ** -41, 5 * 2.0 ** -41, 2.0 ** -40, 1e-6, 1e-12, 0.1, 1 / 3,
+              3600.000001, 16777215.999999, 2.0 ** 24 - 2.0 ** -29, 2.0 ** 24, 1.5e7, -1e-300, math.nan, math.inf,
+              -math.inf, 1e300, 5e-324]
+    values += (10.0 ** rng.uniform(-13, 7.2, 120)).tolist()
+    values += ((rng.integers(1, 1 << 20, 40) * 2 + 1).astype(float) * 2.0 ** -41).tolist()  # exact half ticks
+    out = []
+    for value in values:
+        try:
+            ticks = ref.clock._seconds_to_ticks(value)
+        except ValueError as error:
+            out.append(dict(seconds=repr(float(value)), error=str(error)))
+            continue
+        out.append(dict(seconds=repr(float(value)), ticks=str(ticks), words=ref.clock._words(ticks).tolist()))
+    return out
+
+
+ORIGIN = datetime(2023, 9, 7, 8, tzinfo=timezone.utc)
+
+
+def series_cases(ref, rng, work: Path):
+    out = []
+    for case in range(10):
+        n = int(rng.integers(2, 12)) if case != 6 else 1
+        steps = rng.choice([0.25, 0.5, 1, 7.5, 60, 300, 1e-3], size=n) * rng.integers(1, 5, size=n)
+        times = -float(rng.uniform(0, 60)) + np.concatenate([[0.0], np.cumsum(steps[1:])])
+        if case == 7:
+            times[-1] = times[-2]
+        values = [repr(float(round(v, 4))) for v in rng.normal(0, 5, n)]
+        if case == 8:
+            values[0] = 'nan'
+        lines = ['time,value']
+        for t, v in zip(times, values):
+            offset = timezone(timedelta(hours=int(rng.integers(-11, 13)), minutes=int(rng.choice([0, 30]))))
+            lines.append(f'{(ORIGIN + timedelta(seconds=float(t))).astimezone(offset).isoformat()},{v}')
+        text = '\n'.join(lines) + '\n'
+        end = float(times[-1]) + (5.0 if case == 9 else -float(rng.uniform(0, 0.1 * (times[-1] - times[0]))))
+        path = work / f'series{case}.csv'
+        path.write_text(text)
+        spec = dict(csv=text, begin=0.0, end=max(end, 0.0))
+        try:
+            series = ref.series.TimeSeries.load(path, ORIGIN, spec['begin'], spec['end'])
+        except ValueError as error:
+            out.append(dict(spec, error=str(error).replace(str(path), '{path}')))
+            continue
+        queries = np.concatenate([series.times, rng.uniform(series.times[0] - 10, series.times[-1] + 10, 30)])
+        out.append(dict(spec, error=None, times=series.times.tolist(), values=series.values.tolist(),
+                        queries=queries.tolist(), at=[series.at(q) for q in queries]))
+    return out
+
+
+def rain_cases(ref, rng):
+    out = []
+    for case in range(6):
+        bands, pixels = int(rng.integers(1, 8)), int(rng.integers(1, 6))
+        durations = rng.choice([60.0, 300.0, 0.5, 1800.0, 7.25], size=bands)
+        starts = -float(rng.uniform(0, 100)) + np.concatenate([[0.0], np.cumsum(durations[:-1])])
+        ends = starts + durations
+        mm = rng.uniform(0, 30, (bands, pixels)).astype(np.float32).astype(float)
+        mapping = rng.integers(0, pixels, 20).astype(np.int32)
+        mapping[0] = 0
+        field = ref.series.RainField(starts, ends, mm, mapping)
+        queries = np.concatenate([starts, ends, rng.uniform(starts[0] - 5, ends[-1] + 5, 20)])
+        out.append(dict(starts=starts.tolist(), ends=ends.tolist(), millimetres=mm.tolist(), pixel_index=mapping.tolist(),
+                        queries=queries.tolist(), index=[field.index_at(q) for q in queries],
+                        rates=[field.rates(i).tolist() for i in range(bands)]))
+    return out
+
+
+# ---------------------------------------------------------------- budget rows and gate reports
+
+def budget_cases(ref, rng, work: Path):
+    out = []
+    for case in range(6):
+        nb = int(rng.integers(0, 4)) if case else 0
+        boundaries = [NS(kind=str(rng.choice(['level', 'discharge'])), name=f'edge{i}') for i in range(nb)]
+        initial = float(rng.uniform(0, 1e4)) if case else 0.0
+        path = work / f'budget{case}.csv'
+        budget = ref.budget.WaterBudget(path, boundaries, initial)
+        calls = []
+        for k in range(4):
+            for _ in range(int(rng.integers(1, 6))):
+                dt = float(np.float32(rng.uniform(0.01, 1)))
+                rain = float(rng.uniform(0, 5)) if case else 0.0
+                values = rng.normal(0, 3, nb) if case else np.zeros(nb)
+                budget.add_forcing(dt, rain, values)
+                calls.append(['forcing', dt, rain, values.tolist()])
+            terms = rng.normal(0, 10, 4 + 6 * nb) if case else np.zeros(4 + 6 * nb)
+            budget.set_device_terms(terms)
+            calls.append(['terms', terms.tolist()])
+            date, seconds = ORIGIN + timedelta(seconds=300 * k), 300 * k
+            storage = float(rng.uniform(0, 2e4)) if case else 0.0
+            phase = 'warmup' if k == 0 else 'simulation'
+            budget.output(date, seconds, storage, phase)
+            calls.append(['output', date.isoformat(), seconds, storage, phase])
+        budget.close()
+        out.append(dict(boundaries=[[b.kind, b.name] for b in boundaries], initial=initial, calls=calls,
+                        csv=path.read_text()))
+    return out
+
+
+class Field:
+    """A stand-in for a device field: to_numpy() returns a copy."""
+
+    def __init__(self, array):
+        self.array = np.asarray(array)
+
+    def to_numpy(self):
+        return self.array.copy()
+
+
+def report_cases(ref, rng, arrays, gates, work: Path):
+    """GateController.report on seeded controller state for the first valid
+    gate layout, and gate_balance.csv rows appended from three reports."""
+    spec = next(g for g in gates if g['error'] is None and len(g['gates']) == 3)
+    types_ = arrays['gate_types']
+    n_gates = len(spec['gates'])
+    cells = [np.array(c, dtype=np.int32) for c in spec['cells']]
+    layout = NS(cells=cells, controls=np.array(spec['controls'], dtype=np.int32))
+    bed = arrays['gate_bed']
+    pond = (types_ == spec['pond_land_type']).astype(np.int32)
+    pond[0] = 0
+    area = np.full(len(types_), 4.0)
+    out = []
+    path = work / 'gate_balance.csv'
+    for case in range(3):
+        origin_seconds = float(rng.choice([0.0, 3600.0, 1234.5]))
+        formal = ref.clock._seconds_to_ticks(origin_seconds)
+        commanded = rng.integers(0, 2, n_gates).astype(np.int32)
+        flow_seen = rng.integers(0, 2, n_gates).astype(np.int32)
+        opened = rng.integers(0, 2, n_gates).astype(np.int32)
+
+        def words():
+            ticks = formal + rng.integers(0, 1 << 52, n_gates).astype(np.uint64)
+            return np.stack([ticks >> np.uint64(32), ticks & np.uint64(0xffffffff)], axis=1).astype(np.uint32)
+
+        command, first_flow, opened_at = words(), words(), words()
+        totals = rng.normal(0, 50, 4 * n_gates + 8 + 6 * n_gates)
+        depth = rng.uniform(0, 2, len(types_)).astype(np.float32)
+        initial_storage = float(rng.uniform(0, 500))
+        initial_channel = rng.uniform(0, 50, n_gates)
+        config = NS(gates=[NS(name=g['name']) for g in spec['gates']], opening_seconds=float(rng.uniform(60, 900)),
+                    trigger_level=float(rng.uniform(0, 3)), pond_land_type=spec['pond_land_type'],
+                    open_elevation=spec['open_elevation'])
+        clock_seconds = float(rng.uniform(0, 2e5))
+        controller = NS(budget=NS(flush=lambda t=totals: t.copy()), commanded=Field(commanded), command=Field(command),
+                        flow_seen=Field(flow_seen), first_flow=Field(first_flow), opened=Field(opened),
+                        opened_at=Field(opened_at), formal_tick=formal, config=config, closed=Field(bed),
+                        layout=layout, channel_source_offset=4 * n_gates + 8, initial_channel_storage=initial_channel,
+                        offset=4 * n_gates, pond=Field(pond), initial_storage=initial_storage)
+        report = ref.report(controller, depth, area, clock_seconds)
+        ref.balance.append_gate_balance(path, ORIGIN + timedelta(seconds=clock_seconds), clock_seconds, report)
+        out.append(dict(origin_seconds=origin_seconds, commanded=commanded.tolist(), command=command.tolist(),
+                        flow_seen=flow_seen.tolist(), first_flow=first_flow.tolist(), opened=opened.tolist(),
+                        opened_at=opened_at.tolist(), totals=totals.tolist(), depth=depth.tolist(),
+                        initial_storage=initial_storage, initial_channel=initial_channel.tolist(),
+                        opening_seconds=config.opening_seconds, trigger_level=config.trigger_level,
+                        clock_seconds=clock_seconds, report=report))
+    return dict(gate_case=gates.index(spec), area=4.0, cases=out, balance_csv=path.read_text())
+
+
 # ---------------------------------------------------------------- configs
 
 DOMAIN = dict(ne='NE', ns='NS', epsg_code=2326, domain_dir='OUT', start='2023-09-07T16:00:00+08:00',
@@ -392,12 +594,17 @@ def main():
         arrays[f'mesh_{key}'] = mesh[key]
     golden = dict(land=land_cases(ref, rng, mesh, arrays), faces=face_fraction_cases(ref, rng, mesh, arrays),
                   still=still_water_cases(ref, rng, mesh, arrays), gate=gate_cases(ref, rng, arrays))
+    golden['ticks'] = tick_cases(ref, rng)
+    golden['rain'] = rain_cases(ref, rng)
     with tempfile.TemporaryDirectory() as work:
         golden['configs'], golden['times'] = config_cases(ref, Path(work))
-    (HERE / 'host_golden.json').write_text(json.dumps(golden, indent=1) + '\n')
+        golden['series'] = series_cases(ref, rng, Path(work))
+        golden['budget'] = budget_cases(ref, rng, Path(work))
+        golden['report'] = report_cases(ref, rng, arrays, golden['gate'], Path(work))
+    (HERE / 'host_golden.json').write_text(json.dumps(golden, separators=(',', ':')) + '\n')
     np.savez_compressed(HERE / 'host_golden.npz', **arrays)
     summary = {k: (sum(c.get('error') is not None for c in v if isinstance(c, dict)), len(v))
-               for k, v in golden.items()}
+               for k, v in golden.items() if isinstance(v, list)}
     print('cases (errors, total):', summary)
 
 

@@ -1,9 +1,14 @@
-"""Golden vectors from the reference's own code (tests/golden/make_golden.py
-ran preprocess/hydraulics.py, preprocess/gate.py and input/*.py of
-nh-flood-2d on seeded quadtree meshes and configs). Every case is replayed
+"""Golden vectors from the reference's own code. tests/golden/make_golden.py
+ran nh-flood-2d's preprocess/hydraulics.py, preprocess/gate.py and
+input/*.py, and the plain-Python definitions of core/clock.py (tick
+conversion), preprocess/force.py (TimeSeries, RainField), core/run_record.py
+(WaterBudget) and core/gate.py (GateController.report, append_gate_balance)
+on seeded meshes, configs and controller states. Every case is replayed
 through nhflood: arrays must match bit for bit, errors by message, configs
-by acceptance, error locations and the validated dump."""
+by acceptance, error locations and the validated dump, CSV files byte for
+byte."""
 import json
+from datetime import datetime, timedelta, timezone
 from pathlib import Path
 from types import SimpleNamespace as NS
 
@@ -11,14 +16,18 @@ import numpy as np
 import pytest
 from pydantic import ValidationError
 
-from nhflood.gate import GateLayout
+from nhflood.clock import seconds_to_ticks, words
+from nhflood.forcing import RainField, TimeSeries
+from nhflood.gate import GateController, GateLayout, append_gate_balance
 from nhflood.geometry import connected_still_water, map_land_parameters, open_boundary_face_fractions
 from nhflood.input import DomainConfig, ForceConfig, LandParameters, absolute_time
+from nhflood.run_record import WaterBudget
 
 GOLDEN = Path(__file__).parent / 'golden'
 CASES = json.loads((GOLDEN / 'host_golden.json').read_text())
 ARRAYS = np.load(GOLDEN / 'host_golden.npz')
 MESH = {key[5:]: ARRAYS[key] for key in ARRAYS.files if key.startswith('mesh_')}
+ORIGIN = datetime(2023, 9, 7, 8, tzinfo=timezone.utc)
 
 
 def same_bits(actual, expected):
@@ -123,3 +132,91 @@ def test_absolute_time_matches_the_reference(case):
         assert str(error.value) == case['error']
     else:
         assert absolute_time(case['text']).isoformat() == case['value']
+
+
+@pytest.mark.parametrize('case', CASES['ticks'], ids=lambda c: c['seconds'])
+def test_clock_ticks_match_the_reference(case):
+    seconds = float(case['seconds'])
+    if 'error' in case:
+        with pytest.raises(ValueError) as error:
+            seconds_to_ticks(seconds)
+        assert str(error.value) == case['error']
+        return
+    ticks = seconds_to_ticks(seconds)
+    assert ticks == int(case['ticks'])
+    assert words(ticks).tolist() == case['words']
+
+
+@pytest.mark.parametrize('case', range(len(CASES['series'])))
+def test_time_series_match_the_reference(tmp_path, case):
+    spec = CASES['series'][case]
+    path = tmp_path / 'series.csv'
+    path.write_text(spec['csv'])
+    if spec['error'] is not None:
+        with pytest.raises(ValueError) as error:
+            TimeSeries.load(path, ORIGIN, spec['begin'], spec['end'])
+        assert str(error.value) == spec['error'].replace('{path}', str(path))
+        return
+    series = TimeSeries.load(path, ORIGIN, spec['begin'], spec['end'])
+    assert series.times.tolist() == spec['times'] and series.values.tolist() == spec['values']
+    assert [series.at(q) for q in spec['queries']] == spec['at']
+
+
+@pytest.mark.parametrize('case', range(len(CASES['rain'])))
+def test_rain_intervals_match_the_reference(case):
+    spec = CASES['rain'][case]
+    field = RainField(np.array(spec['starts']), np.array(spec['ends']), np.array(spec['millimetres']),
+                      np.array(spec['pixel_index'], dtype=np.int32))
+    assert [field.index_at(q) for q in spec['queries']] == spec['index']
+    assert [field.rates(i).tolist() for i in range(len(spec['starts']))] == spec['rates']
+
+
+@pytest.mark.parametrize('case', range(len(CASES['budget'])))
+def test_mass_balance_rows_match_the_reference(tmp_path, case):
+    spec = CASES['budget'][case]
+    path = tmp_path / 'mass_balance.csv'
+    budget = WaterBudget(path, [NS(kind=kind, name=name) for kind, name in spec['boundaries']], spec['initial'])
+    for call in spec['calls']:
+        if call[0] == 'forcing':
+            budget.add_forcing(call[1], call[2], np.array(call[3]))
+        elif call[0] == 'terms':
+            budget.set_device_terms(np.array(call[1]))
+        else:
+            budget.output(datetime.fromisoformat(call[1]), call[2], call[3], call[4])
+    budget.close()
+    assert path.read_text() == spec['csv']
+
+
+def gate_controller(spec, case):
+    """nhflood's GateController in the state the reference's report was given."""
+    layout_spec = CASES['gate'][spec['gate_case']]
+    config = NS(gates=[NS(name=g['name']) for g in layout_spec['gates']], opening_seconds=case['opening_seconds'],
+                trigger_level=case['trigger_level'], pond_land_type=layout_spec['pond_land_type'],
+                open_elevation=layout_spec['open_elevation'])
+    layout = GateLayout(np.array(layout_spec['cell_gate'], dtype=np.int32),
+                        np.array(layout_spec['controls'], dtype=np.int32),
+                        [np.array(c, dtype=np.int32) for c in layout_spec['cells']])
+    controller = GateController.build(config, layout, ARRAYS['gate_bed'], ARRAYS['gate_types'],
+                                      ARRAYS['gate_topology'], case['origin_seconds'])
+    controller.totals = np.array(case['totals'])
+    controller.initial_storage = case['initial_storage']
+    controller.initial_channel_storage = np.array(case['initial_channel'])
+    controller.state.update(commanded=np.array(case['commanded'], dtype=np.int32),
+                            command=np.array(case['command'], dtype=np.uint32),
+                            flow_seen=np.array(case['flow_seen'], dtype=np.int32),
+                            first_flow=np.array(case['first_flow'], dtype=np.uint32),
+                            opened=np.array(case['opened'], dtype=np.int32),
+                            opened_at=np.array(case['opened_at'], dtype=np.uint32))
+    return controller
+
+
+def test_gate_report_and_balance_rows_match_the_reference(tmp_path):
+    spec = CASES['report']
+    area = np.full(len(ARRAYS['gate_types']), spec['area'])
+    path = tmp_path / 'gate_balance.csv'
+    for case in spec['cases']:
+        report = gate_controller(spec, case).report(np.array(case['depth'], dtype=np.float32), area,
+                                                     case['clock_seconds'])
+        assert json.loads(json.dumps(report)) == case['report']
+        append_gate_balance(path, ORIGIN + timedelta(seconds=case['clock_seconds']), case['clock_seconds'], report)
+    assert path.read_text() == spec['balance_csv']
