@@ -85,6 +85,9 @@ def load_reference(root: Path):
     ref.budget = NS(**definitions(pkg / 'core/run_record.py', ['WaterBudget'], dict(np=np, csv=csv)))
     ref.balance = NS(**definitions(pkg / 'core/gate.py', ['append_gate_balance'], dict(csv=csv, Path=Path)))
     ref.report = definitions(pkg / 'core/gate.py', ['report'], dict(np=np), inside='GateController')['report']
+    ref.pressure = NS(**definitions(pkg / 'core/pressure.py', ['HangingGeometry', 'hanging_geometry'],
+                                    dict(np=np, dataclass=dataclass)))
+    ref.domain = definitions(pkg / 'preprocess/domain.py', ['_filter_ne_ns'], dict(Path=Path))
     return ref
 
 
@@ -121,10 +124,12 @@ def quadtree(rng, nx, ny, split_fraction):
     side_id = {key: i for i, key in enumerate(sorted(owner), 1)}
     topology = np.zeros((len(side_id) + 1, 3), dtype=np.int32)
     length = np.zeros(len(side_id) + 1, dtype=np.float32)
+    side_xy = np.zeros((len(side_id) + 1, 2), dtype=np.float64)
     for key, i in side_id.items():
-        orient, _, u, w = key
+        orient, coord, u, w = key
         topology[i] = (orient, owner[key].get('lo', 0), owner[key].get('hi', 0))
         length[i] = w - u
+        side_xy[i] = (coord, (u + w) / 2) if orient == 2 else ((u + w) / 2, coord)
     n = len(cells) + 1
     face_ptr = np.zeros((n, 4), dtype=np.int32)
     face_count = np.zeros((n, 4), dtype=np.int32)
@@ -139,7 +144,8 @@ def quadtree(rng, nx, ny, split_fraction):
     area = np.zeros(n, dtype=np.float64)
     area[1:] = (bounds[1:, 2] - bounds[1:, 0]) * (bounds[1:, 3] - bounds[1:, 1])
     return dict(topology=topology, length=length, face_ptr=face_ptr, face_count=face_count,
-                flat=np.array(flat, dtype=np.int32), bounds=bounds, area=area)
+                flat=np.array(flat, dtype=np.int32), bounds=bounds, area=area, side_xy=side_xy,
+                centre=np.column_stack([(bounds[:, 0] + bounds[:, 2]) / 2, (bounds[:, 1] + bounds[:, 3]) / 2]))
 
 
 def exterior_cells(mesh, side):
@@ -328,6 +334,59 @@ def gate_cases(ref, rng, arrays):
     return out
 
 
+def hanging_cases(ref, rng, arrays):
+    """hanging_geometry on a uniform grid (None), and on quadtrees."""
+    out = []
+    for case, (nx, ny, split) in enumerate([(6, 5, 0.0), (12, 9, 0.3), (10, 10, 0.6), (7, 3, 0.15)]):
+        mesh = quadtree(rng, nx, ny, split)
+        x, y = mesh['centre'][:, 0], mesh['centre'][:, 1]
+        sx, sy = mesh['side_xy'][:, 0], mesh['side_xy'][:, 1]
+        for key, value in (('x', x), ('y', y), ('sx', sx), ('sy', sy), ('topology', mesh['topology'])):
+            arrays[f'hang{case}_{key}'] = value
+        result = ref.pressure.hanging_geometry(x, y, sx, sy, mesh['topology'])
+        if result is None:
+            out.append(dict(none=True))
+            continue
+        for key in ('edge_index', 'offsets', 'gradient_slots', 'cells', 'axes'):
+            arrays[f'hang{case}_{key}'] = getattr(result, key)
+        out.append(dict(none=False))
+    return out
+
+
+def ne_ns_text(rng, mesh, missing_fraction):
+    """NE lines (id, 4 face counts, side ids, x, y, z, class) and NS lines
+    (id, orient, left, right, bottom, top, length, x, y, z, attr) of a
+    quadtree, with some cells given the z = -9999 marker."""
+    ne = []
+    for cell in range(1, len(mesh['bounds'])):
+        ids = [mesh['flat'][mesh['face_ptr'][cell, d] + k] for d in range(4) for k in range(mesh['face_count'][cell, d])]
+        z = '-9999' if rng.random() < missing_fraction else repr(float(np.float32(rng.uniform(-5, 40))))
+        if z == '-9999' and rng.random() < .3:
+            z = '-9999.0'
+        x, y = mesh['centre'][cell]
+        ne.append(','.join(map(str, [cell, *mesh['face_count'][cell].tolist(), *ids, x, y, z, int(rng.integers(1, 5))])))
+    ns = []
+    for side in range(1, len(mesh['topology'])):
+        orient, lo, hi = mesh['topology'][side].tolist()
+        nb = (lo, hi, 0, 0) if orient == 2 else (0, 0, lo, hi)
+        x, y = mesh['side_xy'][side]
+        ns.append(','.join(map(str, [side, orient, *nb, float(mesh['length'][side]), x, y, 0, 0])))
+    return '\n'.join(ne) + '\n', '\n'.join(ns) + '\n'
+
+
+def filter_cases(ref, rng, work: Path):
+    out = []
+    for case, (nx, ny, split, missing) in enumerate([(5, 4, 0.3, 0.0), (8, 6, 0.4, 0.15), (6, 6, 0.5, 0.5)]):
+        ne_text, ns_text = ne_ns_text(rng, quadtree(rng, nx, ny, split), missing)
+        (work / 'ne.txt').write_text(ne_text)
+        (work / 'ns.txt').write_text(ns_text)
+        ref.domain['_filter_ne_ns'](str(work / 'ne.txt'), str(work / 'ns.txt'), str(work / 'ne_out.txt'),
+                                    str(work / 'ns_out.txt'))
+        out.append(dict(ne=ne_text, ns=ns_text, ne_out=(work / 'ne_out.txt').read_text(),
+                        ns_out=(work / 'ns_out.txt').read_text()))
+    return out
+
+
 # ---------------------------------------------------------------- clock, series, rain
 
 def tick_cases(ref, rng):
@@ -355,7 +414,8 @@ def series_cases(ref, rng, work: Path):
     for case in range(10):
         n = int(rng.integers(2, 12)) if case != 6 else 1
         steps = rng.choice([0.25, 0.5, 1, 7.5, 60, 300, 1e-3], size=n) * rng.integers(1, 5, size=n)
-        times = -float(rng.uniform(0, 60)) + np.concatenate([[0.0], np.cumsum(steps[1:])])
+        times = np.concatenate([[0.0], np.cumsum(steps[1:])])
+        times -= float(rng.uniform(0, 0.5 * times[-1]))
         if case == 7:
             times[-1] = times[-2]
         values = [repr(float(round(v, 4))) for v in rng.normal(0, 5, n)]
@@ -594,6 +654,7 @@ def main():
         arrays[f'mesh_{key}'] = mesh[key]
     golden = dict(land=land_cases(ref, rng, mesh, arrays), faces=face_fraction_cases(ref, rng, mesh, arrays),
                   still=still_water_cases(ref, rng, mesh, arrays), gate=gate_cases(ref, rng, arrays))
+    golden['hanging'] = hanging_cases(ref, rng, arrays)
     golden['ticks'] = tick_cases(ref, rng)
     golden['rain'] = rain_cases(ref, rng)
     with tempfile.TemporaryDirectory() as work:
@@ -601,6 +662,7 @@ def main():
         golden['series'] = series_cases(ref, rng, Path(work))
         golden['budget'] = budget_cases(ref, rng, Path(work))
         golden['report'] = report_cases(ref, rng, arrays, golden['gate'], Path(work))
+        golden['filter'] = filter_cases(ref, rng, Path(work))
     (HERE / 'host_golden.json').write_text(json.dumps(golden, separators=(',', ':')) + '\n')
     np.savez_compressed(HERE / 'host_golden.npz', **arrays)
     summary = {k: (sum(c.get('error') is not None for c in v if isinstance(c, dict)), len(v))

@@ -1,9 +1,10 @@
 """Golden vectors from the reference's own code. tests/golden/make_golden.py
 ran nh-flood-2d's preprocess/hydraulics.py, preprocess/gate.py and
 input/*.py, and the plain-Python definitions of core/clock.py (tick
-conversion), preprocess/force.py (TimeSeries, RainField), core/run_record.py
-(WaterBudget) and core/gate.py (GateController.report, append_gate_balance)
-on seeded meshes, configs and controller states. Every case is replayed
+conversion), core/pressure.py (hanging_geometry), preprocess/domain.py
+(_filter_ne_ns), preprocess/force.py (TimeSeries, RainField),
+core/run_record.py (WaterBudget) and core/gate.py (GateController.report,
+append_gate_balance) on seeded meshes, configs and controller states. Every case is replayed
 through nhflood: arrays must match bit for bit, errors by message, configs
 by acceptance, error locations and the validated dump, CSV files byte for
 byte."""
@@ -19,8 +20,10 @@ from pydantic import ValidationError
 from nhflood.clock import seconds_to_ticks, words
 from nhflood.forcing import RainField, TimeSeries
 from nhflood.gate import GateController, GateLayout, append_gate_balance
-from nhflood.geometry import connected_still_water, map_land_parameters, open_boundary_face_fractions
+from nhflood.geometry import (connected_still_water, hanging_geometry, map_land_parameters,
+                              open_boundary_face_fractions)
 from nhflood.input import DomainConfig, ForceConfig, LandParameters, absolute_time
+from nhflood.preprocess import filter_ne_ns
 from nhflood.run_record import WaterBudget
 
 GOLDEN = Path(__file__).parent / 'golden'
@@ -220,3 +223,39 @@ def test_gate_report_and_balance_rows_match_the_reference(tmp_path):
         assert json.loads(json.dumps(report)) == case['report']
         append_gate_balance(path, ORIGIN + timedelta(seconds=case['clock_seconds']), case['clock_seconds'], report)
     assert path.read_text() == spec['balance_csv']
+
+
+@pytest.mark.parametrize('case', range(len(CASES['hanging'])))
+def test_hanging_geometry_matches_the_reference(case):
+    arrays = {key: ARRAYS[f'hang{case}_{key}'] for key in ('x', 'y', 'sx', 'sy', 'topology')}
+    result = hanging_geometry(arrays['x'], arrays['y'], arrays['sx'], arrays['sy'], arrays['topology'])
+    if CASES['hanging'][case]['none']:
+        assert result is None
+        return
+    for key in ('edge_index', 'offsets', 'gradient_slots', 'cells', 'axes'):
+        same_bits(getattr(result, key), ARRAYS[f'hang{case}_{key}'])
+
+
+@pytest.mark.parametrize('case', range(len(CASES['filter'])))
+def test_ne_ns_filter_matches_the_reference(case):
+    spec = CASES['filter'][case]
+    ne, ns = filter_ne_ns(spec['ne'].splitlines(keepends=True), spec['ns'].splitlines(keepends=True))
+    assert ''.join(line + '\n' for line in ne) == spec['ne_out']
+    assert ''.join(line + '\n' for line in ns) == spec['ns_out']
+
+
+@pytest.mark.parametrize('case', range(len(CASES['filter'])))
+def test_native_preprocessing_builds_the_tables_of_the_reference_filter(case):
+    """libnhfprep.so filters in C++; its tables equal the tables built from
+    the reference filter's output text."""
+    from nhflood import preprocess
+    from nhflood.build import build_host
+    build_host()
+    spec = CASES['filter'][case]
+    ne, ns = preprocess.native_tables(spec['ne'].encode(), spec['ns'].encode())
+    expected_ne = preprocess.build_ne_tables(spec['ne_out'].splitlines(keepends=True))
+    expected_ns = preprocess.build_ns_tables(spec['ns_out'].splitlines(keepends=True))
+    for actual, expected in ((ne, expected_ne), (ns, expected_ns)):
+        assert actual.keys() == expected.keys()
+        for key in actual:
+            same_bits(actual[key], np.asarray(expected[key]))
