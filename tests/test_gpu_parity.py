@@ -211,3 +211,35 @@ def test_tile_1024_both_cfl_forms_bit_exact(cuda_available, cfl):
     assert runs[1].elapsed > 0
     for r in runs:
         r.close()
+
+
+@pytest.mark.parametrize('name,batches', [('multires_quadtree', 2), ('dambreak_4096', 1)])
+def test_full_size_configurations_bit_exact(cuda_available, name, batches):
+    """The bench's full-size meshes, 1,362,175 quadtree cells (20 km, 2:1,
+    hanging edges) and 16,777,216 dam-break cells (33.5 M sides, 1024-cell
+    tiles, the separate CFL pass): the first 32-step batches on the fused
+    step as planned for the mesh and on the CPU restatement give identical
+    trace rows, state arrays and budget totals."""
+    from lockstep import FIELDS
+    from nhflood.plain import PlainRun
+    from nhflood.workloads import dambreak, multires_quadtree
+    from runner import oracle_factory
+    workload = multires_quadtree() if name == 'multires_quadtree' else dambreak()
+    runs = [PlainRun(workload, factory, batch_size=32) for factory in (oracle_factory, cuda_engine('auto'))]
+    try:
+        assert 'cfl=pass' in runs[1].engine.path, runs[1].engine.path
+        for _ in range(batches):
+            rows = []
+            for run in runs:
+                target, origin = run.begin()
+                rows.append(run.engine.run_batch(target, origin))
+                run.finish(rows[-1])
+            np.testing.assert_array_equal(rows[0], rows[1])
+            assert (rows[0][:, 3] == 1).all()  # every step completed
+        for field in FIELDS:
+            a, b = (run.engine.get(field) for run in runs)
+            np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32), err_msg=field)
+        np.testing.assert_array_equal(runs[0].engine.budget_flush(), runs[1].engine.budget_flush())
+    finally:
+        for run in runs:
+            run.close()
