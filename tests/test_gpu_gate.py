@@ -172,3 +172,37 @@ def test_gated_polder_matches_the_oracle_batch_by_batch(path):
     assert all(runs[1].engine.gate_state()['commanded'] == 1)
     for r in runs:
         r.close()
+
+
+def test_gated_polder_full_size_matches_the_oracle_batch_by_batch():
+    """The bench's polder at its full size, 1024 x 1024 cells of 5 m (four
+    gates of 64 cells commanded at t = 0 and opening over 600 s), on the
+    fused step: state, controller words and gate totals identical to the CPU
+    restatement after each of the first three 32-step batches."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / 'oracle'))
+    from engine import OracleEngine
+    from nhflood import workloads
+    from nhflood.model import STATE_F32, STATE_U32
+    from nhflood.native import CudaEngine
+    from nhflood.plain import PlainRun
+    w = workloads.gated_polder()
+    runs = [PlainRun(w, lambda a, p: OracleEngine(a, p)), PlainRun(w, CudaEngine)]
+    try:
+        assert runs[1].engine.path.startswith('tiled(tile=256') and 'cfl=pass' in runs[1].engine.path
+        bed0 = runs[1].engine.get('bed').copy()
+        for _ in range(3):
+            steps = [r.advance() for r in runs]
+            assert steps[0] == steps[1] == 32
+            for name in STATE_F32 + STATE_U32:
+                assert runs[0].engine.get(name).tobytes() == runs[1].engine.get(name).tobytes(), name
+            a, b = (r.engine.gate_state() for r in runs)
+            for name in a:
+                np.testing.assert_array_equal(a[name], b[name], err_msg=name)
+            np.testing.assert_array_equal(runs[0].engine.gate_flush(), runs[1].engine.gate_flush())
+        assert all(runs[1].engine.gate_state()['commanded'] == 1)
+        assert (runs[1].engine.get('bed') < bed0).sum() == 4 * 64  # every gate cell has moved down
+    finally:
+        for r in runs:
+            r.close()
