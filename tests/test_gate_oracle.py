@@ -3,7 +3,8 @@ time loop: the known answers of the reference's tests/test_gate_solver.py
 (bed motion, strict trigger, latching, independent gates, warmup, still
 water, bitwise restart, exchange and source accounting, hanging faces,
 limiter, replayed beds) and tests/test_gate_extended.py (large components,
-paired uniform/hanging sections)."""
+paired uniform/hanging sections, the refined dry-channel transient, the
+30,000 s command clock)."""
 import csv
 import functools
 
@@ -486,3 +487,39 @@ def test_disabled_and_never_triggered_gates_leave_the_step_bitwise_unchanged(tmp
         for field in ('depth', 'bed', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_speed'):
             assert getattr(base.state, field).tobytes() == getattr(r.state, field).tobytes(), (name, field)
     assert gate_of(results['idle'])['command_seconds'] is None
+
+
+def test_dry_multicell_transient_refines_first_water_volume_and_oscillation(tmp_path):
+    """A river cell 4 m deep beside a dry four-cell gate channel (bed 2 m,
+    opening to 0 m in 0.5 s) and a dry pond cell, for 16 s at step limits of
+    1/8, 1/16 and 1/32 s (tests/test_gate_extended.py:86-94,197-225): both
+    control volumes close, water first reaches the pond no later at the
+    finest step, and the pond volumes and the oscillation of the per-second
+    pond exchange converge."""
+    cells = [(4 * i, 4 * (i + 1), 0, 4) for i in range(6)]
+    measurements = []
+    for step in (.125, .0625, .03125):
+        path = tmp_path / str(step)
+        dc, force, *_ = setup(path, cells=cells, types=[1, 11, 11, 11, 11, 10], bed=[0., 2., 2., 2., 2., 0.],
+                              depth=[4., 0., 0., 0., 0., 0.],
+                              gate=dict(gates=[dict(name='A', inside_point=(6, 2), control_point=(2, 2))],
+                                        opening_seconds=.5, trigger_level=1., open_elevation=0.,
+                                        pond_land_type=10))
+        force = force.model_copy(update={'rainfall': type(force.rainfall)(**event_steps(path, step, 16., 24, 4))})
+        r = run(dc, force, 16.)
+        gate, pond = gate_of(r), pond_of(r)
+        assert_control_volume(pond, scale=100.)
+        assert_control_volume(gate['channel_budget'], scale=100.)
+        assert np.all(r.state.depth >= 0)
+        assert gate['first_effective_flow_seconds'] is not None
+        rows = [row for row in csv.DictReader((path / 'out/gate_balance.csv').open()) if row['region'] == 'A']
+        cumulative = np.array([float(row['pond_net_m3']) for row in rows])
+        measurements.append(dict(first_water_s=gate['first_effective_flow_seconds'], pond_in_m3=gate['pond_in_m3'],
+                                 pond_out_m3=gate['pond_out_m3'],
+                                 oscillation_m3=float(np.sum(np.abs(np.diff(np.diff(cumulative)))))))
+    coarse, middle, fine = measurements
+    assert fine['first_water_s'] <= coarse['first_water_s'] + .5
+    for key in ('pond_in_m3', 'pond_out_m3', 'oscillation_m3'):
+        assert np.isfinite([m[key] for m in measurements]).all()
+        assert abs(fine[key] - middle[key]) <= abs(middle[key] - coarse[key]) + .02
+    assert fine['pond_in_m3'] > 0
