@@ -6,7 +6,6 @@ import csv
 import hashlib
 import json
 import os
-import platform
 import subprocess
 import time
 from datetime import datetime, timedelta, timezone
@@ -178,7 +177,3 @@ class WaterBudget:
 
     def close(self):
         self.file.close()
-
-
-def host_device_name() -> str:
-    return platform.processor() or platform.machine()
