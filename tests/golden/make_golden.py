@@ -387,6 +387,48 @@ def filter_cases(ref, rng, work: Path):
     return out
 
 
+def hanging_gate_cases(ref, arrays):
+    """GateLayout.load on a refined quadtree: two gate strips (class 10) of
+    mixed 2 m and 1 m cells, joined within each strip through hanging
+    subedges, between river (1) and pond (11) cells."""
+    rng = np.random.default_rng(7)
+    mesh = quadtree(rng, 12, 8, 0.4)
+    cx, cy = mesh['centre'][:, 0], mesh['centre'][:, 1]
+    types_ = np.where(cx < 10, 1, 11).astype(np.uint8)
+    strip = (cx > 10) & (cx < 14)
+    types_[strip] = 1
+    types_[strip & ((cy < 6) | (cy > 10))] = 10
+    types_[0] = 0
+    bed = np.where(types_ == 10, 2.0, 0.5).astype(np.float32)
+    bed[0] = 0
+    for key, value in (('bounds', mesh['bounds']), ('topology', mesh['topology']), ('types', types_), ('bed', bed)):
+        arrays[f'hgate_{key}'] = value
+    low, high, river = ('low', (12.0, 3.0), (5.0, 3.0)), ('high', (11.0, 13.0), (5.0, 13.0)), (5.0, 8.0)
+    variants = [
+        dict(gates=[low, high]),
+        dict(gates=[('low', (12.0, 2.0), (10.0, 4.0)), ('high', (13.0, 11.0), (10.0, 16.0))]),
+        dict(gates=[low]),
+        dict(gates=[low, ('high', (11.0, 13.0), (12.0, 12.0))]),
+        dict(gates=[low, ('high', (12.0, 8.0), river)]),
+        dict(gates=[low, high], open_elevation=2.5),
+    ]
+    out = []
+    for v in variants:
+        config = NS(land_type=10, pond_land_type=11, open_elevation=v.get('open_elevation', 1.0),
+                    gates=[NS(name=n, inside_point=p, control_point=q) for n, p, q in v['gates']])
+        spec = dict(land_type=10, pond_land_type=11, open_elevation=config.open_elevation,
+                    gates=[dict(name=n, inside_point=list(p), control_point=list(q)) for n, p, q in v['gates']],
+                    overlap=False, level_cells=[])
+        try:
+            layout = ref.gate.GateLayout.load(config, NS(bounds=mesh['bounds']), types_, mesh['topology'], [], bed)
+        except ValueError as error:
+            out.append(dict(spec, error=str(error)))
+            continue
+        out.append(dict(spec, error=None, cell_gate=layout.cell_gate.tolist(), controls=layout.controls.tolist(),
+                        cells=[c.tolist() for c in layout.cells]))
+    return out
+
+
 # ---------------------------------------------------------------- clock, series, rain
 
 def tick_cases(ref, rng):
@@ -663,6 +705,7 @@ def main():
         golden['budget'] = budget_cases(ref, rng, Path(work))
         golden['report'] = report_cases(ref, rng, arrays, golden['gate'], Path(work))
         golden['filter'] = filter_cases(ref, rng, Path(work))
+    golden['hanging_gate'] = hanging_gate_cases(ref, arrays)
     (HERE / 'host_golden.json').write_text(json.dumps(golden, separators=(',', ':')) + '\n')
     np.savez_compressed(HERE / 'host_golden.npz', **arrays)
     summary = {k: (sum(c.get('error') is not None for c in v if isinstance(c, dict)), len(v))

@@ -80,10 +80,8 @@ def test_still_water_fill_matches_the_reference(case):
     assert meta == spec['meta']
 
 
-@pytest.mark.parametrize('case', range(len(CASES['gate'])))
-def test_gate_layout_matches_the_reference(case):
-    spec = CASES['gate'][case]
-    types_ = ARRAYS['gate_types'].copy()
+def check_gate_layout(spec, prefix):
+    types_ = ARRAYS[f'{prefix}_types'].copy()
     if spec['overlap']:
         types_[types_ == spec['land_type']] = spec['pond_land_type']
     config = NS(land_type=spec['land_type'], pond_land_type=spec['pond_land_type'],
@@ -91,7 +89,8 @@ def test_gate_layout_matches_the_reference(case):
                 gates=[NS(name=g['name'], inside_point=tuple(g['inside_point']),
                           control_point=tuple(g['control_point'])) for g in spec['gates']])
     boundaries = [NS(kind='level', cells=np.asarray(cells, dtype=np.int64)) for cells in spec['level_cells']]
-    args = (config, ARRAYS['gate_bounds'], types_, ARRAYS['gate_topology'], boundaries, ARRAYS['gate_bed'])
+    args = (config, ARRAYS[f'{prefix}_bounds'], types_, ARRAYS[f'{prefix}_topology'], boundaries,
+            ARRAYS[f'{prefix}_bed'])
     if spec['error'] is not None:
         with pytest.raises(ValueError) as error:
             GateLayout.load(*args)
@@ -101,6 +100,16 @@ def test_gate_layout_matches_the_reference(case):
     assert layout.cell_gate.tolist() == spec['cell_gate']
     assert layout.controls.tolist() == spec['controls']
     assert [c.tolist() for c in layout.cells] == spec['cells']
+
+
+@pytest.mark.parametrize('case', range(len(CASES['gate'])))
+def test_gate_layout_matches_the_reference(case):
+    check_gate_layout(CASES['gate'][case], 'gate')
+
+
+@pytest.mark.parametrize('case', range(len(CASES['hanging_gate'])))
+def test_gate_layout_through_hanging_subedges_matches_the_reference(case):
+    check_gate_layout(CASES['hanging_gate'][case], 'hgate')
 
 
 @pytest.mark.parametrize('case', range(len(CASES['configs'])))
