@@ -226,7 +226,10 @@ int nhf_gate_flush(nhf_handle *h, double *totals);
  * > 0 = that many blocks; -2 = member graphs: every member runs its own
  * batch graph (its own step form, tile size and CFL placement) on its own
  * stream, all members launched together; members then need to share only
- * the batch size. */
+ * the batch size. A member with a gate controller (nhf_gate_attach) runs
+ * only in the member-graph schedule: the one-launch step has no gate passes,
+ * so creating it with such a member fails with NHF_EINVAL, and a batch of it
+ * after a member attached one fails with NHF_ESTATE. */
 typedef struct nhf_ensemble nhf_ensemble;
 int nhf_ensemble_create(nhf_handle *const *members, int32_t n, int32_t grid_blocks, void *stream,
                         nhf_ensemble **out);

@@ -182,6 +182,10 @@ int nhf_ensemble_create(nhf_handle *const *members, int32_t n, int32_t grid_bloc
         const nhf_handle *h = members[i];
         if (!h) return efail(nullptr, NHF_EINVAL, "member %d is null", i);
         if (!h->tiled) return efail(nullptr, NHF_EINVAL, "member %d is not on the fused tiled step (%s)", i, h->path.c_str());
+        // the one-launch step has no gate passes: a gated member runs its own
+        // batch graph in the member-graph schedule
+        if (h->gate_on)
+            return efail(nullptr, NHF_EINVAL, "member %d has a gate controller; use the member-graph schedule", i);
         if (h->tb.plan.tile != tile) return efail(nullptr, NHF_EINVAL, "member %d has tile %d, member 0 has %d", i, h->tb.plan.tile, tile);
         if (h->p.batch_size != h0->p.batch_size) return efail(nullptr, NHF_EINVAL, "member %d has another batch size", i);
         if (h->dev.theta_one != h0->dev.theta_one) return efail(nullptr, NHF_EINVAL, "members mix theta = 1 and theta < 1");
@@ -307,6 +311,9 @@ int nhf_ensemble_run_batch_async(nhf_ensemble *e, const uint32_t *targets, const
         for (cudaStream_t st : e->streams) ECK(e, cudaStreamWaitEvent(st, e->ev_out, 0));
         return NHF_OK;
     }
+    for (int i = 0; i < n; ++i)
+        if (e->members[i]->gate_on)
+            return efail(e, NHF_ESTATE, "member %d has a gate controller attached after the one-launch ensemble was made", i);
     for (int i = 0; i < n; ++i) {
         e->h_words[4 * i] = targets[2 * i];
         e->h_words[4 * i + 1] = targets[2 * i + 1];

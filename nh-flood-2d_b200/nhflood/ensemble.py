@@ -70,7 +70,12 @@ class EnsembleRun:
             factory = tiled_factory(tile, device)
         self.tile, self.grid_blocks = tile, grid_blocks
         self.runs = [PlainRun(w, factory, batch_size=batch_size) for w in self.workloads]
-        self.ensemble = CudaEnsemble([r.engine for r in self.runs], grid_blocks)
+        try:
+            self.ensemble = CudaEnsemble([r.engine for r in self.runs], grid_blocks)
+        except Exception:
+            for r in self.runs:
+                r.close()
+            raise
         self.cells = np.array([w.cells for w in self.workloads], np.int64)
         self.h2d_bytes = 0
 

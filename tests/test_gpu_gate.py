@@ -206,3 +206,35 @@ def test_gated_polder_full_size_matches_the_oracle_batch_by_batch():
     finally:
         for r in runs:
             r.close()
+
+
+def test_gated_members_run_in_the_member_graph_schedule_only():
+    """A gated polder in an ensemble: the one-launch schedule, which has no
+    gate passes, refuses it; in the member-graph schedule, beside an ungated
+    member, it matches its own single run bit for bit, gate words and totals
+    included."""
+    from nhflood import workloads
+    from nhflood.ensemble import EnsembleRun
+    from nhflood.model import STATE_F32, STATE_U32
+    from nhflood.native import CudaEngine
+    from nhflood.plain import PlainRun
+    gated, plain = workloads.gated_polder(n=128, dx=40.0), workloads.plain_uniform_256(n=64)
+    with pytest.raises(RuntimeError, match='gate controller'):
+        EnsembleRun([plain, gated], tile=256, grid_blocks=-1)
+    ens, single = EnsembleRun([plain, gated]), PlainRun(gated, CudaEngine)
+    try:
+        assert ens.schedule == 'member graphs'
+        for _ in range(4):
+            completed = ens.advance()
+            assert completed[1] == single.advance() > 0
+            member = ens.runs[1].engine
+            for name in STATE_F32 + STATE_U32:
+                assert member.get(name).tobytes() == single.engine.get(name).tobytes(), name
+            a, b = member.gate_state(), single.engine.gate_state()
+            for name in a:
+                np.testing.assert_array_equal(a[name], b[name], err_msg=name)
+            np.testing.assert_array_equal(member.gate_flush(), single.engine.gate_flush())
+        assert all(member.gate_state()['commanded'] == 1)
+    finally:
+        ens.close()
+        single.close()
