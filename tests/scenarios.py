@@ -243,3 +243,16 @@ def two_cell_case(path: Path, bands, duration, *, land_type=10, q=0., warmup=0, 
                 land={land_type: dict(manning_n=.03, infiltration=infiltration)}, stations=stations)
     fc = ForceConfig(boundaries=boundaries, rainfall=rain)
     return dc, fc
+
+
+def all_cells_filtered(path: Path):
+    """The two-cell rain case with both cells marked z = -9999: the NE/NS
+    filter leaves no cell and no side, only the sentinels."""
+    dc, fc = two_cell_case(path, [[6, 6]], 10)
+    lines = []
+    for line in (path / 'ne.txt').read_text().splitlines():
+        fields = line.split(',')
+        fields[-2] = '-9999'
+        lines.append(','.join(fields))
+    (path / 'ne.txt').write_text('\n'.join(lines) + '\n')
+    return dc, fc

@@ -14,7 +14,8 @@ import numpy as np
 import pytest
 
 from runner import run
-from scenarios import grid3_mesh, grid_cell, grid_horizontal, grid_vertical, seed_checkpoint, two_cell_case, domain
+from scenarios import (all_cells_filtered, domain, grid3_mesh, grid_cell, grid_horizontal, grid_vertical,
+                       seed_checkpoint, two_cell_case)
 
 pytestmark = pytest.mark.gpu
 
@@ -243,3 +244,20 @@ def test_full_size_configurations_bit_exact(cuda_available, name, batches):
     finally:
         for run in runs:
             run.close()
+
+
+def test_mesh_without_cells_runs_like_the_oracle(tmp_path, cuda_available):
+    """Every cell filtered out: the engine takes the multi-pass step (no
+    tiles to plan) and runs the same ten empty steps as the oracle."""
+    from nhflood.native import CudaEngine
+    paths = []
+
+    def factory(arrays, params):
+        engine = CudaEngine(arrays, params)
+        paths.append(engine.path)
+        return engine
+    results = [run(*all_cells_filtered(tmp_path / name), engine)
+               for name, engine in (('oracle', 'oracle'), ('cuda', factory))]
+    assert paths == ['multipass (mesh has no cells)']
+    assert_runs_identical(*results)
+    assert results[0].manifest['steps'] == 10 and len(results[0].state.depth) == 1

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from runner import run
-from scenarios import two_cell_case
+from scenarios import all_cells_filtered, two_cell_case
 
 ORACLE = 'oracle'
 
@@ -218,3 +218,12 @@ def test_subsecond_level_knot_and_between_frame_peak(tmp_path):
     assert all(read_depth_frame(p)[2] < 2e-6 for _, p in list_depth_frames(root))
     peak = (int(extrema.first_time_hi[2]) * 2 ** 32 + int(extrema.first_time_lo[2])) / 2 ** 40
     assert peak == pytest.approx(.000002, abs=5e-13)
+
+
+def test_mesh_without_cells_runs_with_zero_storage(tmp_path):
+    """Every cell filtered out (z = -9999): the reference's loops run over
+    empty ranges, so the run completes at dt = 1 s with nothing stored."""
+    r = run(*all_cells_filtered(tmp_path), 'oracle')
+    assert r.manifest['steps'] == 10 and r.manifest['status'] == 'completed'
+    assert len(r.state.depth) == 1
+    assert r.budget['storage_m3'] == 0 and r.budget['residual_m3'] == 0
