@@ -9,8 +9,14 @@
  * The reference itself is Python + Taichi JIT kernels and cannot run here
  * (taichi 1.7.4 / fastdb4py 0.2.4 are not installed). Parity with Taichi's
  * own floating-point lowering is therefore pinned only through the
- * reference tests' known answers (tests/test_oracle_pins.py); bit-level
- * agreement with a Taichi CPU run is unpinned.
+ * reference tests' known answers (tests/test_oracle_pins.py,
+ * tests/test_oracle_physics.py, tests/test_oracle_clock.py,
+ * tests/test_oracle_restart.py, tests/test_gate_oracle.py); bit-level
+ * agreement with a Taichi CPU run is unpinned. The host-side inputs the
+ * step consumes (land parameters, hanging-edge tables, face fractions,
+ * still-water depths, gate layout, clock ticks, series and rain rates) are
+ * pinned bit for bit to the reference's own code by the golden vectors in
+ * tests/golden/ (tests/test_golden_host.py).
  *
  * Differences from the reference that are deliberate (north-star design):
  *  - budget diagnostics are accumulated as FP64 per-block partials
