@@ -88,6 +88,8 @@ def load_reference(root: Path):
     ref.pressure = NS(**definitions(pkg / 'core/pressure.py', ['HangingGeometry', 'hanging_geometry'],
                                     dict(np=np, dataclass=dataclass)))
     ref.domain = definitions(pkg / 'preprocess/domain.py', ['_filter_ne_ns'], dict(Path=Path))
+    output_names = ['STATION_FIELDS', '_float_array', '_uint_array', 'append_station_samples']
+    ref.output = NS(**definitions(pkg / 'core/output.py', output_names, dict(np=np, csv=csv, Path=Path)))
     return ref
 
 
@@ -429,6 +431,33 @@ def hanging_gate_cases(ref, arrays):
     return out
 
 
+def output_cases(ref, work: Path):
+    """The checkpoint and frame array rules and stations.csv rows."""
+    values = [[0.0, 1.5, -2.25], [], [[1.0, 2.0]], [1.0, float('nan')], [1.0, float('inf')], [1e39], [0, 1, 4294967295],
+              [0, 4294967296], [-1, 2], [1.5, 2.0], [True, False], [7], [3.0, 4.0], 5]
+    arrays = []
+    for value in values:
+        case = dict(value=[repr(v) if isinstance(v, float) else v for v in value] if isinstance(value, list) else value)
+        for kind, check in (('float', ref.output._float_array), ('uint', ref.output._uint_array)):
+            try:
+                result = check(value if not isinstance(value, list) else np.array(value), 'field')
+                case[kind] = dict(dtype=str(result.dtype), values=result.tolist())
+            except ValueError as error:
+                case[kind] = dict(error=str(error))
+        arrays.append(case)
+    path = work / 'stations.csv'
+    rng = np.random.default_rng(11)
+    for k in range(3):
+        samples = {name: dict(cell_id=int(rng.integers(1, 1000)), depth=float(np.float32(rng.uniform(0, 2))),
+                              level=float(rng.uniform(-5, 20)), u=float(rng.normal()), v=float(rng.normal()))
+                   for name in rng.permutation(['gauge_b', 'Gauge_a', 'gauge_c', 'z1'])[:int(rng.integers(1, 5))]}
+        ref.output.append_station_samples(path, elapsed_seconds=300 * k, time=f'2023-09-07T08:{5 * k:02d}:00+00:00',
+                                          samples=samples)
+        arrays.append(dict(stations_call=dict(elapsed_seconds=300 * k, time=f'2023-09-07T08:{5 * k:02d}:00+00:00',
+                                              samples=samples)))
+    return dict(cases=arrays, stations_csv=path.read_text())
+
+
 # ---------------------------------------------------------------- clock, series, rain
 
 def tick_cases(ref, rng):
@@ -705,6 +734,7 @@ def main():
         golden['budget'] = budget_cases(ref, rng, Path(work))
         golden['report'] = report_cases(ref, rng, arrays, golden['gate'], Path(work))
         golden['filter'] = filter_cases(ref, rng, Path(work))
+        golden['output'] = output_cases(ref, Path(work))
     golden['hanging_gate'] = hanging_gate_cases(ref, arrays)
     (HERE / 'host_golden.json').write_text(json.dumps(golden, separators=(',', ':')) + '\n')
     np.savez_compressed(HERE / 'host_golden.npz', **arrays)

@@ -268,3 +268,34 @@ def test_native_preprocessing_builds_the_tables_of_the_reference_filter(case):
         assert actual.keys() == expected.keys()
         for key in actual:
             same_bits(actual[key], np.asarray(expected[key]))
+
+
+def golden_value(value):
+    if isinstance(value, list):
+        return np.array([golden_value(v) for v in value])
+    return float(value) if isinstance(value, str) else value
+
+
+@pytest.mark.parametrize('case', [c for c in CASES['output']['cases'] if 'value' in c], ids=lambda c: str(c['value']))
+def test_output_array_rules_match_the_reference(case):
+    """The F32 and U32 array rules of the checkpoint, frame and extrema
+    writers accept and reject what the reference's do, with its messages."""
+    from nhflood.output import _float_array, _uint_array
+    for kind, check in (('float', _float_array), ('uint', _uint_array)):
+        expected = case[kind]
+        if 'error' in expected:
+            with pytest.raises(ValueError) as error:
+                check(golden_value(case['value']), 'field')
+            assert str(error.value) == expected['error']
+        else:
+            result = check(golden_value(case['value']), 'field')
+            assert str(result.dtype) == expected['dtype'] and result.tolist() == expected['values']
+
+
+def test_station_rows_match_the_reference(tmp_path):
+    from nhflood.output import append_station_samples
+    path = tmp_path / 'stations.csv'
+    for case in CASES['output']['cases']:
+        if 'stations_call' in case:
+            append_station_samples(path, **case['stations_call'])
+    assert path.read_text() == CASES['output']['stations_csv']
