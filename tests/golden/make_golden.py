@@ -7,9 +7,13 @@ Three parts of nh-flood-2d run without Taichi, rasterio or fastdb4py:
     connected_still_water (the warm-up fill);
   * preprocess/gate.py – GateLayout.load (gate components, control cells,
     validation);
-  * input/domain.py, input/force.py – the config schema and absolute_time.
-This script imports those modules unchanged from a reference checkout,
-feeds them seeded synthetic meshes and configs, and writes what they return
+  * input/domain.py, input/force.py – the config schema and absolute_time;
+and, from files that import Taichi, rasterio or fastdb4py at the top, the
+plain-Python definitions of core/clock.py, core/pressure.py,
+preprocess/domain.py, preprocess/force.py, core/run_record.py, core/gate.py
+and core/output.py, compiled from their unchanged source (``definitions``).
+The script runs that code from a reference checkout, feeds it seeded
+synthetic meshes, configs and states, and writes what it returns
 (or the error they raise) to host_golden.json and host_golden.npz next to
 it. tests/test_golden_host.py replays every case through nhflood.
 

@@ -3,8 +3,9 @@ ran nh-flood-2d's preprocess/hydraulics.py, preprocess/gate.py and
 input/*.py, and the plain-Python definitions of core/clock.py (tick
 conversion), core/pressure.py (hanging_geometry), preprocess/domain.py
 (_filter_ne_ns), preprocess/force.py (TimeSeries, RainField),
-core/run_record.py (WaterBudget) and core/gate.py (GateController.report,
-append_gate_balance) on seeded meshes, configs and controller states. Every case is replayed
+core/run_record.py (WaterBudget), core/gate.py (GateController.report,
+append_gate_balance) and core/output.py (array rules, station rows) on
+seeded meshes, configs and controller states. Every case is replayed
 through nhflood: arrays must match bit for bit, errors by message, configs
 by acceptance, error locations and the validated dump, CSV files byte for
 byte."""
