@@ -78,9 +78,11 @@ class HostClock:
         status = np.asarray(rows)[:, 3]
         stops = np.flatnonzero(status != COMPLETED)
         n = int(stops[0]) if len(stops) else len(rows)
-        if n < len(rows) and int(status[n]) not in (BAD_CFL, BAD_DT, OVERSHOOT, DONE):
-            raise RuntimeError(f'Unknown clock trace status {int(status[n])}')
         if n:
             self.now_ticks = ticks_of(rows[n - 1][1], rows[n - 1][2])
+        # an unknown status is refused after the completed rows before it
+        # have advanced the clock, and the batch stays pending
+        if n < len(rows) and int(status[n]) not in (BAD_CFL, BAD_DT, OVERSHOOT, DONE):
+            raise RuntimeError(f'Unknown clock trace status {int(status[n])}')
         self.pending = False
         return rows

@@ -462,6 +462,84 @@ def output_cases(ref, work: Path):
     return dict(cases=arrays, stations_csv=path.read_text())
 
 
+class ClockField:
+    """A stand-in for a device field of StepClock: it keeps what is uploaded
+    and returns the trace rows it is given."""
+
+    def __init__(self):
+        self.value, self.rows = None, None
+
+    def from_numpy(self, array):
+        self.value = np.array(array)
+
+    def fill(self, value):
+        self.value = value
+
+    def to_numpy(self):
+        return np.array(self.rows, dtype=np.uint32)
+
+
+def trace_rows(start_ticks, statuses, rng):
+    """Trace rows whose completed steps end at increasing tick counts."""
+    rows, now = [], start_ticks
+    for status in statuses:
+        row = [0] * 10
+        row[3] = status
+        if status == 1:
+            now += int(rng.integers(1, 1 << 40))
+            row[1], row[2] = now >> 32, now & 0xffffffff
+        rows.append(row)
+    return rows
+
+
+def clock_protocol_cases(ref, pkg: Path):
+    """StepClock.begin / read_trace (core/clock.py:71-92,187-203) on a
+    stand-in clock: the words uploaded, the host tick mirror and the errors."""
+    names = dict(math=math, np=np, _seconds_to_ticks=ref.clock._seconds_to_ticks, _words=ref.clock._words,
+                 _TICKS_PER_SECOND=ref.clock._TICKS_PER_SECOND)
+    fns = definitions(pkg / 'core/clock.py', ['host_now_seconds', 'begin', 'read_trace'], names, inside='StepClock')
+
+    class Clock:
+        DONE, COMPLETED, BAD_CFL, BAD_DT, OVERSHOOT = 0, 1, 2, 3, 4
+        host_now_seconds = property(fns['host_now_seconds'])
+        begin, read_trace = fns['begin'], fns['read_trace']
+
+        def __init__(self, seconds):
+            self._host_now_ticks = ref.clock._seconds_to_ticks(seconds)
+            self._batch_pending = False
+            self.next, self.origin, self.trace = ClockField(), ClockField(), ClockField()
+
+    rng = np.random.default_rng(13)
+    out = []
+    for initial, script in [
+        (0.0, [('begin', 10.0, 0.0), ('trace', [1, 1, 1, 0, 0]), ('begin', 20.0, 'now'), ('trace', [1] * 32)]),
+        (0.0, [('begin', 10.0, 2e-6), ('begin', 10.0, 5e-7), ('begin', 11.0, 0.0)]),
+        (1234.5, [('begin', 1234.0, 1234.5), ('begin', 1234.5, 1234.5 + 1e-7), ('trace', [0] * 4)]),
+        (0.0, [('trace', [1, 0]), ('begin', 5.0, math.nan), ('begin', 5.0, 0.0), ('trace', [1, 2, 1])]),
+        (7.25, [('begin', 9.0, 7.25), ('trace', [1, 1, 9, 1]), ('begin', 9.0, 'now'), ('trace', [1, 3])]),
+        (0.0, [('begin', 3.0, 0.0), ('trace', [1, 4, 0]), ('begin', 3.0, 'now'), ('trace', [1, 1, 5])]),
+    ]:
+        clock, steps = Clock(initial), []
+        for op in script:
+            step = dict(op=op[0])
+            try:
+                if op[0] == 'begin':
+                    origin = clock.host_now_seconds if op[2] == 'now' else op[2]
+                    step.update(target=op[1], origin=repr(float(origin)))
+                    clock.begin(op[1], origin)
+                    step.update(next=clock.next.value.tolist(), origin_words=clock.origin.value.tolist())
+                else:
+                    clock.trace.rows = trace_rows(clock._host_now_ticks, op[1], rng)
+                    step.update(rows=clock.trace.rows)
+                    clock.read_trace()
+            except (ValueError, RuntimeError) as error:
+                step.update(error=type(error).__name__, message=str(error))
+            step.update(now=str(clock._host_now_ticks), pending=clock._batch_pending)
+            steps.append(step)
+        out.append(dict(initial=initial, steps=steps))
+    return out
+
+
 # ---------------------------------------------------------------- clock, series, rain
 
 def tick_cases(ref, rng):
@@ -740,6 +818,7 @@ def main():
         golden['filter'] = filter_cases(ref, rng, Path(work))
         golden['output'] = output_cases(ref, Path(work))
     golden['hanging_gate'] = hanging_gate_cases(ref, arrays)
+    golden['clock_protocol'] = clock_protocol_cases(ref, args.reference / 'src' / 'nh_flood_2d')
     (HERE / 'host_golden.json').write_text(json.dumps(golden, separators=(',', ':')) + '\n')
     np.savez_compressed(HERE / 'host_golden.npz', **arrays)
     summary = {k: (sum(c.get('error') is not None for c in v if isinstance(c, dict)), len(v))

@@ -301,3 +301,26 @@ def test_station_rows_match_the_reference(tmp_path):
         if 'stations_call' in case:
             append_station_samples(path, **case['stations_call'])
     assert path.read_text() == CASES['output']['stations_csv']
+
+
+@pytest.mark.parametrize('case', range(len(CASES['clock_protocol'])))
+def test_batch_clock_protocol_matches_the_reference(case):
+    """HostClock.begin / read_trace against StepClock.begin / read_trace:
+    the uploaded target and origin words, the host tick mirror, the pending
+    flag and every refusal, step by step."""
+    from nhflood.clock import HostClock
+    spec = CASES['clock_protocol'][case]
+    clock = HostClock(spec['initial'])
+    for step in spec['steps']:
+        try:
+            if step['op'] == 'begin':
+                target_words, origin_words = clock.begin(step['target'], float(step['origin']))
+            else:
+                clock.read_trace(np.array(step['rows'], dtype=np.uint32))
+        except (ValueError, RuntimeError) as error:
+            assert (type(error).__name__, str(error)) == (step.get('error'), step.get('message')), step
+        else:
+            assert 'error' not in step, step
+            if step['op'] == 'begin':
+                assert target_words.tolist() == step['next'] and origin_words.tolist() == step['origin_words']
+        assert (clock.now_ticks, clock.pending) == (int(step['now']), step['pending']), step
