@@ -1,7 +1,7 @@
 """Golden vectors from the reference's own code. tests/golden/make_golden.py
 ran nh-flood-2d's preprocess/hydraulics.py, preprocess/gate.py and
 input/*.py, and the plain-Python definitions of core/clock.py (tick
-conversion), core/pressure.py (hanging_geometry), preprocess/domain.py
+conversion, batch begin and trace read-back), core/pressure.py (hanging_geometry), preprocess/domain.py
 (_filter_ne_ns), preprocess/force.py (TimeSeries, RainField),
 core/run_record.py (WaterBudget), core/gate.py (GateController.report,
 append_gate_balance) and core/output.py (array rules, station rows) on
