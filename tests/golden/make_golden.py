@@ -92,7 +92,7 @@ def load_reference(root: Path):
     ref.pressure = NS(**definitions(pkg / 'core/pressure.py', ['HangingGeometry', 'hanging_geometry'],
                                     dict(np=np, dataclass=dataclass)))
     ref.domain = definitions(pkg / 'preprocess/domain.py', ['_filter_ne_ns'], dict(Path=Path))
-    output_names = ['STATION_FIELDS', '_float_array', '_uint_array', 'append_station_samples']
+    output_names = ['STATION_FIELDS', '_float_array', '_uint_array', 'append_station_samples', 'list_depth_frames']
     ref.output = NS(**definitions(pkg / 'core/output.py', output_names, dict(np=np, csv=csv, Path=Path)))
     return ref
 
@@ -459,7 +459,20 @@ def output_cases(ref, work: Path):
                                           samples=samples)
         arrays.append(dict(stations_call=dict(elapsed_seconds=300 * k, time=f'2023-09-07T08:{5 * k:02d}:00+00:00',
                                               samples=samples)))
-    return dict(cases=arrays, stations_csv=path.read_text())
+    frame_sets = [['depth_900.fdb', 'depth_0.fdb', 'depth_10800.fdb', 'depth_2700.fdb'], ['depth_0900.fdb', 'depth_-5.fdb'],
+                  ['depth_1e3.fdb'], ['depth_.fdb'], [], ['depth_300.fdb', 'other.fdb', 'depth_300.txt']]
+    frames = []
+    for k, names in enumerate(frame_sets):
+        root = work / f'frames{k}'
+        (root / 'frames').mkdir(parents=True)
+        for name in names:
+            (root / 'frames' / name).write_bytes(b'')
+        try:
+            listed = [[seconds, Path(p).name] for seconds, p in ref.output.list_depth_frames(root)]
+            frames.append(dict(names=names, listed=listed))
+        except ValueError as error:
+            frames.append(dict(names=names, error=str(error).replace(str(root), '{root}')))
+    return dict(cases=arrays, stations_csv=path.read_text(), frames=frames)
 
 
 class ClockField:

@@ -324,3 +324,17 @@ def test_batch_clock_protocol_matches_the_reference(case):
             if step['op'] == 'begin':
                 assert target_words.tolist() == step['next'] and origin_words.tolist() == step['origin_words']
         assert (clock.now_ticks, clock.pending) == (int(step['now']), step['pending']), step
+
+
+@pytest.mark.parametrize('case', CASES['output']['frames'], ids=lambda c: ','.join(c['names']) or 'none')
+def test_depth_frame_listing_matches_the_reference(tmp_path, case):
+    from nhflood.output import list_depth_frames
+    (tmp_path / 'frames').mkdir()
+    for name in case['names']:
+        (tmp_path / 'frames' / name).write_bytes(b'')
+    if 'error' in case:
+        with pytest.raises(ValueError) as error:
+            list_depth_frames(tmp_path)
+        assert str(error.value) == case['error'].replace('{root}', str(tmp_path))
+    else:
+        assert [[seconds, path.name] for seconds, path in list_depth_frames(tmp_path)] == case['listed']
