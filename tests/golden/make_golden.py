@@ -82,6 +82,7 @@ def load_reference(root: Path):
              input=importlib.import_module('nh_flood_2d.input'),
              force=importlib.import_module('nh_flood_2d.input.force'))
     pkg = src / 'nh_flood_2d'
+    ref.pkg = pkg
     ref.clock = NS(**definitions(pkg / 'core/clock.py', ['_TICKS_PER_SECOND', '_MAX_TICKS', '_seconds_to_ticks',
                                                          '_words'], dict(math=math, np=np)))
     ref.series = NS(**definitions(pkg / 'preprocess/force.py', ['TimeSeries', 'RainField'],
@@ -472,7 +473,41 @@ def output_cases(ref, work: Path):
             frames.append(dict(names=names, listed=listed))
         except ValueError as error:
             frames.append(dict(names=names, error=str(error).replace(str(root), '{root}')))
-    return dict(cases=arrays, stations_csv=path.read_text(), frames=frames)
+    return dict(cases=arrays, stations_csv=path.read_text(), frames=frames, timelines=bed_timeline_cases(ref))
+
+
+def bed_timeline_cases(ref):
+    """BedTimeline.at (core/output.py:299-343) over seeded bed events and gate
+    openings; the base bed comes from a stand-in for the bed.fdb reader."""
+    rng = np.random.default_rng(17)
+    out = []
+    for case in range(3):
+        n = 24
+        bed = rng.uniform(-2, 5, n).astype(np.float32)
+        bed[0] = 0
+        events = [dict(elapsed_seconds=float(t), cell_ids=rng.choice(np.arange(1, n), 3, replace=False).tolist(),
+                       new_bed=[float(np.float32(v)) for v in rng.uniform(-3, 3, 3)])
+                  for t in rng.permutation([0.0, 450.0, 1200.5, 3600.0])]
+        origin = float(rng.choice([0.0, 1800.0, 7.125]))
+        formal = round(origin * 2 ** 40)
+        gates = []
+        for g in range(2):
+            cells = list(range(3 + 8 * g, 7 + 8 * g))
+            command = None if (case, g) == (1, 1) else float(rng.uniform(0, 900))
+            ticks = None if command is None else formal + round(command * 2 ** 40)
+            gates.append(dict(cell_ids=cells, closed_elevation=[float(bed[c]) for c in cells], command_seconds=command,
+                              command_clock_ticks=None if ticks is None else [ticks >> 32, ticks & 0xffffffff]))
+        manifest = dict(bed_events=events, gate_control=dict(gates=gates, clock_origin_before_start_s=origin,
+                                                              opening_seconds=float(rng.uniform(60, 1200)),
+                                                              open_elevation=-1.0))
+        names = dict(np=np, Path=Path, json=json, _uint_array=ref.output._uint_array,
+                     _float_array=ref.output._float_array, read_bed=lambda path, count, b=bed: b.copy())
+        timeline_class = definitions(ref.pkg / 'core/output.py', ['read_manifest', 'BedTimeline'], names)['BedTimeline']
+        timeline = timeline_class('output', manifest)
+        times = [0.0, 100.0, 450.0, 700.25, 1200.5, 2000.0, 3600.0, 9000.0]
+        out.append(dict(bed=bed.tolist(), manifest=manifest, times=times,
+                        beds=[timeline.at(t).astype(np.float32).tolist() for t in times]))
+    return out
 
 
 class ClockField:

@@ -338,3 +338,15 @@ def test_depth_frame_listing_matches_the_reference(tmp_path, case):
         assert str(error.value) == case['error'].replace('{root}', str(tmp_path))
     else:
         assert [[seconds, path.name] for seconds, path in list_depth_frames(tmp_path)] == case['listed']
+
+
+@pytest.mark.parametrize('case', range(len(CASES['output']['timelines'])))
+def test_bed_timeline_matches_the_reference(tmp_path, case):
+    """Frame-time beds: recorded bed events, then the gate beds re-derived
+    with the F32 opening arithmetic, bit for bit at every frame time."""
+    from nhflood.output import BedTimeline, write_bed
+    spec = CASES['output']['timelines'][case]
+    write_bed(tmp_path / 'output' / 'bed.fdb', np.array(spec['bed'], dtype=np.float32))
+    timeline = BedTimeline(tmp_path / 'output', spec['manifest'])
+    for seconds, expected in zip(spec['times'], spec['beds']):
+        same_bits(timeline.at(seconds).astype(np.float32), np.array(expected, dtype=np.float32))
