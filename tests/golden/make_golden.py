@@ -17,7 +17,7 @@ synthetic meshes, configs and states, and writes what it returns
 (or the error they raise) to host_golden.json and host_golden.npz next to
 it. tests/test_golden_host.py replays every case through nhflood.
 
-    python tests/golden/make_golden.py [--reference PATH]
+    python tests/golden/make_golden.py --reference PATH   (or NHF_REFERENCE=PATH)
 
 The reference's preprocess/__init__.py imports its Taichi domain pass, so
 the package object is registered without running that file; the two
@@ -32,6 +32,7 @@ import csv
 import importlib
 import json
 import math
+import os
 import sys
 import types
 from collections import defaultdict
@@ -845,8 +846,12 @@ def config_cases(ref, work: Path):
 def main():
     import tempfile
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    parser.add_argument('--reference', type=Path, default=Path('/root/reference'))
+    parser.add_argument('--reference', type=Path, default=os.environ.get('NHF_REFERENCE'),
+                        help='a checkout of nh-flood-2d (or set NHF_REFERENCE)')
     args = parser.parse_args()
+    if args.reference is None:
+        parser.error('give --reference PATH or set NHF_REFERENCE')
+    args.reference = Path(args.reference)
     ref = load_reference(args.reference)
     rng = np.random.default_rng(20261204)
     arrays = {}

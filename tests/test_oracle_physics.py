@@ -153,7 +153,7 @@ def test_one_cell_caches_both_axes_and_reconstructs_linear_plane(tmp_path):
 
 # ------------------------------------------------- coarse/fine channel flow
 
-def channel_case(path: Path, theta: float, engine='oracle'):
+def channel_case(path: Path, theta: float, engine='oracle', end_time=None):
     path.mkdir(parents=True)
     cells = channel_cells()
     bed = np.r_[0, [10 - .002 * (x0 + x1) / 2 for x0, x1, _, _ in cells]].astype(np.float32)
@@ -172,7 +172,7 @@ def channel_case(path: Path, theta: float, engine='oracle'):
     sampled = [(i, c) for i, c in enumerate(cells, 1) if c == (510, 512, 0, 2) or c[:2] == (512, 513)]
     stations = {str(i): ((x0 + x1) / 2, (y0 + y1) / 2) for i, (x0, x1, y0, y1) in sampled}
     dc = domain(path, duration=duration, yield_step=300, restart=seed, stations=stations, sita=theta)
-    r = run(dc, ForceConfig(boundaries=boundaries, rainfall=rain), engine)
+    r = run(dc, ForceConfig(boundaries=boundaries, rainfall=rain), engine, end_time=end_time)
     samples = list(csv.DictReader((Path(dc.output_dir) / 'stations.csv').open(newline='')))
     return cells, r, samples
 
@@ -209,7 +209,7 @@ def test_coarse_fine_channel_reaches_continuous_steady_flow(tmp_path, theta):
 PERIOD = 86_400
 
 
-def open_boundary_case(path: Path, kind: str, theta: float, afa: float, engine='oracle'):
+def open_boundary_case(path: Path, kind: str, theta: float, afa: float, engine='oracle', end_time=None):
     """A flat 40 x 2 strip: a channel between a 10 m3/s inflow and a 1 m level
     (10 m cells, 6000 s), or a basin driven by a daily 1 m tide at its west
     edge (100 m cells, two days); tests/test_open_boundary.py:135-205."""
@@ -234,7 +234,7 @@ def open_boundary_case(path: Path, kind: str, theta: float, afa: float, engine='
     seed = seed_checkpoint(path / 'seed.fdb', path / 'ne.txt', path / 'ns.txt', depth=depth)
     dc = domain(path, duration=duration, yield_step=500 if kind == 'channel' else 600, restart=seed,
                 sita=theta, afa=afa)
-    r = run(dc, ForceConfig(boundaries=boundaries, rainfall=rain), engine)
+    r = run(dc, ForceConfig(boundaries=boundaries, rainfall=rain), engine, end_time=end_time)
     from nhflood.output import list_depth_frames
     return r, list_depth_frames(dc.output_dir), nx, ny, Path(dc.output_dir)
 
