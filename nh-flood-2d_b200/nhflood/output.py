@@ -1,13 +1,22 @@
-"""Frames, extrema, checkpoints and station samples (host I/O only).
+"""Solver outputs on disk: the bed, depth frames, extrema, checkpoints,
+station samples, the manifest, and the bed replay of frame times.
 
-Same file names, table names and columns as the reference's core/output.py
-(lines 20-348); the container is nhflood.fdb (same schema, own byte format).
+What is shared with nh-flood-2d (core/output.py), so that downstream tools
+and restart files carry over: the file names, the FDB table names and
+columns, the stations.csv columns, and which arrays are accepted or refused,
+with the same messages. The container bytes are nhflood.fdb's own format.
+
+Every FDB file kind is described once, as a layout: an ordered list of
+(feature, table) pairs. ``_store`` writes the arrays of a layout and
+``_fetch`` reads them back. The functions below only validate and assemble.
 """
 from __future__ import annotations
 
 import csv
 import json
 import os
+import re
+from collections import deque
 from dataclasses import dataclass
 from pathlib import Path
 
@@ -16,10 +25,122 @@ import numpy as np
 from . import fdb
 
 STATION_FIELDS = ('elapsed_seconds', 'time', 'station', 'cell_id', 'depth', 'level', 'u', 'v')
-_CHECKPOINT_FLOATS = ('depth', 'bed', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_speed')
-_CHECKPOINT_INTS = ('clock_hi', 'clock_lo', 'gate_open')
-_CHECKPOINT_TIME = ('first_time_hi', 'first_time_lo')
+_U32_MAX = 0xFFFFFFFF
 
+
+# ------------------------------------------------------------ array rules
+# Acceptance rules of a stored array (core/output.py:53-66): F32 arrays are
+# finite and one-dimensional; U32 arrays are one-dimensional whole numbers in
+# [0, 2**32).
+
+def _float_array(value, name):
+    array = np.asarray(value, dtype=np.float32)
+    if array.ndim == 1 and bool(np.isfinite(array).all()):
+        return array
+    raise ValueError(f'{name} must be a finite one-dimensional F32 array')
+
+
+def _uint_array(value, name):
+    array = np.asarray(value)
+    valid = array.ndim == 1 and np.issubdtype(array.dtype, np.number)
+    if valid:
+        whole = np.isfinite(array).all() and (array == np.floor(array)).all()
+        valid = bool(whole and (array >= 0).all() and (array <= _U32_MAX).all())
+    if not valid:
+        raise ValueError(f'{name} must be a one-dimensional U32 array')
+    return array.astype(np.uint32)
+
+
+# ---------------------------------------------------------------- layouts
+
+_COLUMN = {'F32Value': 'value', 'IndexLike': 'index', 'U8Value': 'value'}
+
+
+@dataclass(frozen=True)
+class _Table:
+    feature: str
+    name: str
+
+    @property
+    def column(self) -> str:
+        return _COLUMN[self.feature]
+
+
+def _f32(*names):
+    return tuple(_Table('F32Value', n) for n in names)
+
+
+def _u32(*names):
+    return tuple(_Table('IndexLike', n) for n in names)
+
+
+_CELL_F32 = ('depth', 'bed', 'rain_time', 'infiltration', 'max_depth', 'max_speed')
+_STATE_F32 = ('depth', 'bed', 'q', 'rain_time', 'infiltration', 'max_depth', 'max_speed')
+_SCALARS = ('clock_hi', 'clock_lo', 'gate_open')
+_TIMES = ('first_time_hi', 'first_time_lo')
+
+BED_LAYOUT = _f32('bed')
+FRAME_LAYOUT = _f32('depth')
+EXTREMA_LAYOUT = _f32('max_depth', 'max_speed') + _u32(*_TIMES)
+CHECKPOINT_LAYOUT = _f32(*_STATE_F32) + _u32(*_SCALARS) + _u32(*_TIMES) + (_Table('U8Value', 'state_meta'),)
+
+
+def _store(path, layout, arrays: dict) -> None:
+    fdb.save(path, [(t.feature, t.name, {t.column: arrays[t.name]}) for t in layout])
+
+
+def _fetch(path, layout) -> dict:
+    db = fdb.load(path)
+    return {t.name: db.table(t.feature, t.name)[t.column] for t in layout}
+
+
+def _counted(path, name, values, expected_count):
+    if expected_count is not None and len(values) != expected_count:
+        raise ValueError(f'{path}: {name} has {len(values)} rows, expected {expected_count}')
+    return values
+
+
+# --------------------------------------------------------- bed and frames
+
+def write_bed(path, bed):
+    _store(path, BED_LAYOUT, {'bed': _float_array(bed, 'bed')})
+
+
+def read_bed(path, expected_count=None):
+    return _counted(path, 'bed', _fetch(path, BED_LAYOUT)['bed'], expected_count)
+
+
+def write_depth_frame(path, depth):
+    values = _float_array(depth, 'depth')
+    if (values < 0).any():
+        raise ValueError('depth must be nonnegative')
+    _store(path, FRAME_LAYOUT, {'depth': values})
+
+
+def read_depth_frame(path, expected_count=None):
+    values = _counted(path, 'depth', _fetch(path, FRAME_LAYOUT)['depth'], expected_count)
+    if not np.isfinite(values).all() or (values < 0).any():
+        raise ValueError(f'{path}: invalid depth frame')
+    return values
+
+
+_FRAME_NAME = re.compile(r'depth_(.*)')
+
+
+def list_depth_frames(output_root):
+    """(elapsed seconds, path) of every frames/depth_<seconds>.fdb, by time."""
+    found = []
+    for path in (Path(output_root) / 'frames').glob('depth_*.fdb'):
+        label = _FRAME_NAME.fullmatch(path.stem).group(1)
+        try:
+            found.append((int(label), path))
+        except ValueError as exc:
+            raise ValueError(f'Invalid depth frame name: {path}') from exc
+    found.sort()
+    return found
+
+
+# ---------------------------------------------------------------- extrema
 
 @dataclass
 class Extrema:
@@ -28,6 +149,26 @@ class Extrema:
     first_time_lo: np.ndarray
     max_speed: np.ndarray
 
+
+def write_extrema(path, max_depth, first_time_hi, first_time_lo, max_speed):
+    arrays = {'max_depth': _float_array(max_depth, 'max_depth'),
+              'max_speed': _float_array(max_speed, 'max_speed'),
+              'first_time_hi': _uint_array(first_time_hi, 'first_time_hi'),
+              'first_time_lo': _uint_array(first_time_lo, 'first_time_lo')}
+    if len({a.size for a in arrays.values()}) > 1:
+        raise ValueError('extrema arrays must have the same number of cells')
+    _store(path, EXTREMA_LAYOUT, arrays)
+
+
+def read_extrema(path, expected_count=None):
+    arrays = _fetch(path, EXTREMA_LAYOUT)
+    sizes = {len(a) for a in arrays.values()}
+    if len(sizes) > 1 or (expected_count is not None and sizes != {expected_count}):
+        raise ValueError(f'{path}: extrema cell count differs from mesh')
+    return Extrema(arrays['max_depth'], arrays['first_time_hi'], arrays['first_time_lo'], arrays['max_speed'])
+
+
+# ------------------------------------------------------------- checkpoints
 
 @dataclass
 class Checkpoint:
@@ -46,232 +187,173 @@ class Checkpoint:
     metadata_json: str
 
 
-def _float_array(value, name):
-    array = np.asarray(value, dtype=np.float32)
-    if array.ndim != 1 or not np.all(np.isfinite(array)):
-        raise ValueError(f'{name} must be a finite one-dimensional F32 array')
-    return array
-
-
-def _uint_array(value, name):
-    array = np.asarray(value)
-    if (array.ndim != 1 or not np.issubdtype(array.dtype, np.number)
-            or not np.all(np.isfinite(array)) or np.any(array != np.floor(array))
-            or np.any(array < 0) or np.any(array > np.iinfo(np.uint32).max)):
-        raise ValueError(f'{name} must be a one-dimensional U32 array')
-    return array.astype(np.uint32)
-
-
-def write_bed(path, bed):
-    fdb.save(path, [('F32Value', 'bed', {'value': _float_array(bed, 'bed')})])
-
-
-def _read_named(path, feature, name, column, expected_count=None):
-    values = fdb.load(path).table(feature, name)[column]
-    if expected_count is not None and len(values) != expected_count:
-        raise ValueError(f'{path}: {name} has {len(values)} rows, expected {expected_count}')
-    return values
-
-
-def read_bed(path, expected_count=None):
-    return _read_named(path, 'F32Value', 'bed', 'value', expected_count)
-
-
-def write_depth_frame(path, depth):
-    values = _float_array(depth, 'depth')
-    if np.any(values < 0):
-        raise ValueError('depth must be nonnegative')
-    fdb.save(path, [('F32Value', 'depth', {'value': values})])
-
-
-def read_depth_frame(path, expected_count=None):
-    values = _read_named(path, 'F32Value', 'depth', 'value', expected_count)
-    if not np.all(np.isfinite(values)) or np.any(values < 0):
-        raise ValueError(f'{path}: invalid depth frame')
-    return values
-
-
-def list_depth_frames(output_root):
-    """(elapsed seconds, path) pairs in numeric order."""
-    frames = []
-    for path in (Path(output_root) / 'frames').glob('depth_*.fdb'):
-        try:
-            seconds = int(path.stem.removeprefix('depth_'))
-        except ValueError as exc:
-            raise ValueError(f'Invalid depth frame name: {path}') from exc
-        frames.append((seconds, path))
-    return sorted(frames)
-
-
-def write_extrema(path, max_depth, first_time_hi, first_time_lo, max_speed):
-    arrays = {
-        'max_depth': _float_array(max_depth, 'max_depth'),
-        'max_speed': _float_array(max_speed, 'max_speed'),
-        'first_time_hi': _uint_array(first_time_hi, 'first_time_hi'),
-        'first_time_lo': _uint_array(first_time_lo, 'first_time_lo'),
-    }
-    if len({len(a) for a in arrays.values()}) != 1:
-        raise ValueError('extrema arrays must have the same number of cells')
-    fdb.save(path, [('F32Value', 'max_depth', {'value': arrays['max_depth']}),
-                    ('F32Value', 'max_speed', {'value': arrays['max_speed']}),
-                    ('IndexLike', 'first_time_hi', {'index': arrays['first_time_hi']}),
-                    ('IndexLike', 'first_time_lo', {'index': arrays['first_time_lo']})])
-
-
-def read_extrema(path, expected_count=None):
-    db = fdb.load(path)
-    result = Extrema(db.table('F32Value', 'max_depth')['value'],
-                     db.table('IndexLike', 'first_time_hi')['index'],
-                     db.table('IndexLike', 'first_time_lo')['index'],
-                     db.table('F32Value', 'max_speed')['value'])
-    sizes = {len(result.max_depth), len(result.first_time_hi), len(result.first_time_lo), len(result.max_speed)}
-    if len(sizes) != 1 or (expected_count is not None and len(result.max_depth) != expected_count):
-        raise ValueError(f'{path}: extrema cell count differs from mesh')
-    return result
-
-
 def write_checkpoint(path, *, depth, bed, q, rain_time, infiltration, max_depth, first_time_hi,
                      first_time_lo, max_speed, clock_hi, clock_lo, gate_open, metadata_json):
-    """Persist a completed step; metadata_json is kept verbatim (output.py:171-211)."""
-    arrays = {name: _float_array(value, name) for name, value in
-              [('depth', depth), ('bed', bed), ('q', q), ('rain_time', rain_time),
-               ('infiltration', infiltration), ('max_depth', max_depth), ('max_speed', max_speed)]}
-    if len({len(arrays[n]) for n in ('depth', 'bed', 'rain_time', 'infiltration', 'max_depth', 'max_speed')}) != 1:
+    """A completed step's state and its metadata text (kept byte for byte)."""
+    given = dict(depth=depth, bed=bed, q=q, rain_time=rain_time, infiltration=infiltration,
+                 max_depth=max_depth, max_speed=max_speed)
+    arrays = {name: _float_array(given[name], name) for name in _STATE_F32}
+    cells = len(arrays['depth'])
+    if any(len(arrays[name]) != cells for name in _CELL_F32):
         raise ValueError('checkpoint cell arrays must have the same length')
-    times = {name: _uint_array(value, name) for name, value in
-             [('first_time_hi', first_time_hi), ('first_time_lo', first_time_lo)]}
-    if any(len(v) != len(arrays['depth']) for v in times.values()):
+    for name, value in (('first_time_hi', first_time_hi), ('first_time_lo', first_time_lo)):
+        arrays[name] = _uint_array(value, name)
+    if len(arrays['first_time_hi']) != cells or len(arrays['first_time_lo']) != cells:
         raise ValueError('checkpoint first-time arrays must match cell count')
-    if np.any(arrays['depth'] < 0):
+    if (arrays['depth'] < 0).any():
         raise ValueError('checkpoint depth must be nonnegative')
     if not isinstance(metadata_json, str):
         raise TypeError('metadata_json must be a JSON string')
     json.loads(metadata_json)
     if not isinstance(gate_open, (bool, np.bool_)):
         raise TypeError('gate_open must be boolean')
-    ints = [_uint_array([v], n) for n, v in
-            [('clock_hi', clock_hi), ('clock_lo', clock_lo), ('gate_open', int(gate_open))]]
-    tables = [('F32Value', n, {'value': a}) for n, a in arrays.items()]
-    tables += [('IndexLike', n, {'index': a}) for n, a in zip(_CHECKPOINT_INTS, ints)]
-    tables += [('IndexLike', n, {'index': a}) for n, a in times.items()]
-    tables.append(('U8Value', 'state_meta', {'value': np.frombuffer(metadata_json.encode('utf-8'), np.uint8)}))
-    fdb.save(path, tables)
+    for name, value in (('clock_hi', clock_hi), ('clock_lo', clock_lo), ('gate_open', int(gate_open))):
+        arrays[name] = _uint_array([value], name)
+    arrays['state_meta'] = np.frombuffer(metadata_json.encode('utf-8'), np.uint8)
+    _store(path, CHECKPOINT_LAYOUT, arrays)
 
 
 def read_checkpoint(path, expected_cells=None, expected_sides=None):
-    db = fdb.load(path)
-    floats = {n: db.table('F32Value', n)['value'] for n in _CHECKPOINT_FLOATS}
-    ints = {n: db.table('IndexLike', n)['index'] for n in _CHECKPOINT_INTS}
-    times = {n: db.table('IndexLike', n)['index'] for n in _CHECKPOINT_TIME}
-    metadata_json = db.table('U8Value', 'state_meta')['value'].tobytes().decode('utf-8')
-    if len({len(floats[n]) for n in ('depth', 'bed', 'rain_time', 'infiltration', 'max_depth', 'max_speed')}) != 1:
+    a = _fetch(path, CHECKPOINT_LAYOUT)
+    cells = len(a['depth'])
+    if any(len(a[name]) != cells for name in _CELL_F32):
         raise ValueError(f'{path}: inconsistent checkpoint cell counts')
-    if any(len(v) != len(floats['depth']) for v in times.values()):
+    if any(len(a[name]) != cells for name in _TIMES):
         raise ValueError(f'{path}: inconsistent checkpoint first-time counts')
-    if expected_cells is not None and len(floats['depth']) != expected_cells:
+    if expected_cells is not None and cells != expected_cells:
         raise ValueError(f'{path}: checkpoint cell count differs from mesh')
-    if expected_sides is not None and len(floats['q']) != expected_sides:
+    if expected_sides is not None and len(a['q']) != expected_sides:
         raise ValueError(f'{path}: checkpoint side count differs from mesh')
-    if any(len(v) != 1 for v in ints.values()):
+    if any(len(a[name]) != 1 for name in _SCALARS):
         raise ValueError(f'{path}: checkpoint scalar count must be one')
-    if any(not np.all(np.isfinite(v)) for v in floats.values()) or np.any(floats['depth'] < 0):
+    if not all(np.isfinite(a[name]).all() for name in _STATE_F32) or (a['depth'] < 0).any():
         raise ValueError(f'{path}: invalid checkpoint F32 state')
-    if ints['gate_open'][0] not in (0, 1):
+    if int(a['gate_open'][0]) not in (0, 1):
         raise ValueError(f'{path}: invalid checkpoint gate state')
+    metadata_json = a['state_meta'].tobytes().decode('utf-8')
     json.loads(metadata_json)
-    return Checkpoint(floats['depth'], floats['bed'], floats['q'], floats['rain_time'],
-                      floats['infiltration'], floats['max_depth'], times['first_time_hi'],
-                      times['first_time_lo'], floats['max_speed'], int(ints['clock_hi'][0]),
-                      int(ints['clock_lo'][0]), bool(ints['gate_open'][0]), metadata_json)
+    return Checkpoint(a['depth'], a['bed'], a['q'], a['rain_time'], a['infiltration'], a['max_depth'],
+                      a['first_time_hi'], a['first_time_lo'], a['max_speed'], int(a['clock_hi'][0]),
+                      int(a['clock_lo'][0]), bool(a['gate_open'][0]), metadata_json)
 
+
+# ---------------------------------------------------------------- stations
 
 def resolve_station_cells(points, geometry):
-    """Station -> smallest real cell id whose closed rectangle holds the point
-    (output.py:246-268)."""
-    left, bottom, right, top = (geometry.bounds[1:, i] for i in range(4))
+    """Station name -> the smallest real cell id whose closed rectangle holds
+    the point; a point on a shared edge belongs to the lower id
+    (core/output.py:246-268)."""
+    box = geometry.bounds[1:]
     resolved = {}
     for name, (x, y) in points.items():
-        if not np.isfinite(x) or not np.isfinite(y):
+        if not (np.isfinite(x) and np.isfinite(y)):
             raise ValueError(f'Station {name}: coordinates must be finite')
-        hit = np.flatnonzero((left <= x) & (x <= right) & (bottom <= y) & (y <= top))
-        if not len(hit):
+        inside = (box[:, 0] <= x) & (x <= box[:, 2]) & (box[:, 1] <= y) & (y <= box[:, 3])
+        if not inside.any():
             raise ValueError(f'Station {name}: ({x}, {y}) lies outside the mesh')
-        resolved[name] = int(hit[0] + 1)
+        resolved[name] = int(np.argmax(inside)) + 1
     return resolved
 
 
 def append_station_samples(path, *, elapsed_seconds, time, samples):
+    """One stations.csv row per station, stations in name order; the header
+    is written with the first rows."""
     path = Path(path)
     path.parent.mkdir(parents=True, exist_ok=True)
-    needs_header = not path.exists()
+    fresh = not path.exists()
+    rows = [{'elapsed_seconds': elapsed_seconds, 'time': time, 'station': name,
+             'cell_id': samples[name]['cell_id'], 'depth': samples[name]['depth'],
+             'level': samples[name]['level'], 'u': samples[name]['u'], 'v': samples[name]['v']}
+            for name in sorted(samples)]
     with path.open('a', newline='') as stream:
         writer = csv.DictWriter(stream, fieldnames=STATION_FIELDS)
-        if needs_header:
+        if fresh:
             writer.writeheader()
-        for name in sorted(samples):
-            sample = samples[name]
-            writer.writerow({'elapsed_seconds': elapsed_seconds, 'time': time, 'station': name,
-                             **{k: sample[k] for k in ('cell_id', 'depth', 'level', 'u', 'v')}})
+        writer.writerows(rows)
 
+
+# ---------------------------------------------------------------- manifest
 
 def write_manifest(path, manifest):
+    """manifest.json, replaced in one step through a sibling temporary file."""
     path = Path(path)
     path.parent.mkdir(parents=True, exist_ok=True)
-    temporary = path.with_name(f'.{path.name}.{os.getpid()}.tmp')
-    temporary.write_text(json.dumps(manifest, ensure_ascii=False, indent=2) + '\n')
-    os.replace(temporary, path)
+    staging = path.parent / f'.{path.name}.{os.getpid()}.tmp'
+    staging.write_text(json.dumps(manifest, ensure_ascii=False, indent=2) + '\n')
+    os.replace(staging, path)
 
 
 def read_manifest(path):
     return json.loads(Path(path).read_text())
 
 
+# -------------------------------------------------------------- bed replay
+
+@dataclass
+class _GateOpening:
+    """One gate of the manifest's gate_control report: its cells' closed beds
+    and, once commanded, the F32 opening fraction at a frame time, computed
+    as the device computes it (core/gate.py:115-135, core/output.py:323-341)."""
+    cells: np.ndarray
+    closed: np.ndarray
+    command_seconds: float | None
+    command_tick: int
+    origin: float
+    opening_seconds: np.float32
+    open_elevation: np.float32
+
+    @classmethod
+    def from_report(cls, gate, control):
+        hi, lo = gate['command_clock_ticks'] if gate.get('command_clock_ticks') else (0, 0)
+        return cls(np.asarray(gate['cell_ids'], dtype=np.int64), np.asarray(gate['closed_elevation'], np.float32),
+                   gate['command_seconds'], (int(hi) << 32) | int(lo), control['clock_origin_before_start_s'],
+                   np.float32(control['opening_seconds']), np.float32(control['open_elevation']))
+
+    def fraction(self, elapsed_seconds) -> np.float32:
+        if self.command_seconds is None or elapsed_seconds < self.command_seconds:
+            return np.float32(0.)
+        tick = round((elapsed_seconds + self.origin) * 2 ** 40)
+        age = max(tick - self.command_tick, 0)
+        seconds = np.float32(age >> 32) / np.float32(256.) + np.float32(age & _U32_MAX) * np.float32(2. ** -40)
+        return np.minimum(seconds / self.opening_seconds, np.float32(1.))
+
+    def apply(self, bed, elapsed_seconds):
+        f = self.fraction(elapsed_seconds)
+        bed[self.cells] = self.closed + (self.open_elevation - self.closed) * f
+        if f >= 1.:
+            bed[self.cells] = self.open_elevation
+
+
 class BedTimeline:
-    """Working bed at a frame time: bed.fdb plus recorded bed events, then the
-    gate beds re-derived from the manifest's ``gate_control`` block with the
-    device's F32 opening arithmetic (output.py:299-343)."""
+    """The working bed at nondecreasing frame times: bed.fdb, then the
+    manifest's bed events up to each time in time order, then the gate beds
+    of its gate_control report."""
 
     def __init__(self, output_root, manifest=None, expected_count=None):
-        output_root = Path(output_root)
-        manifest = read_manifest(output_root.parent / 'manifest.json') if manifest is None else manifest
-        self.bed = read_bed(output_root / 'bed.fdb', expected_count)
-        self.events = sorted(manifest.get('bed_events', []), key=lambda e: e['elapsed_seconds'])
-        self.gate_control = manifest.get('gate_control', {})
-        self.cursor = 0
+        root = Path(output_root)
+        if manifest is None:
+            manifest = read_manifest(root.parent / 'manifest.json')
+        self.bed = read_bed(root / 'bed.fdb', expected_count)
+        self._events = deque(sorted(manifest.get('bed_events', []), key=lambda e: e['elapsed_seconds']))
+        control = manifest.get('gate_control', {})
+        self._gates = [_GateOpening.from_report(g, control) for g in control.get('gates', [])]
         self.seconds = float('-inf')
 
-    def _gate_beds(self, elapsed_seconds):
-        control = self.gate_control
-        f32 = np.float32
-        for gate in control.get('gates', []):
-            cells = np.asarray(gate['cell_ids'], dtype=np.int64)
-            closed = np.asarray(gate['closed_elevation'], dtype=f32)
-            fraction = f32(0.)
-            command = gate['command_seconds']
-            if command is not None and elapsed_seconds >= command:
-                hi, lo = gate['command_clock_ticks']
-                tick = round((elapsed_seconds + control['clock_origin_before_start_s']) * 2 ** 40)
-                age_ticks = max(tick - ((int(hi) << 32) | int(lo)), 0)
-                age = f32(age_ticks >> 32) / f32(256.) + f32(age_ticks & 0xffffffff) * f32(2. ** -40)
-                fraction = np.minimum(age / f32(control['opening_seconds']), f32(1.))
-            opened = f32(control['open_elevation'])
-            self.bed[cells] = closed + (opened - closed) * fraction
-            if fraction >= 1.:
-                self.bed[cells] = opened
+    def _apply_event(self, event):
+        ids = _uint_array(event['cell_ids'], 'bed event cell_ids')
+        values = _float_array(event['new_bed'], 'bed event new_bed')
+        if len(ids) != len(values) or (ids >= len(self.bed)).any():
+            raise ValueError('bed event has invalid cell ids or values')
+        self.bed[ids] = values
 
     def at(self, elapsed_seconds):
         if elapsed_seconds < self.seconds:
             raise ValueError('BedTimeline requires nondecreasing frame times')
-        while self.cursor < len(self.events) and self.events[self.cursor]['elapsed_seconds'] <= elapsed_seconds:
-            event = self.events[self.cursor]
-            ids = _uint_array(event['cell_ids'], 'bed event cell_ids')
-            new_bed = _float_array(event['new_bed'], 'bed event new_bed')
-            if len(ids) != len(new_bed) or np.any(ids >= len(self.bed)):
-                raise ValueError('bed event has invalid cell ids or values')
-            self.bed[ids] = new_bed
-            self.cursor += 1
+        while self._events and self._events[0]['elapsed_seconds'] <= elapsed_seconds:
+            self._apply_event(self._events.popleft())
         self.seconds = elapsed_seconds
-        self._gate_beds(elapsed_seconds)
+        for gate in self._gates:
+            gate.apply(self.bed, elapsed_seconds)
         return self.bed
 
 
