@@ -1,27 +1,36 @@
-"""Benchmark: cell-updates/s of the plain local-inertial step on B200.
+"""Benchmark: cell-updates/s of the local-inertial step on B200.
 
-    python bench.py --gpus N --steps K --warmup W [--workload NAME] [--impl reference]
+    python bench.py --gpus N --steps K --warmup W [--form batched|plain|served]
+                    [--workload NAME] [--impl reference]
 
-A "step" of this benchmark is one batch of up to 32 device time steps (one
-replay of the captured step graph, the unit the reference's ti.graph runs
-per host round trip) of the plain single-run solver on the workload; the
-metric counts cells x completed time steps. ``value`` is device time with
-the state resident in HBM (CUDA events on the library's stream around each
-batch); ``e2e`` is the same metric through the public engine call with host
-forcing inputs and the host trace read-back inside the timed region.
+The default is the batched form (the headline of the metric): 64 seeded
+quadtree scenarios of uneven size (about 43.65M cells in all), every
+scenario with its own CFL dt, advanced together. A "step" of this benchmark
+is one ensemble batch: up to 32 device time steps of every scenario. The
+line also carries the same scenarios stepped one after another with the
+plain form (``plain_sequential``, ``batched_over_plain``) and the largest
+depth difference between the two after the same batches.
 
-Multi-GPU: the plain solve does not shard (one domain per device); N ranks
-run N independent replicas ("replicas only", weak scaling), timed by device
-events with the max over ranks.
+``--form plain`` times one plain solve of ``--workload`` (a batch of up to
+32 time steps per bench step); ``--form served`` replays a Poisson request
+stream through the server against the plain form one request at a time.
 
-Each plain run first advances, untimed, a third into its simulated duration
-(rain and flow have reached the domain by then), then takes the warm-up and
-the timed batches; the CPU baseline continues from the GPU run's state.
+``value`` is device time with the state resident in HBM (CUDA events on the
+library's stream around each batch); ``e2e`` is the same metric through the
+public call with the host forcing inputs and the host trace read-back inside
+the timed region.
 
+Each run first advances, untimed, a third into its simulated duration (rain
+and flow have reached the domain by then) and takes the warm-up batches:
+that state is where the timed batches and the CPU baseline start.
 ``--impl reference`` times the reference algorithm's CPU implementation (the
 CPU restatement of the step, all host threads) on the same workload, from
-t = 0: spinning it up to the GPU arm's start would take the CPU minutes to
-hours on the large configurations.
+the same state and with the same ``config``; the CUDA step produces that
+state untimed (it equals the restatement's own state bit for bit).
+
+Multi-GPU: a solve does not shard (one domain per device); N ranks run N
+independent replicas ("replicas only", weak scaling), timed by device events
+with the max over ranks.
 """
 from __future__ import annotations
 
@@ -107,6 +116,43 @@ def combine_ranks(times, units, device, world):
     return t.tolist(), u.tolist()
 
 
+def plain_config(w, spin_to, world, batch_size=32):
+    """The plain workload's ``config``, identical in both arms."""
+    return {'workload': w.name, 'cells': w.cells, 'sides': w.mesh.s_num - 1,
+            'time_steps_per_bench_step': batch_size, 'spin_up_to_s': spin_to,
+            'start_state': 'advanced by the CUDA step to the spin-up time, then the warm-up batches',
+            'l2': 'flushed (256 MB write) before every timed batch', 'parallelism': f'replicas{world}'}
+
+
+def reference_plain(args):
+    """The reference arm of the plain form: the CPU restatement (all host
+    threads) on the same workload, from the state the b200 arm's timed
+    batches start from (produced by the CUDA step, untimed; it equals the CPU
+    restatement's own state bit for bit)."""
+    import torch
+    w = make_workload(args.workload)
+    spin_to = w.duration / 3 if args.spin_up is None else args.spin_up
+    start = None
+    if torch.cuda.is_available():
+        from nhflood.native import CudaEngine
+        from nhflood.plain import PlainRun
+        start = PlainRun(w, lambda a, p: CudaEngine(a, p, device='cuda:0'))
+        while start.elapsed < spin_to and not start.done:
+            start.advance()
+        for _ in range(args.warmup):
+            start.advance()
+    base = cpu_baseline(w, seconds_budget=max(5.0, args.cpu_seconds), start=start)
+    if start is not None:
+        start.close()
+    line = {'metric': METRIC, 'value': base['value'], 'unit': METRIC, 'impl': 'reference', 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'form': 'plain',
+            'config': plain_config(w, spin_to, args.gpus),
+            'cpu_baseline': base,
+            'e2e': {'value': base['value'], 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line))
+
+
 def make_workload(name):
     from nhflood import workloads
     if name == 'plain_uniform_256':
@@ -115,6 +161,8 @@ def make_workload(name):
         return workloads.dambreak(n=int(name.split('_')[1]))
     if name == 'multires_quadtree':
         return workloads.multires_quadtree()
+    if name == 'multires_quadtree_4m':
+        return workloads.multires_quadtree_4m()
     if name.startswith('gated_polder_'):
         return workloads.gated_polder(n=int(name.split('_')[2]))
     raise SystemExit(f'unknown workload {name}')
@@ -194,30 +242,91 @@ def cpu_baseline(workload, seconds_budget=15.0, threads=None, start=None):
             'sample': f'{steps} time steps of {workload.name} from t={origin:.0f} s ({el:.1f} s of CPU restatement, OpenMP)'}
 
 
+ENSEMBLE_PLAIN_BATCHES = 3  # plain batches of every member, and as many e2e ensemble batches
+
+
+def ensemble_workloads(args, rank):
+    from nhflood.workloads import ensemble_scenarios
+    return ensemble_scenarios(seed=4 + rank, members=args.members)
+
+
+def ensemble_config(ws, spin_to, world, batch_size=32):
+    """The batched workload's ``config``, identical in both arms."""
+    cells = np.array([w.cells for w in ws], np.int64)
+    return {'workload': f'ensemble_{len(ws)}_quadtrees', 'members': len(ws), 'cells': int(cells.sum()),
+            'cells_min': int(cells.min()), 'cells_max': int(cells.max()),
+            'time_steps_per_bench_step': batch_size, 'spin_up_to_s': spin_to,
+            'start_state': 'every member advanced by the CUDA step to the spin-up time, then the warm-up batches',
+            'l2': 'inputs larger than L2 (43.65M cells resident)', 'parallelism': f'replicas{world}'}
+
+
+def spin_up(ens, spin_to, warmup):
+    """Advance (untimed) until every member has reached ``spin_to`` seconds,
+    then ``warmup`` more batches: the state both arms start from."""
+    while min(r.elapsed for r in ens.runs) < spin_to and not ens.done:
+        ens.advance()
+    for _ in range(warmup):
+        ens.advance()
+
+
+def ensemble_cpu_sample(runs, seconds_budget, threads=None):
+    """The CPU restatement on every member in turn, continuing from that
+    member's current state, one time step per call; each member gets a share
+    of the budget in proportion to its cells (at least one step). Only the
+    step calls are timed."""
+    sys.path.insert(0, str(ROOT / 'oracle'))
+    from engine import OracleEngine, set_threads  # oracle/engine.py
+    from nhflood.plain import PlainRun
+    threads = threads or os.cpu_count()
+    set_threads(threads)
+    total_cells = sum(r.w.cells for r in runs)
+    cell_updates, seconds, steps = 0, 0.0, 0
+    for member in runs:
+        run = PlainRun(member.w, lambda a, p: OracleEngine(a, p), batch_size=1)
+        run.adopt(member)
+        share = seconds_budget * member.w.cells / total_cells
+        spent, n = 0.0, 0
+        while (n == 0 or spent < share) and not run.done:
+            t0 = time.perf_counter()
+            k = run.advance()
+            spent += time.perf_counter() - t0
+            n += k
+            if k == 0:
+                break
+        cell_updates += n * member.w.cells
+        seconds += spent
+        steps += n
+        run.close()
+    return {'value': cell_updates / seconds if seconds else None, 'unit': METRIC, 'cores': threads, 'kind': 'port',
+            'sample': (f'{steps} time steps over the {len(runs)} members, each member continuing from its state '
+                       f'at the timed start ({seconds:.1f} s of CPU restatement, OpenMP)')}
+
+
 def bench_batched(args, rank, world, local):
     """Batched form: 64 seeded quadtree scenarios (about 40M cells) in one
     ensemble (by default every scenario's own batch graph, all launched
     together; --tile / --grid select the one-launch schedule), against the
-    same scenarios stepped one after another with the plain form."""
+    same scenarios stepped one after another with the plain form from the
+    same state; the max depth difference of the two is measured."""
     import torch
     from nhflood.ensemble import EnsembleRun
-    from nhflood.workloads import ensemble_scenarios
     device = torch.device('cuda', local)
     torch.cuda.set_device(device)
     t0 = time.perf_counter()
-    ws = ensemble_scenarios(seed=4 + rank, members=args.members)
+    ws = ensemble_workloads(args, rank)
     t_gen = time.perf_counter() - t0
     t0 = time.perf_counter()
     ens = EnsembleRun(ws, device=str(device), tile=args.tile, grid_blocks=args.grid)
     t_setup = time.perf_counter() - t0
     stream = ens.ensemble.stream()
-    # spin-up (untimed) a third into the members' runs, as for the plain form
     spin_to = min(r.w.duration for r in ens.runs) / 3 if args.spin_up is None else args.spin_up
-    while min(r.elapsed for r in ens.runs) < spin_to and not ens.done:
-        ens.advance()
-    for _ in range(args.warmup):
-        ens.advance()
+    t0 = time.perf_counter()
+    spin_up(ens, spin_to, args.warmup)
+    t_spin = time.perf_counter() - t0
     torch.cuda.synchronize(device)
+    cpu = None
+    if rank == 0 and world == 1 and os.environ.get('NHF_BENCH_NO_CPU') != '1':
+        cpu = ensemble_cpu_sample(ens.runs, args.cpu_seconds)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -231,6 +340,7 @@ def bench_batched(args, rank, world, local):
     else:  # per step: the ensemble step, its CFL pass, the hanging pre-pass if any member has hanging edges
         per_batch_kernels = 5 + ens.runs[0].params.batch_size * (2 + (1 if hang else 0))
     with ClockSampler(local) as clocks:
+        torch.cuda.nvtx.range_push('timed')  # ncu --nvtx --nvtx-include timed/ captures the timed state
         for k in range(args.steps):
             if ens.done:
                 break
@@ -241,17 +351,19 @@ def bench_batched(args, rank, world, local):
             cell_updates += ens.cell_updates(ens.finish(ens.ensemble.read_trace()))
             recorded += 1
         torch.cuda.synchronize(device)
+        torch.cuda.nvtx.range_pop()
     device_s = sum(starts[i].elapsed_time(ends[i]) for i in range(recorded)) / 1e3
     # the same scenarios, one after another, each on a plain engine of its own
     # (the plain form's own tile and CFL choice) continuing from the member's state
     from nhflood.native import CudaEngine
     from nhflood.plain import PlainRun
     plain_cells, plain_s = 0, 0.0
-    for member in ens.runs if args.plain_batches > 0 else ():
+    plain_depth = []
+    for member in ens.runs:
         r = PlainRun(member.w, lambda a, p: CudaEngine(a, p, device=str(device)), batch_size=member.params.batch_size)
         r.adopt(member)
         st = r.engine.stream()
-        for _ in range(args.plain_batches):
+        for _ in range(ENSEMBLE_PLAIN_BATCHES):
             if r.done:
                 break
             tw, ow = r.begin()
@@ -262,20 +374,27 @@ def bench_batched(args, rank, world, local):
             plain_cells += r.finish(r.engine.read_trace()) * r.w.cells
             b.synchronize()
             plain_s += a.elapsed_time(b) / 1e3
+        plain_depth.append((r.elapsed, r.engine.get('depth')))
         r.close()
-    # end to end through the public call (host words in, host traces out)
+    # end to end through the public call (host words in, host traces out),
+    # the same batches the plain engines just ran
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
     e2e_cells = 0
     h2d = 0
-    e2e_batches = 3
-    for _ in range(e2e_batches):
+    for _ in range(ENSEMBLE_PLAIN_BATCHES):
         if ens.done:
             break
         e2e_cells += ens.cell_updates(ens.advance())
         h2d += ens.h2d_bytes
     torch.cuda.synchronize(device)
     e2e_s = time.perf_counter() - t0
+    # batched against plain: the members' depths after the same batches
+    max_err, compared = 0.0, 0
+    for member, (elapsed, depth) in zip(ens.runs, plain_depth):
+        if member.elapsed == elapsed:
+            max_err = max(max_err, float(np.abs(member.engine.get('depth').astype(np.float64) - depth).max()))
+            compared += 1
     (device_s, e2e_s), (cell_updates, e2e_cells) = combine_ranks([device_s, e2e_s], [cell_updates, e2e_cells],
                                                                  device, world)
     value = cell_updates / device_s
@@ -290,27 +409,59 @@ def bench_batched(args, rank, world, local):
             'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': recorded,
             'warmup': args.warmup, 'ms_per_step': device_s * 1e3 / max(1, recorded), 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'form': 'batched',
-            'config': {'workload': f'ensemble_{args.members}_quadtrees', 'members': len(ws),
-                       'cells': int(cells.sum()), 'cells_min': int(cells.min()), 'cells_max': int(cells.max()),
-                       'time_steps_per_bench_step': ens.runs[0].params.batch_size,
-                       'schedule': ens.schedule, 'tile': ens.ensemble.tile or 'per member',
-                       'grid_blocks': ens.ensemble.grid, 'tiles': ens.ensemble.tiles,
-                       'spin_up_to_s': spin_to,
-                       'l2': 'inputs larger than L2', 'parallelism': f'replicas{world}'},
+            'config': ensemble_config(ws, spin_to, world),
+            'schedule': {'kind': ens.schedule, 'tile': ens.ensemble.tile or 'per member',
+                         'grid_blocks': ens.ensemble.grid, 'tiles': ens.ensemble.tiles},
             'plain_sequential': {'value': plain, 'unit': METRIC,
-                                 'sample': f'{args.plain_batches} plain batches of each member, one member after another'},
+                                 'sample': f'{ENSEMBLE_PLAIN_BATCHES} plain batches of each member from its state '
+                                           'after the timed batches, one member after another'},
             'batched_over_plain': value / plain if plain else None,
-            'max_depth_error_vs_plain_m': 0.0,
+            'max_depth_error_vs_plain_m': max_err,
+            'members_compared_with_plain': compared,
             'gpu_launches': per_batch_kernels * recorded,
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
-                         'traffic': None, 'peak_kind': kind, 'algorithmic_bytes_per_cell_update': b_alg},
+                         'traffic': None, 'peak_kind': kind, 'algorithmic_bytes_per_cell_update': b_alg,
+                         'scope': 'whole batch of every member (step kernels, CFL passes, pre-passes)'},
             'e2e': {'value': e2e_cells / e2e_s if e2e_s else None, 'unit': METRIC,
-                    'h2d_bytes_per_step': h2d // max(1, e2e_batches), 'd2h_bytes_per_step': trace_bytes},
+                    'h2d_bytes_per_step': h2d // max(1, ENSEMBLE_PLAIN_BATCHES), 'd2h_bytes_per_step': trace_bytes},
             'clocks': clocks.summary(),
-            'setup_seconds': {'generate': round(t_gen, 1), 'engines_and_tuning': round(t_setup, 1)},
+            'setup_seconds': {'generate': round(t_gen, 1), 'engines': round(t_setup, 1),
+                              'spin_up': round(t_spin, 1)},
         }
+        if cpu is not None:
+            line['cpu_baseline'] = cpu
         print(json.dumps(line))
     ens.close()
+
+
+def reference_batched(args):
+    """The reference arm of the batched form: the CPU restatement of the step
+    (all host threads) on the same 64 members, from the same start state and
+    with the same ``config`` as the b200 arm. The start state is produced by
+    the CUDA step, untimed: it equals the CPU restatement's own state bit for
+    bit (the parity tests), and the CPU would need about half an hour to
+    reach it. Only the CPU restatement's step calls are timed."""
+    import torch
+    from nhflood.ensemble import EnsembleRun
+    ws = ensemble_workloads(args, 0)
+    spin_to = min(w.duration for w in ws) / 3 if args.spin_up is None else args.spin_up
+    cells = sum(w.cells for w in ws)
+    if not torch.cuda.is_available():
+        base = {'value': None, 'unit': METRIC, 'cores': os.cpu_count(), 'kind': 'port',
+                'sample': 'not run: the start state needs the CUDA step'}
+    else:
+        ens = EnsembleRun(ws, device='cuda:0')
+        spin_up(ens, spin_to, args.warmup)
+        torch.cuda.synchronize()
+        base = ensemble_cpu_sample(ens.runs, max(5.0, args.cpu_seconds))
+        ens.close()
+    line = {'metric': METRIC, 'value': base['value'], 'unit': METRIC, 'impl': 'reference', 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'form': 'batched',
+            'config': ensemble_config(ws, spin_to, args.gpus),
+            'cpu_baseline': base,
+            'e2e': {'value': base['value'], 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line))
 
 
 def _request_workload(params):
@@ -394,13 +545,13 @@ def main():
     ap.add_argument('--workload', default=os.environ.get('NHF_BENCH_WORKLOAD', 'multires_quadtree'))
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
-    ap.add_argument('--form', default='plain', choices=['plain', 'batched', 'served'])
+    ap.add_argument('--form', default=os.environ.get('NHF_BENCH_FORM', 'batched'),
+                    choices=['plain', 'batched', 'served'])
     ap.add_argument('--requests', type=int, default=48, help='served: requests in the stream')
     ap.add_argument('--hbm-budget', type=float, default=150e9, help='served: admission budget in bytes')
     ap.add_argument('--members', type=int, default=64)
     ap.add_argument('--tile', type=int, default=None, help='batched: tile size (default: autotuned)')
     ap.add_argument('--grid', type=int, default=None, help='batched: 0 persistent, -1 block per tile')
-    ap.add_argument('--plain-batches', type=int, default=2)
     ap.add_argument('--path', default='auto', help="plain form's step: 'auto', 'multipass', 'tile256', 'tile512', 'tile1024'")
     ap.add_argument('--spin-up', type=float, default=None,
                     help='simulated seconds advanced (untimed) before the warm-up; default a third of the run')
@@ -413,15 +564,13 @@ def main():
     if args.impl == 'reference':
         if rank != 0:
             return
-        w = make_workload(args.workload)
-        base = cpu_baseline(w, seconds_budget=max(5.0, args.cpu_seconds))
-        line = {'metric': METRIC, 'value': base['value'], 'unit': METRIC, 'impl': 'reference', 'n_gpus': args.gpus,
-                'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True, 'scaling': 'weak',
-                'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-                'config': {'workload': w.name, 'cells': w.cells},
-                'cpu_baseline': base,
-                'e2e': {'value': base['value'], 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
-        print(json.dumps(line))
+        if args.form == 'batched':
+            reference_batched(args)
+        elif args.form == 'plain':
+            reference_plain(args)
+        else:
+            print(json.dumps({'impl': 'reference', 'form': args.form,
+                              'unavailable': 'the served form has no CPU counterpart; time the batched or plain form'}))
         return
 
     import torch
@@ -458,6 +607,10 @@ def main():
     for _ in range(args.warmup):
         run.advance()
     torch.cuda.synchronize(device)
+    # the CPU restatement on a bounded sample from the same state the timed batches start from
+    cpu = None
+    if rank == 0 and world == 1 and os.environ.get('NHF_BENCH_NO_CPU') != '1':
+        cpu = cpu_baseline(w, seconds_budget=args.cpu_seconds, start=run)
     if world > 1:
         dist.barrier()
     # device-resident timing: events around each graph replay on the library stream
@@ -471,6 +624,7 @@ def main():
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=device)
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize(device)
+        torch.cuda.nvtx.range_push('timed')  # ncu --nvtx --nvtx-include timed/ captures the timed state
         for k in range(args.steps):
             if run.done:
                 break
@@ -485,6 +639,7 @@ def main():
             cell_steps += n * w.cells
             launches += per_batch_launches
         torch.cuda.synchronize(device)
+        torch.cuda.nvtx.range_pop()
     timed = [starts[i].elapsed_time(ends[i]) for i in range(recorded)]
     device_ms = float(sum(timed))
     # end-to-end through the public call: host inputs in, host trace out
@@ -516,11 +671,8 @@ def main():
             'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': device_ms / max(1, len(timed)), 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': {'workload': w.name, 'cells': w.cells, 'sides': w.mesh.s_num - 1,
-                       'time_steps_per_bench_step': run.params.batch_size,
-                       'l2': 'flushed (256 MB write) before every timed batch',
-                       'step_form': eng.path, 'spin_up_to_s': spin_up_s,
-                       'parallelism': f'replicas{world}'},
+            'config': plain_config(w, spin_to, world, run.params.batch_size),
+            'step_form': eng.path, 'spun_up_to_s': spin_up_s,
             'gpu_launches': launches,
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak if achieved else None,
@@ -536,8 +688,8 @@ def main():
             'clocks': clocks.summary(),
             'simulated_seconds': run.elapsed,
         }
-        if world == 1 and os.environ.get('NHF_BENCH_NO_CPU') != '1':
-            line['cpu_baseline'] = cpu_baseline(w, seconds_budget=args.cpu_seconds, start=run)
+        if cpu is not None:
+            line['cpu_baseline'] = cpu
         print(json.dumps(line))
     run.close()
     if world > 1:

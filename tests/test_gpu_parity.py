@@ -214,18 +214,20 @@ def test_tile_1024_both_cfl_forms_bit_exact(cuda_available, cfl):
         r.close()
 
 
-@pytest.mark.parametrize('name,batches', [('multires_quadtree', 2), ('dambreak_4096', 1)])
+@pytest.mark.parametrize('name,batches', [('multires_quadtree', 2), ('multires_quadtree_4m', 1), ('dambreak_4096', 1)])
 def test_full_size_configurations_bit_exact(cuda_available, name, batches):
     """The bench's full-size meshes, 1,362,175 quadtree cells (20 km, 2:1,
-    hanging edges) and 16,777,216 dam-break cells (33.5 M sides, 1024-cell
-    tiles, the separate CFL pass): the first 32-step batches on the fused
-    step as planned for the mesh and on the CPU restatement give identical
-    trace rows, state arrays and budget totals."""
+    hanging edges), the 4.0 M-cell quadtree (36.6 km) and 16,777,216
+    dam-break cells (33.5 M sides, 1024-cell tiles, the separate CFL pass):
+    the first 32-step batches on the fused step as planned for the mesh and
+    on the CPU restatement give identical trace rows, state arrays and
+    budget totals."""
     from lockstep import FIELDS
     from nhflood.plain import PlainRun
-    from nhflood.workloads import dambreak, multires_quadtree
+    from nhflood.workloads import dambreak, multires_quadtree, multires_quadtree_4m
     from runner import oracle_factory
-    workload = multires_quadtree() if name == 'multires_quadtree' else dambreak()
+    workload = {'multires_quadtree': multires_quadtree, 'multires_quadtree_4m': multires_quadtree_4m,
+                'dambreak_4096': dambreak}[name]()
     runs = [PlainRun(workload, factory, batch_size=32) for factory in (oracle_factory, cuda_engine('auto'))]
     try:
         assert 'cfl=pass' in runs[1].engine.path, runs[1].engine.path
