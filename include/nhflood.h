@@ -6,7 +6,7 @@
  * src/nh_flood_2d/core/solver_compact.py:179-1008). The reference has no
  * FFI of its own: every entry point below replaces one host call on a
  * Taichi field or kernel, cited beside it. A Python host binds it with
- * ctypes (nhflood/native.py); INTEGRATION.md shows the binding.
+ * ctypes (nhflood/native.py is that binding).
  *
  * Conventions
  *  - Arrays keep the reference's layout: cell and side index 0 is the
@@ -54,6 +54,18 @@ extern "C" {
 #define NHF_STEP_BAD_DT 3
 #define NHF_STEP_OVERSHOOT 4
 
+/* The physics type of the build. The step computes in F32 as the
+ * reference's fields do (libnhflood.so). Compiled with -DNHF_REAL_DOUBLE, the
+ * same multi-pass kernels compute in F64 instead (libnhflood_f64.so): the
+ * FP64 build the precision study compares the F32 state with. Every array
+ * below typed nhf_real is F64 there; the clock (dt, its fixed-point words,
+ * the trace) stays F32 in both, and the budget partials are FP64 in both. */
+#ifdef NHF_REAL_DOUBLE
+typedef double nhf_real;
+#else
+typedef float nhf_real;
+#endif
+
 typedef struct nhf_mesh {
     int32_t e_num;      /* cells including sentinel 0 */
     int32_t s_num;      /* sides including sentinel 0 */
@@ -63,36 +75,36 @@ typedef struct nhf_mesh {
     int32_t hang_cells; /* hanging-edge gradient cells (0: aligned mesh) */
     int32_t hang_edges; /* hanging edges */
     /* static cell arrays [e_num], device */
-    const float *x, *y, *area, *width, *height;
-    const float *f0, *fc, *k; /* Horton, m/s and 1/h (hydraulics.py:63-93) */
-    const float *weight;      /* boundary cell weight */
+    const nhf_real *x, *y, *area, *width, *height;
+    const nhf_real *f0, *fc, *k; /* Horton, m/s and 1/h (hydraulics.py:63-93) */
+    const nhf_real *weight;      /* boundary cell weight */
     const int32_t *boundary_id, *rain_index;
     const int32_t *face_ptr, *face_count; /* [e_num*4] */
     const int32_t *isl_data;              /* [isl_len] */
     /* static side arrays [s_num], device */
     const int32_t *topology; /* [s_num*3] */
-    const float *length, *side_n;
+    const nhf_real *length, *side_n;
     const uint8_t *sbf; /* 1 = closed exterior side */
     /* boundaries [max(1,b_num)], device: 0 level, 1 discharge */
     const int32_t *kind;
     /* theta < 1 only: open-face fractions [e_num*4], device (NULL if theta == 1) */
-    const float *open_face;
+    const nhf_real *open_face;
     /* hanging-edge reconstruction (core/pressure.py:19-45), device */
     const int32_t *edge_index; /* [s_num] */
-    const float *offsets;      /* [hang_edges*2] */
+    const nhf_real *offsets;   /* [hang_edges*2] */
     const int32_t *slots;      /* [hang_edges*2] */
     const int32_t *hcells;     /* [hang_cells] */
     const int32_t *axes;       /* [hang_cells*2] */
     /* mutable state, device */
-    float *bed, *depth, *q, *rain_time, *infiltration, *max_depth, *max_speed, *u, *v;
+    nhf_real *bed, *depth, *q, *rain_time, *infiltration, *max_depth, *max_speed, *u, *v;
     uint32_t *peak_hi, *peak_lo;
 } nhf_mesh;
 
 typedef struct nhf_params {
-    float g;          /* 9.81 */
-    float afa;        /* Courant number */
-    float sita;       /* theta time weighting */
-    float min_h;      /* wet threshold */
+    nhf_real g;       /* 9.81 */
+    nhf_real afa;     /* Courant number */
+    nhf_real sita;    /* theta time weighting */
+    nhf_real min_h;   /* wet threshold */
     float min_dt;     /* F32(1e-4) CFL floor (solver_compact.py:31) */
     int32_t batch_size; /* steps per batch, 1..64 (clock.py:48-51) */
     int32_t path;       /* 0: fused tiled step when the mesh allows it, else
@@ -117,6 +129,8 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
 int nhf_destroy(nhf_handle *h);
 const char *nhf_last_error(const nhf_handle *h);
 const char *nhf_version(void);
+/* sizeof(nhf_real) of this build: 4, or 8 for the FP64 build. */
+int nhf_real_bytes(void);
 
 /* initialize() (solver_compact.py:398-410): depth = 0, infiltration = f0,
  * per-side centre distance. */
@@ -127,12 +141,12 @@ int nhf_get_clock(nhf_handle *h, uint32_t now[2]);
 /* clock.active[None] = 1 before the first compute_cfl (solver_compact.py:884). */
 int nhf_set_active(nhf_handle *h, int32_t active);
 /* upload_forcing (solver_compact.py:769-790): coefficients [max(1,b_num)][2]
- * F32 and rain rates [n_rates] F32, both host; rain_rates may be NULL to keep
- * the previous rates. */
-int nhf_set_forcing(nhf_handle *h, const float *coefficients, const float *rain_rates, int32_t raining);
+ * and rain rates [n_rates], both host nhf_real; rain_rates may be NULL to
+ * keep the previous rates. */
+int nhf_set_forcing(nhf_handle *h, const nhf_real *coefficients, const nhf_real *rain_rates, int32_t raining);
 /* apply_initial_levels (solver_compact.py:412-420, 876-883): targets is a
- * device [e_num] F32 array; the level diagnostics enter the budget. */
-int nhf_apply_initial_levels(nhf_handle *h, const float *targets);
+ * device [e_num] nhf_real array; the level diagnostics enter the budget. */
+int nhf_apply_initial_levels(nhf_handle *h, const nhf_real *targets);
 /* compute_cfl (solver_compact.py:617-641). */
 int nhf_compute_cfl(nhf_handle *h);
 /* initial_diagnostics (solver_compact.py:657-672). */
@@ -154,17 +168,17 @@ int nhf_read_trace(nhf_handle *h, uint32_t *trace);
 int nhf_budget_flush(nhf_handle *h, double *totals);
 int nhf_budget_terms(const nhf_handle *h);
 /* ndt_t / cfl_arg_t / flow_depth_t[cfl_arg] (solver_compact.py:644-655). */
-int nhf_get_cfl(nhf_handle *h, float *ndt, int32_t *arg, float *flow_depth);
+int nhf_get_cfl(nhf_handle *h, nhf_real *ndt, int32_t *arg, nhf_real *flow_depth);
 /* limit_value_t / limit_ids_t (solver_compact.py:330-331,839,854). */
-int nhf_limits(nhf_handle *h, float values[5], int32_t ids[3]);
+int nhf_limits(nhf_handle *h, nhf_real values[5], int32_t ids[3]);
 int nhf_reset_limits(nhf_handle *h);
 /* sample_stations (solver_compact.py:681-687): ids host [n], out host [n][4]
  * = depth, level, u, v. */
-int nhf_sample_stations(nhf_handle *h, const int32_t *ids, int32_t n, float *out);
+int nhf_sample_stations(nhf_handle *h, const int32_t *ids, int32_t n, nhf_real *out);
 /* Face flux sums eq_t [e_num][4] (device destination). */
-int nhf_read_eq(nhf_handle *h, float *eq);
+int nhf_read_eq(nhf_handle *h, nhf_real *eq);
 /* Hanging-edge gradients [hang_cells][2] (device destination). */
-int nhf_read_gradients(nhf_handle *h, float *gradients);
+int nhf_read_gradients(nhf_handle *h, nhf_real *gradients);
 int nhf_synchronize(nhf_handle *h);
 /* The library's own stream (cudaStream_t) on which every batch runs; lets a
  * caller time batches with events on the launching stream. */
@@ -193,7 +207,7 @@ typedef struct nhf_gate {
     int32_t n_flux;          /* recorded sides */
     const int32_t *cell_gate;  /* [e_num] gate of each cell, -1 off gates */
     const int32_t *pond;       /* [e_num] 1 on pond cells, 0 at the sentinel */
-    const float *closed;       /* [e_num] closed (initial) bed */
+    const nhf_real *closed;    /* [e_num] closed (initial) bed */
     const int32_t *targets;    /* [n_targets] gate cells, gate by gate */
     const int32_t *controls;   /* [count] control cell of each gate */
     const int32_t *flux_sides; /* [n_flux] sides between gate and non-gate cells, or pond and non-pond cells */
@@ -257,8 +271,10 @@ int nhf_ensemble_read_trace(nhf_ensemble *e, uint32_t *trace);
  * (held by every device that loads it until exit), which limits it to
  * 67,108,864 sides (larger meshes: NHF_EINVAL). The first call on each
  * device looks up that array's device address and must come before any
- * stream capture. Calls share the array: calls that overlap on the GPU race.
- * Errors are described by nhf_cfl_noalloc_error(). */
+ * stream capture; later calls re-check that address and look it up again
+ * after a context reset. Calls share the array: calls that overlap on the GPU
+ * race. Host pointers are refused (NHF_EINVAL) before any launch.
+ * nhf_cfl_noalloc_error() describes the calling thread's last failure. */
 int nhf_cfl_noalloc(const int32_t *topology, const float *bed, const float *depth, const float *length,
                     const float *q, int32_t s_num, float afa, float g, void *stream, float *ndt_out,
                     int32_t *arg_out);

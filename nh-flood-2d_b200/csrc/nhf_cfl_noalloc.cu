@@ -20,10 +20,15 @@
 // it names a host-side stand-in). On the first call on each device, with that
 // device current, the entry point looks up the device address with
 // cudaGetSymbolAddress and caches it; that first call should therefore come
-// before any stream capture. All calls share the array and it keeps the last
-// call's contents: each call clears the ticket before its kernel runs, and
-// calls whose kernels overlap on the GPU race on the array, so serialise
-// them (one stream, or events between streams).
+// before any stream capture. Every later call checks that the cached address
+// is still device memory of the current context (cudaPointerGetAttributes) and
+// looks it up again if not, so a context torn down by cudaDeviceReset does not
+// leave a stale address behind. All calls share the array and it keeps the
+// last call's contents: each call clears the ticket before its kernel runs,
+// and calls whose kernels overlap on the GPU race on the array, so serialise
+// them (one stream, or events between streams). The inputs and outputs must
+// be device (or managed) memory; a host pointer is refused with NHF_EINVAL
+// before any launch. Error messages are kept per host thread.
 #include <cuda_runtime.h>
 
 #include <cstdarg>
@@ -32,8 +37,12 @@
 #include <string>
 
 #include "../../include/nhflood.h"
+#include "nhf_common.cuh"
 
 namespace {
+
+using nhf::cfl_face_depth;
+using nhf::cfl_value;
 
 constexpr int kNoAllocSlots = 32768;
 constexpr int kThreads = 256;
@@ -47,7 +56,7 @@ static __device__ __align__(256) unsigned long long g_cfl_scratch[kNoAllocSlots 
 
 std::mutex g_setup_mutex;
 unsigned long long *g_scratch_address[kMaxDevices] = {};
-std::string g_error;
+thread_local std::string g_error;  // the calling thread's last failure
 
 int fail(int code, const char *fmt, ...)
 {
@@ -60,11 +69,10 @@ int fail(int code, const char *fmt, ...)
     return code;
 }
 
-__device__ __forceinline__ float maxf(float a, float b) { return a > b ? a : b; }
-
-// Same arithmetic as compute_cfl (solver_compact.py:617-641): interior sides
-// only, face depth floor 0.01, packed (cfl bits << 32 | side) minimum so that
-// ties resolve to the lowest side id.
+// Same arithmetic as compute_cfl (solver_compact.py:617-641), through the same
+// helpers as the handle entry point's k_cfl: interior sides only, face depth
+// floor 0.01, packed (cfl bits << 32 | side) minimum so that ties resolve to
+// the lowest side id.
 __global__ void __launch_bounds__(kThreads)
 k_cfl_noalloc(const int32_t *topology, const float *bed, const float *depth, const float *length,
               const float *q, int32_t s_num, float afa, float g, unsigned long long *scratch,
@@ -79,10 +87,8 @@ k_cfl_noalloc(const int32_t *topology, const float *bed, const float *depth, con
         if (si >= s_num) break;
         int el = topology[3 * si + 1], eh = topology[3 * si + 2];
         if (el == 0 || eh == 0) continue;
-        float zl = bed[el], zh = bed[eh];
-        float head = maxf(zl + depth[el], zh + depth[eh]);
-        float h = maxf(head - maxf(maxf(zl, zh), -999.0f), 0.01f);
-        float cfl = afa * length[si] / (sqrtf(g * h) + fabsf(q[si]) / h);
+        float h = cfl_face_depth(bed[el], depth[el], bed[eh], depth[eh]);
+        float cfl = cfl_value(afa, g, length[si], q[si], h);
         unsigned long long key = ((unsigned long long)__float_as_uint(cfl) << 32) | (unsigned long long)si;
         best = key < best ? key : best;
     }
@@ -142,6 +148,15 @@ int scratch_for_current_device(unsigned long long **out)
     if (e != cudaSuccess) return fail(NHF_ECUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
     if (device < 0 || device >= kMaxDevices) return fail(NHF_EINVAL, "device %d beyond %d devices", device, kMaxDevices);
     std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (g_scratch_address[device]) {
+        // still device memory of the current context? (not after cudaDeviceReset)
+        cudaPointerAttributes attr{};
+        if (cudaPointerGetAttributes(&attr, g_scratch_address[device]) != cudaSuccess ||
+            attr.type != cudaMemoryTypeDevice || attr.device != device) {
+            cudaGetLastError();
+            g_scratch_address[device] = nullptr;
+        }
+    }
     if (!g_scratch_address[device]) {
         void *ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_cfl_scratch);
@@ -150,6 +165,20 @@ int scratch_for_current_device(unsigned long long **out)
         g_scratch_address[device] = (unsigned long long *)ptr;
     }
     *out = g_scratch_address[device];
+    return NHF_OK;
+}
+
+// Inputs and outputs must be memory the kernel can address: device or managed.
+int check_device_pointer(const void *p, const char *name)
+{
+    cudaPointerAttributes attr{};
+    cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NHF_EINVAL, "nhf_cfl_noalloc: %s is not a CUDA pointer (%s)", name, cudaGetErrorString(e));
+    }
+    if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged)
+        return fail(NHF_EINVAL, "nhf_cfl_noalloc: %s is not device memory", name);
     return NHF_OK;
 }
 
@@ -170,6 +199,12 @@ int nhf_cfl_noalloc(const int32_t *topology, const float *bed, const float *dept
         return fail(NHF_EINVAL, "nhf_cfl_noalloc: %d sides exceed the %lld-side limit of its fixed scratch",
                     s_num - 1, kMaxSides);
     if (!(afa > 0.0f) || !(g > 0.0f)) return fail(NHF_EINVAL, "nhf_cfl_noalloc: afa and g must be positive");
+    const void *pointers[7] = {topology, bed, depth, length, q, ndt_out, arg_out};
+    const char *names[7] = {"topology", "bed", "depth", "length", "q", "ndt_out", "arg_out"};
+    for (int i = 0; i < 7; ++i) {
+        int rc = check_device_pointer(pointers[i], names[i]);
+        if (rc) return rc;
+    }
     unsigned long long *scratch = nullptr;
     int rc = scratch_for_current_device(&scratch);
     if (rc) return rc;

@@ -10,8 +10,22 @@
 
 namespace nhf {
 
+// The physics type (nhf_real: float, or double in the FP64 build) and its
+// constants: RC(0.01) is 0.01f in the F32 build.
+typedef nhf_real real;
+#define RC(x) (static_cast<nhf::real>(x))
+#ifdef NHF_REAL_DOUBLE
+typedef unsigned long long scale_bits_t;  // bits of a nonnegative double: same order as the values
+__device__ __forceinline__ scale_bits_t real_bits(double v) { return (scale_bits_t)__double_as_longlong(v); }
+__device__ __forceinline__ double bits_real(scale_bits_t b) { return __longlong_as_double((long long)b); }
+#else
+typedef uint32_t scale_bits_t;  // bits of a nonnegative float: same order as the values
+__device__ __forceinline__ scale_bits_t real_bits(float v) { return __float_as_uint(v); }
+__device__ __forceinline__ float bits_real(scale_bits_t b) { return __uint_as_float(b); }
+#endif
+
 constexpr int kBlock = 256;                 // budget block = reference ei // 256
-constexpr float kDh = -999.0f;              // dh_t without gates (solver_compact.py:405)
+constexpr real kDh = RC(-999.0);            // dh_t without gates (solver_compact.py:405)
 constexpr uint32_t kSnapTicks = 1099512u;   // ceil(1e-6 * 2**40) (clock.py:11)
 constexpr unsigned long long kCflEmpty = 0xFFFFFFFFFFFFFFFFULL;
 
@@ -19,13 +33,17 @@ constexpr unsigned long long kCflEmpty = 0xFFFFFFFFFFFFFFFFULL;
 // limiter counters, CFL result, limiting-edge snapshot) and the batch trace.
 struct Ctl {
     uint32_t now[2], next[2], origin[2], step_end[2];
-    float dt, local, end_local, ndt;
+    float dt, local, end_local;  // the clock's F32 values
+    real ndt;
     int32_t active, slot, raining, cfl_arg;
-    uint32_t limited_cells, limited_faces, min_scale_bits, wet;
+    uint32_t limited_cells, limited_faces, wet;
+    scale_bits_t min_scale_bits;
     unsigned long long cfl_packed;
+    unsigned long long cfl_min_bits;  // FP64 build: the CFL minimum's bits, then
+    int32_t cfl_arg_min;              // the lowest side id that attains it
     uint32_t done_blocks;
     int32_t parity;  // 1: the current depth/q/rain_time live in the second buffers
-    float limit_value[5];
+    real limit_value[5];
     int32_t limit_ids[3];
     uint32_t trace[NHF_MAX_BATCH * NHF_TRACE_COLS];
 };
@@ -49,7 +67,7 @@ struct TilePlan {
 struct GateDev {
     int32_t count, n_targets, n_flux, terms, blocks;
     const int32_t *cell_gate, *pond, *targets, *controls, *flux_sides;
-    const float *closed;
+    const real *closed;
     uint32_t formal_hi, formal_lo;
     float trigger_level, opening_seconds, open_elevation;
     int32_t *commanded, *flow_seen, *opened;
@@ -59,23 +77,26 @@ struct GateDev {
 
 struct Dev {
     nhf_mesh m;
-    float g, neg_g, afa, sita, half_rest, seven_thirds, min_h, min_dt;
+    real g, neg_g, afa, sita, half_rest, seven_thirds, min_h;
+    float min_dt;
     int32_t terms, blocks, batch_size, theta_one;
     Ctl *ctl;
-    const float *coef;
-    float *values, *level_values, *rain_rates, *sdc, *donor_scale, *face_qn, *eq, *gradients;
+    const real *coef;
+    real *values, *level_values, *rain_rates, *sdc, *donor_scale, *face_qn, *eq, *gradients;
     double *acc_sum, *acc_comp;
     // second buffers of the double-buffered state (tiled form)
-    float *depth_b, *q_b, *rain_time_b;
+    real *depth_b, *q_b, *rain_time_b;
     float2 *sdn;  // per side {centre distance, Manning n} (tiled form; filled by initialize)
     TilePlan plan;
 };
 
 __device__ __forceinline__ float maxf(float a, float b) { return a > b ? a : b; }
 __device__ __forceinline__ float minf(float a, float b) { return b < a ? b : a; }
+__device__ __forceinline__ real rmax(real a, real b) { return a > b ? a : b; }
+__device__ __forceinline__ real rmin(real a, real b) { return b < a ? b : a; }
 
-__device__ __forceinline__ const float *cur_depth(const Dev &d, int parity) { return parity ? d.depth_b : d.m.depth; }
-__device__ __forceinline__ const float *cur_q(const Dev &d, int parity) { return parity ? d.q_b : d.m.q; }
+__device__ __forceinline__ const real *cur_depth(const Dev &d, int parity) { return parity ? d.depth_b : d.m.depth; }
+__device__ __forceinline__ const real *cur_q(const Dev &d, int parity) { return parity ? d.q_b : d.m.q; }
 
 __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 {
@@ -118,15 +139,28 @@ __device__ __forceinline__ void acc_add(double *sum, double *comp, double p)
     *sum = s;
 }
 
+// Face depth and CFL value of an interior side (solver_compact.py:628-631):
+// h = max(max(eta_l, eta_h) - max(z_l, z_h, dh), 0.01), cfl = afa L / (sqrt(g h) + |q| / h).
+__device__ __forceinline__ real cfl_face_depth(real zl, real depth_l, real zh, real depth_h)
+{
+    real head = rmax(zl + depth_l, zh + depth_h);
+    return rmax(head - rmax(rmax(zl, zh), kDh), RC(0.01));
+}
+
+__device__ __forceinline__ real cfl_value(real afa, real g, real length, real q, real h)
+{
+    return afa * length / (sqrt(g * h) + fabs(q) / h);
+}
+
 // flow_depth_t[si] (solver_compact.py:628-630) from a depth array; side 0
 // keeps the field's initial zero.
-__device__ __forceinline__ float flow_depth_of(const nhf_mesh &m, const float *depth, int si)
+__device__ __forceinline__ real flow_depth_of(const nhf_mesh &m, const real *depth, int si)
 {
-    if (si == 0) return 0.0f;
+    if (si == 0) return RC(0);
     int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
-    float zl = m.bed[el], zh = m.bed[eh];
-    float head = maxf(zl + __ldcg(depth + el), zh + __ldcg(depth + eh));
-    return maxf(head - maxf(maxf(zl, zh), kDh), 0.01f);
+    real zl = m.bed[el], zh = m.bed[eh];
+    real head = rmax(zl + __ldcg(depth + el), zh + __ldcg(depth + eh));
+    return rmax(head - rmax(rmax(zl, zh), kDh), RC(0.01));
 }
 
 // StepClock.choose (clock.py:94-167)
@@ -192,26 +226,27 @@ __device__ __forceinline__ void clock_choose(const Dev &d, Ctl *c, float candida
 
 // prepare_step (solver_compact.py:364-382) for trace slot c->slot; `depth` and
 // `q` are the current state (read through L2: written by other blocks).
-__device__ __forceinline__ void prepare_step(const Dev &d, Ctl *c, const float *depth, const float *q)
+__device__ __forceinline__ void prepare_step(const Dev &d, Ctl *c, const real *depth, const real *q)
 {
     const nhf_mesh &m = d.m;
-    clock_choose(d, c, c->ndt, c->slot);
+    clock_choose(d, c, (float)c->ndt, c->slot);
     if (!c->active) return;
     c->limited_cells = 0; c->limited_faces = 0;
-    c->min_scale_bits = __float_as_uint(1.0f);
+    c->min_scale_bits = real_bits(RC(1.0));
     c->wet = 0;
+    const real local = c->local, end_local = c->end_local, dt = c->dt;
     for (int bi = 0; bi < m.b_num; ++bi) {
-        d.values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * (c->local + c->dt / 2.0f);
-        d.level_values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * c->end_local;
+        d.values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * (local + dt / RC(2.0));
+        d.level_values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * end_local;
     }
     if (c->ndt < c->limit_value[0]) {
         int si = c->cfl_arg;
         int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
-        float h = flow_depth_of(m, depth, si);
+        real h = flow_depth_of(m, depth, si);
         c->limit_value[0] = c->ndt;
         c->limit_value[1] = __ldcg(depth + el); c->limit_value[2] = __ldcg(depth + eh);
         c->limit_value[3] = h;
-        c->limit_value[4] = __ldcg(q + si) / maxf(h, 1e-30f);
+        c->limit_value[4] = __ldcg(q + si) / rmax(h, RC(1e-30));
         c->limit_ids[0] = si; c->limit_ids[1] = el; c->limit_ids[2] = eh;
     }
 }
@@ -223,7 +258,7 @@ __device__ __forceinline__ void finish_step(Ctl *c)
     if (c->active) {
         row[6] = c->limited_cells;
         row[7] = c->limited_faces;
-        row[8] = c->min_scale_bits;
+        row[8] = __float_as_uint((float)bits_real(c->min_scale_bits));
         row[9] = c->wet;
         c->now[0] = c->step_end[0]; c->now[1] = c->step_end[1];
         row[0] = __float_as_uint(c->dt);
@@ -234,32 +269,32 @@ __device__ __forceinline__ void finish_step(Ctl *c)
 }
 
 // PressureReconstruction.difference (pressure.py:118-129)
-__device__ __forceinline__ float pressure_difference(const Dev &d, const float *depth, int side, int lower,
-                                                     int higher, float raw)
+__device__ __forceinline__ real pressure_difference(const Dev &d, const real *depth, int side, int lower,
+                                                    int higher, real raw)
 {
     const nhf_mesh &m = d.m;
-    float result = raw;
+    real result = raw;
     int index = m.edge_index[side];
     if (index >= 0 && depth[lower] > d.min_h && depth[higher] > d.min_h) {
         int axis = m.topology[3 * side] == 2 ? 1 : 0;
-        float o0 = m.offsets[2 * index], o1 = m.offsets[2 * index + 1];
-        if (o0 != 0.0f) result -= d.gradients[2 * m.slots[2 * index] + axis] * o0;
-        if (o1 != 0.0f) result += d.gradients[2 * m.slots[2 * index + 1] + axis] * o1;
+        real o0 = m.offsets[2 * index], o1 = m.offsets[2 * index + 1];
+        if (o0 != RC(0)) result -= d.gradients[2 * m.slots[2 * index] + axis] * o0;
+        if (o1 != RC(0)) result += d.gradients[2 * m.slots[2 * index + 1] + axis] * o1;
     }
     return result;
 }
 
 // boundary_neighbor_sum (solver_compact.py:135-149)
-__device__ __forceinline__ float boundary_neighbor_sum(float q, float left, float right, float lext, float rext)
+__device__ __forceinline__ real boundary_neighbor_sum(real q, real left, real right, real lext, real rext)
 {
-    float result = left + right;
-    if (lext > 0.0f || rext > 0.0f) {
-        if (lext == 1.0f || rext == 1.0f) {
-            result = 2.0f * q;
+    real result = left + right;
+    if (lext > RC(0) || rext > RC(0)) {
+        if (lext == RC(1) || rext == RC(1)) {
+            result = RC(2) * q;
         } else {
-            float product = lext * rext;
-            result = ((1.0f - rext) * left + (1.0f - lext) * right
-                      + 2.0f * q * (lext + rext - 2.0f * product)) / (1.0f - product);
+            real product = lext * rext;
+            result = ((RC(1) - rext) * left + (RC(1) - lext) * right
+                      + RC(2) * q * (lext + rext - RC(2) * product)) / (RC(1) - product);
         }
     }
     return result;
@@ -290,8 +325,8 @@ __device__ __forceinline__ void gate_move_beds(const Dev &d, const GateDev &g, u
                 g.opened_at[2 * gate] = hi; g.opened_at[2 * gate + 1] = lo;
             }
         } else {
-            float closed = g.closed[cell];
-            m.bed[cell] = closed + (g.open_elevation - closed) * fraction;
+            real closed = g.closed[cell];
+            m.bed[cell] = closed + ((real)g.open_elevation - closed) * (real)fraction;
         }
     }
 }
@@ -302,7 +337,7 @@ __device__ __forceinline__ void gate_move_beds(const Dev &d, const GateDev &g, u
 __device__ __forceinline__ void gate_check(const Dev &d, const GateDev &g, uint32_t hi, uint32_t lo)
 {
     const nhf_mesh &m = d.m;
-    const float *depth = cur_depth(d, d.ctl->parity);
+    const real *depth = cur_depth(d, d.ctl->parity);
     const bool formal = hi > g.formal_hi || (hi == g.formal_hi && lo >= g.formal_lo);
     for (int gate = threadIdx.x; formal && gate < g.count; gate += blockDim.x) {
         int cell = g.controls[gate];

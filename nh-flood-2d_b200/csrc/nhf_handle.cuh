@@ -18,10 +18,10 @@ struct nhf_handle {
     uint32_t *h_begin = nullptr;  // pinned {next, origin}
     uint32_t *d_begin = nullptr;
     uint32_t *h_trace = nullptr;  // pinned
-    float *h_small = nullptr;     // pinned staging for forcing / scalars
+    nhf::real *h_small = nullptr; // pinned staging for forcing / scalars
     double *h_acc = nullptr;      // pinned budget staging
     int32_t *d_ids = nullptr;
-    float *d_samples = nullptr;
+    nhf::real *d_samples = nullptr;
     int ids_cap = 0;
     cudaGraph_t graph_def = nullptr;
     cudaGraphExec_t graph = nullptr;

@@ -93,4 +93,19 @@ __device__ __forceinline__ float pow_f32(float x, float y)
 
 __device__ __forceinline__ float exp_f32(float a) { return (float)exp_f64((double)a); }
 
+// The same two functions in the build's physics type: rounded once to F32,
+// or in the FP64 build kept in double.
+#ifdef NHF_REAL_DOUBLE
+__device__ __forceinline__ double pow_real(double x, double y)
+{
+    if (x != x) return x;
+    if (x == 0.0) return 0.0;
+    return exp_f64(y * ln_f64(x));
+}
+__device__ __forceinline__ double exp_real(double a) { return exp_f64(a); }
+#else
+__device__ __forceinline__ float pow_real(float x, float y) { return pow_f32(x, y); }
+__device__ __forceinline__ float exp_real(float a) { return exp_f32(a); }
+#endif
+
 }  // namespace nhf

@@ -40,18 +40,30 @@ namespace {
 
 // --------------------------------------------------------------- small kernels
 
+// eq_t[ei][0..3] (one 16-byte store in the F32 build)
+__device__ __forceinline__ void store4(real *p, real a, real b, real c, real e)
+{
+#ifdef NHF_REAL_DOUBLE
+    p[0] = a; p[1] = b; p[2] = c; p[3] = e;
+#else
+    *reinterpret_cast<float4 *>(p) = make_float4(a, b, c, e);
+#endif
+}
+
 __global__ void k_initialize(Dev d)
 {
     const nhf_mesh &m = d.m;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 1 && i < m.e_num) {
-        m.depth[i] = 0.0f;
+        m.depth[i] = RC(0.0);
         m.infiltration[i] = m.f0[i];
     }
     if (i >= 1 && i < m.s_num) {
         int so = m.topology[3 * i], el = m.topology[3 * i + 1], eh = m.topology[3 * i + 2];
-        d.sdc[i] = so == 2 ? maxf(fabsf(m.x[eh] - m.x[el]), 0.01f) : maxf(fabsf(m.y[eh] - m.y[el]), 0.01f);
+        d.sdc[i] = so == 2 ? rmax(fabs(m.x[eh] - m.x[el]), RC(0.01)) : rmax(fabs(m.y[eh] - m.y[el]), RC(0.01));
+#ifndef NHF_REAL_DOUBLE
         if (d.sdn) d.sdn[i] = make_float2(d.sdc[i], m.side_n[i]);
+#endif
     }
 }
 
@@ -82,13 +94,13 @@ __global__ void k_prepare(Dev d)
 
 // ------------------------------------------------------ pressure (pressure.py)
 
-__device__ void face_difference(const Dev &d, const float *depth, int cell, int direction, int axis,
-                                float &value_out, float &distance_out, int &usable_out)
+__device__ void face_difference(const Dev &d, const real *depth, int cell, int direction, int axis,
+                                real &value_out, real &distance_out, int &usable_out)
 {
     const nhf_mesh &m = d.m;
-    float value = 0.0f, distance = 0.0f, total = 0.0f;
+    real value = RC(0.0), distance = RC(0.0), total = RC(0.0);
     int usable = 1;
-    float eta = m.bed[cell] + depth[cell];
+    real eta = m.bed[cell] + depth[cell];
     int start = m.face_ptr[4 * cell + direction];
     int count = m.face_count[4 * cell + direction];
     for (int j = 0; j < count; ++j) {
@@ -97,14 +109,14 @@ __device__ void face_difference(const Dev &d, const float *depth, int cell, int 
         if (other == 0 || depth[other] <= d.min_h) {
             usable = 0;
         } else {
-            float weight = m.length[side];
+            real weight = m.length[side];
             value += weight * ((m.bed[other] + depth[other]) - eta);
-            float delta = axis == 1 ? m.y[other] - m.y[cell] : m.x[other] - m.x[cell];
+            real delta = axis == 1 ? m.y[other] - m.y[cell] : m.x[other] - m.x[cell];
             distance += weight * delta;
             total += weight;
         }
     }
-    if (total > 0.0f) { value /= total; distance /= total; }
+    if (total > RC(0.0)) { value /= total; distance /= total; }
     else usable = 0;
     value_out = value; distance_out = distance; usable_out = usable;
 }
@@ -116,13 +128,13 @@ __global__ void k_pressure(Dev d)
     int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= m.hang_cells) return;
     int cell = m.hcells[slot];
-    const float *depth = cur_depth(d, d.ctl->parity);
+    const real *depth = cur_depth(d, d.ctl->parity);
     for (int axis = 0; axis < 2; ++axis) {
         if (m.axes[2 * slot + axis] != 1) continue;
-        float value = 0.0f;
+        real value = RC(0.0);
         if (depth[cell] > d.min_h) {
             int minus = axis == 1 ? 2 : 0, plus = axis == 1 ? 3 : 1;
-            float dm, xm, dp, xp; int okm, okp;
+            real dm, xm, dp, xp; int okm, okp;
             face_difference(d, depth, cell, minus, axis, dm, xm, okm);
             face_difference(d, depth, cell, plus, axis, dp, xp, okp);
             if (okm && okp) value = (dp - dm) / (xp - xm);
@@ -141,14 +153,14 @@ __global__ void k_face_qn(Dev d)
     if (!d.ctl->active) return;
     int ei = blockIdx.x * blockDim.x + threadIdx.x;
     if (ei >= m.e_num) return;
-    const float *q = cur_q(d, d.ctl->parity);
+    const real *q = cur_q(d, d.ctl->parity);
     for (int dd = 0; dd < 4; ++dd) {
         int start = m.face_ptr[4 * ei + dd], count = m.face_count[4 * ei + dd];
-        float result = 0.0f;
+        real result = RC(0.0);
         if (count == 1) {
             result = q[m.isl_data[start]];
         } else if (count > 1) {
-            float total = 0.0f, width = 0.0f;
+            real total = RC(0.0), width = RC(0.0);
             for (int o = 0; o < count; ++o) {
                 int side = m.isl_data[start + o];
                 total += q[side] * m.length[side];
@@ -171,33 +183,33 @@ __global__ void k_sides(Dev d)
     if (si >= m.s_num) return;
     const Ctl *c = d.ctl;
     if (!c->active) return;
-    const float dt = c->dt;
-    float bf = m.sbf[si] == 1 ? 0.0f : 1.0f;
+    const real dt = c->dt;
+    real bf = m.sbf[si] == 1 ? RC(0.0) : RC(1.0);
     int so = m.topology[3 * si], el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
-    float zl = m.bed[el], zh = m.bed[eh];
-    float hl = zl + m.depth[el], hr = zh + m.depth[eh];
-    float dx = d.sdc[si];
-    float xq = m.q[si];
-    float xwh = maxf(hl, hr) - maxf(maxf(zl, zh), kDh);
-    float difference = hr - hl;
+    real zl = m.bed[el], zh = m.bed[eh];
+    real hl = zl + m.depth[el], hr = zh + m.depth[eh];
+    real dx = d.sdc[si];
+    real xq = m.q[si];
+    real xwh = rmax(hl, hr) - rmax(rmax(zl, zh), kDh);
+    real difference = hr - hl;
     if (kHanging) difference = pressure_difference(d, m.depth, si, el, eh, difference);
-    float xdq = (d.neg_g * difference / dx) * maxf(xwh, 0.0f) * dt;
-    float n = m.side_n[si];
-    float ratio = 0.0f;
+    real xdq = (d.neg_g * difference / dx) * rmax(xwh, RC(0.0)) * dt;
+    real n = m.side_n[si];
+    real ratio = RC(0.0);
     // xq / p with p = max(wh, 1e-5) ** f32(7/3) > 0: a zero discharge gives a
     // zero ratio without evaluating the power (identical bits).
-    if (xq != 0.0f) ratio = xq / nhf::pow_f32(maxf(xwh, 0.00001f), d.seven_thirds);
-    float xf = 1.0f + d.g * dt * (n * n) * fabsf(ratio);
+    if (xq != RC(0.0)) ratio = xq / nhf::pow_real(rmax(xwh, RC(0.00001)), d.seven_thirds);
+    real xf = RC(1.0) + d.g * dt * (n * n) * fabs(ratio);
     int dl = so == 2 ? 0 : 2, dr = so == 2 ? 1 : 3;
-    float nb;
+    real nb;
     if (kThetaOne) {
-        nb = 0.0f + 0.0f;
+        nb = RC(0.0) + RC(0.0);
     } else {
         nb = boundary_neighbor_sum(xq, d.face_qn[4 * el + dl], d.face_qn[4 * eh + dr],
                                    m.open_face[4 * el + dl], m.open_face[4 * eh + dr]);
     }
-    float new_q = (d.sita * xq + d.half_rest * nb + xdq) / xf;
-    new_q = xwh < d.min_h ? 0.0f : new_q;
+    real new_q = (d.sita * xq + d.half_rest * nb + xdq) / xf;
+    new_q = xwh < d.min_h ? RC(0.0) : new_q;
     new_q *= bf;
     m.q[si] = new_q;
 }
@@ -212,28 +224,28 @@ __global__ void k_donor(Dev d)
     int ei = blockIdx.x * blockDim.x + threadIdx.x + 1;
     bool valid = ei < m.e_num;
     if (!c->active) return;
-    const float dt = c->dt;
+    const real dt = c->dt;
     bool limited = false;
-    float sc = 1.0f;
+    real sc = RC(1.0);
     if (valid) {
         int bi = m.boundary_id[ei];
-        float discharge = 0.0f;
+        real discharge = RC(0.0);
         int kind = bi >= 0 ? m.kind[bi] : -1;
         if (kind == 1) discharge = d.values[bi] * m.weight[ei];
-        float rainq = 0.0f;
+        real rainq = RC(0.0);
         if (c->raining) rainq = d.rain_rates[m.rain_index[ei]];
-        float pipe = 0.0f;
-        float positive = (maxf(pipe, 0.0f) + maxf(discharge, 0.0f)) * dt;
-        float area = m.area[ei];
-        float available = m.depth[ei] * area + positive + rainq * dt * area;
-        float outgoing = (maxf(-pipe, 0.0f) + maxf(-discharge, 0.0f)) * dt;
+        real pipe = RC(0.0);
+        real positive = (rmax(pipe, RC(0.0)) + rmax(discharge, RC(0.0))) * dt;
+        real area = m.area[ei];
+        real available = m.depth[ei] * area + positive + rainq * dt * area;
+        real outgoing = (rmax(-pipe, RC(0.0)) + rmax(-discharge, RC(0.0))) * dt;
         for (int dd = 0; dd < 4; ++dd) {
             int p = m.face_ptr[4 * ei + dd], cnt = m.face_count[4 * ei + dd];
             for (int j = 0; j < cnt; ++j) {
                 int side = m.isl_data[p + j];
-                float signed_q = m.q[side] * m.length[side];
+                real signed_q = m.q[side] * m.length[side];
                 if (dd == 0 || dd == 2) signed_q = -signed_q;
-                outgoing += maxf(signed_q, 0.0f) * dt;
+                outgoing += rmax(signed_q, RC(0.0)) * dt;
             }
         }
         if (outgoing > available && kind != 0) {
@@ -244,9 +256,9 @@ __global__ void k_donor(Dev d)
     }
     unsigned mask = __ballot_sync(0xffffffffu, limited);
     if (mask) {
-        uint32_t bits = __float_as_uint(sc);  // scale >= 0: bit order is value order
+        scale_bits_t bits = real_bits(sc);  // scale >= 0: bit order is value order
         for (int o = 16; o > 0; o >>= 1) {
-            uint32_t w = __shfl_down_sync(0xffffffffu, bits, o);
+            scale_bits_t w = __shfl_down_sync(0xffffffffu, bits, o);
             bits = w < bits ? w : bits;
         }
         if ((threadIdx.x & 31) == 0) {
@@ -268,10 +280,10 @@ __global__ void k_scale(Dev d)
     bool counted = false;
     if (si < m.s_num) {
         int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
-        float q = m.q[si];
-        int donor = q >= 0.0f ? el : eh;
-        float sc = d.donor_scale[donor];
-        counted = q != 0.0f && sc < 1.0f;
+        real q = m.q[si];
+        int donor = q >= RC(0.0) ? el : eh;
+        real sc = d.donor_scale[donor];
+        counted = q != RC(0.0) && sc < RC(1.0);
         m.q[si] = q * sc;
     }
     unsigned mask = __ballot_sync(0xffffffffu, counted);
@@ -291,47 +303,47 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d, GateDev g)
     const nhf_mesh &m = d.m;
     Ctl *c = d.ctl;
     if (!c->active) return;
-    const float dt = c->dt;
+    const real dt = c->dt;
     const int T = d.terms;
     const int B = m.b_num;
     const int blk = blockIdx.x;
     const int ei = blk * kBlock + threadIdx.x;
     const bool valid = ei >= 1 && ei < m.e_num;
-    float t_removed = 0.0f, t_pipe = 0.0f, t_floor = 0.0f;
-    float t_level[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    float t_discharge = 0.0f;
+    real t_removed = RC(0.0), t_pipe = RC(0.0), t_floor = RC(0.0);
+    real t_level[5] = {RC(0.0), RC(0.0), RC(0.0), RC(0.0), RC(0.0)};
+    real t_discharge = RC(0.0);
     int bi = -1, kind = -1;
     bool wet = false;
     int goff = -1;
-    float gv[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    real gv[6] = {RC(0.0), RC(0.0), RC(0.0), RC(0.0), RC(0.0), RC(0.0)};
     if (valid) {
         bi = m.boundary_id[ei];
         kind = bi >= 0 ? m.kind[bi] : -1;
-        float sc = d.donor_scale[ei];
-        float pq = 0.0f;
-        float pipe = maxf(pq, 0.0f) + minf(pq, 0.0f) * sc;
-        float discharge = 0.0f;
+        real sc = d.donor_scale[ei];
+        real pq = RC(0.0);
+        real pipe = rmax(pq, RC(0.0)) + rmin(pq, RC(0.0)) * sc;
+        real discharge = RC(0.0);
         if (kind == 1) {
-            float requested = d.values[bi] * m.weight[ei];
-            discharge = maxf(requested, 0.0f) + minf(requested, 0.0f) * sc;
+            real requested = d.values[bi] * m.weight[ei];
+            discharge = rmax(requested, RC(0.0)) + rmin(requested, RC(0.0)) * sc;
             t_discharge = discharge * dt;
         }
-        float ssq = pipe + discharge;
-        float rainq = 0.0f;
+        real ssq = pipe + discharge;
+        real rainq = RC(0.0);
         if (c->raining) rainq = d.rain_rates[m.rain_index[ei]];
-        float infil = m.infiltration[ei];
-        if (rainq > 0.0f) {
-            float rt = m.rain_time[ei] + dt;
+        real infil = m.infiltration[ei];
+        if (rainq > RC(0.0)) {
+            real rt = m.rain_time[ei] + dt;
             m.rain_time[ei] = rt;
-            float f0 = m.f0[ei], fc = m.fc[ei];
-            float diff = f0 - fc;
+            real f0 = m.f0[ei], fc = m.fc[ei];
+            real diff = f0 - fc;
             // fc + 0 * e == fc for the finite e in (0, 1]: skip exp when f0 == fc.
-            infil = diff == 0.0f ? fc + 0.0f : fc + diff * nhf::exp_f32(-m.k[ei] * rt / 3600.0f);
+            infil = diff == RC(0.0) ? fc + RC(0.0) : fc + diff * nhf::exp_real(-m.k[ei] * rt / RC(3600.0));
             m.infiltration[ei] = infil;
         }
-        float fl[4];
+        real fl[4];
         for (int dd = 0; dd < 4; ++dd) {
-            float face_flux = 0.0f;
+            real face_flux = RC(0.0);
             int p = m.face_ptr[4 * ei + dd], cnt = m.face_count[4 * ei + dd];
             for (int j = 0; j < cnt; ++j) {
                 int si = m.isl_data[p + j];
@@ -339,23 +351,23 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d, GateDev g)
             }
             fl[dd] = face_flux;
         }
-        float ql = fl[0], qr = fl[1], qb = fl[2], qt = fl[3];
-        float tq = ql - qr + qb - qt + ssq;
-        reinterpret_cast<float4 *>(d.eq)[ei] = make_float4(ql, qr, qb, qt);
-        float ea = m.area[ei];
-        float rain_depth = rainq * dt;
-        float increment = tq * dt / ea + rain_depth;
-        float previous = m.depth[ei];
-        float raw_depth = previous + increment;
-        float removed = minf(infil * dt, maxf(raw_depth, 0.0f));
+        real ql = fl[0], qr = fl[1], qb = fl[2], qt = fl[3];
+        real tq = ql - qr + qb - qt + ssq;
+        store4(d.eq + 4 * (size_t)ei, ql, qr, qb, qt);
+        real ea = m.area[ei];
+        real rain_depth = rainq * dt;
+        real increment = tq * dt / ea + rain_depth;
+        real previous = m.depth[ei];
+        real raw_depth = previous + increment;
+        real removed = rmin(infil * dt, rmax(raw_depth, RC(0.0)));
         raw_depth -= removed;
-        float floor_v = maxf(-raw_depth, 0.0f);
+        real floor_v = rmax(-raw_depth, RC(0.0));
         t_removed = removed * ea;
         t_pipe = pipe * dt;
-        float depth;
+        real depth;
         if (kind == 0) {
             t_floor = floor_v * ea;
-            float target = maxf(d.level_values[bi] - m.bed[ei], 0.0f);
+            real target = rmax(d.level_values[bi] - m.bed[ei], RC(0.0));
             t_level[0] = (target - previous) * ea;
             t_level[1] = -(ql - qr + qb - qt) * dt;
             t_level[2] = -pipe * dt;
@@ -364,16 +376,16 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d, GateDev g)
             depth = target;
         } else {
             t_floor = floor_v * ea;
-            depth = maxf(raw_depth, 0.0f);
+            depth = rmax(raw_depth, RC(0.0));
         }
         m.depth[ei] = depth;
         if (kGate) {
             goff = g.pond[ei] == 1 ? 4 * g.count + 2
                  : (g.cell_gate[ei] >= 0 ? 4 * g.count + 8 + 6 * g.cell_gate[ei] : -1);
             if (goff >= 0) {
-                float applied_floor = floor_v, level_exchange = 0.0f;
+                real applied_floor = floor_v, level_exchange = RC(0.0);
                 if (kind == 0) {
-                    applied_floor = 0.0f;
+                    applied_floor = RC(0.0);
                     level_exchange = (depth - previous) * ea - (ql - qr + qb - qt) * dt - pipe * dt
                                      - rain_depth * ea + removed * ea;
                 }
@@ -382,18 +394,18 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d, GateDev g)
                 gv[2] = applied_floor * ea;
                 gv[3] = pipe * dt;
                 gv[4] = (ssq - pipe) * dt + level_exchange;
-                float rounding = (depth - previous) - increment + removed - applied_floor;
+                real rounding = (depth - previous) - increment + removed - applied_floor;
                 gv[5] = rounding * ea - level_exchange;
             }
         }
-        float h = maxf(depth, 0.01f);
-        float u = 0.0f, v = 0.0f;
+        real h = rmax(depth, RC(0.01));
+        real u = RC(0.0), v = RC(0.0);
         if (depth >= d.min_h) {
-            u = (ql + qr) / m.height[ei] / h / 2.0f;
-            v = (qb + qt) / m.width[ei] / h / 2.0f;
+            u = (ql + qr) / m.height[ei] / h / RC(2.0);
+            v = (qb + qt) / m.width[ei] / h / RC(2.0);
         }
         m.u[ei] = u; m.v[ei] = v;
-        m.max_speed[ei] = maxf(m.max_speed[ei], sqrtf(u * u + v * v));
+        m.max_speed[ei] = rmax(m.max_speed[ei], sqrt(u * u + v * v));
         if (depth > m.max_depth[ei]) {
             m.max_depth[ei] = depth;
             m.peak_hi[ei] = c->step_end[0]; m.peak_lo[ei] = c->step_end[1];
@@ -406,14 +418,14 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d, GateDev g)
     double *acc_s = d.acc_sum + (size_t)blk * T;
     double *acc_c = d.acc_comp + (size_t)blk * T;
     for (int t = 0; t < T; ++t) {
-        float val = 0.0f;
+        real val = RC(0.0);
         if (t == 0) val = t_removed;
-        else if (t == 1) val = kind == 0 ? 0.0f : t_floor;
-        else if (t == 2) val = kind == 0 ? t_floor : 0.0f;
+        else if (t == 1) val = kind == 0 ? RC(0.0) : t_floor;
+        else if (t == 2) val = kind == 0 ? t_floor : RC(0.0);
         else if (t == 3) val = t_pipe;
         else if (t < 4 + 5 * B) { int b = (t - 4) / 5; if (b == bi) val = t_level[(t - 4) % 5]; }
         else { int b = t - 4 - 5 * B; if (b == bi) val = t_discharge; }
-        if (!__syncthreads_or(val != 0.0f)) continue;
+        if (!__syncthreads_or(val != RC(0.0))) continue;
         double sum = block_tree((double)val, sh);
         if (threadIdx.x == 0) acc_add(acc_s + t, acc_c + t, sum);
     }
@@ -424,8 +436,8 @@ __global__ void __launch_bounds__(kBlock) k_cells(Dev d, GateDev g)
             if (!__syncthreads_or(goff == off)) continue;
 #pragma unroll
             for (int k = 0; k < 6; ++k) {
-                float val = goff == off ? gv[k] : 0.0f;
-                if (!__syncthreads_or(val != 0.0f)) continue;
+                real val = goff == off ? gv[k] : RC(0.0);
+                if (!__syncthreads_or(val != RC(0.0))) continue;
                 double sum = block_tree((double)val, sh);
                 if (threadIdx.x == 0) {
                     size_t idx = (size_t)blk * g.terms + off + k;
@@ -468,15 +480,15 @@ __global__ void __launch_bounds__(kBlock) k_gate_flux(Dev d, GateDev g, int move
     if (!c->active) return;
     const int p = blockIdx.x * kBlock + threadIdx.x;
     int term = -1;
-    float v0 = 0.0f, v1 = 0.0f;
+    real v0 = RC(0.0), v1 = RC(0.0);
     if (p < g.n_flux) {
         int si = g.flux_sides[p];
         int left = m.topology[3 * si + 1], right = m.topology[3 * si + 2];
-        float volume = cur_q(d, c->parity)[si] * m.length[si] * c->dt;
+        real volume = cur_q(d, c->parity)[si] * m.length[si] * c->dt;
         int gl = g.cell_gate[left], gr = g.cell_gate[right];
         int pl = g.pond[left], pr = g.pond[right];
         int latch = -1;
-        float into = 0.0f;
+        real into = RC(0.0);
         if (gl >= 0 && gr < 0) {
             if (pr == 1) { term = 4 * gl; into = volume; latch = gl; }
             else { term = 4 * gl + 2; into = -volume; }
@@ -487,16 +499,16 @@ __global__ void __launch_bounds__(kBlock) k_gate_flux(Dev d, GateDev g, int move
             term = 4 * g.count;
             into = pr == 1 ? volume : -volume;
         }
-        if (latch >= 0 && volume != 0.0f && atomicOr(&g.flow_seen[latch], 1) == 0) {
+        if (latch >= 0 && volume != RC(0.0) && atomicOr(&g.flow_seen[latch], 1) == 0) {
             g.first_flow[2 * latch] = c->step_end[0]; g.first_flow[2 * latch + 1] = c->step_end[1];
         }
-        v0 = maxf(into, 0.0f);
-        v1 = maxf(-into, 0.0f);
+        v0 = rmax(into, RC(0.0));
+        v1 = rmax(-into, RC(0.0));
     }
     const int T = 4 * g.count + 2;
     for (int t = 0; t < T; ++t) {
-        float val = term < 0 ? 0.0f : (t == term ? v0 : (t == term + 1 ? v1 : 0.0f));
-        if (!__syncthreads_or(val != 0.0f)) continue;
+        real val = term < 0 ? RC(0.0) : (t == term ? v0 : (t == term + 1 ? v1 : RC(0.0)));
+        if (!__syncthreads_or(val != RC(0.0))) continue;
         double sum = block_tree((double)val, sh);
         if (threadIdx.x == 0) {
             size_t idx = (size_t)blockIdx.x * g.terms + t;
@@ -511,6 +523,9 @@ __global__ void __launch_bounds__(kBlock) k_gate_flux(Dev d, GateDev g, int move
 // compute_cfl (solver_compact.py:617-641) + finish_step (384-391).
 // Packed key (cfl bits << 32 | side): the minimum is the smallest CFL and,
 // among equal values, the lowest side id, as the reference's second pass.
+// The FP64 build cannot pack a double and a side id in 64 bits: it takes the
+// reference's two passes, the minimum's bits (k_cfl) and then the lowest
+// side attaining it (k_cfl_arg).
 __global__ void k_cfl(Dev d, int finish)
 {
     __shared__ unsigned long long sh[32];
@@ -525,11 +540,13 @@ __global__ void k_cfl(Dev d, int finish)
     for (int si = blockIdx.x * blockDim.x + threadIdx.x + 1; si < m.s_num; si += gridDim.x * blockDim.x) {
         int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
         if (el != 0 && eh != 0) {
-            float zl = m.bed[el], zh = m.bed[eh];
-            float head = maxf(zl + m.depth[el], zh + m.depth[eh]);
-            float h = maxf(head - maxf(maxf(zl, zh), kDh), 0.01f);
-            float cfl = d.afa * m.length[si] / (sqrtf(d.g * h) + fabsf(m.q[si]) / h);
+            real h = cfl_face_depth(m.bed[el], m.depth[el], m.bed[eh], m.depth[eh]);
+            real cfl = cfl_value(d.afa, d.g, m.length[si], m.q[si], h);
+#ifdef NHF_REAL_DOUBLE
+            unsigned long long key = (unsigned long long)__double_as_longlong(cfl);
+#else
             unsigned long long key = ((unsigned long long)__float_as_uint(cfl) << 32) | (unsigned)si;
+#endif
             best = key < best ? key : best;
         }
     }
@@ -552,6 +569,11 @@ __global__ void k_cfl(Dev d, int finish)
     __threadfence();
     unsigned long long packed = atomicExch(&c->cfl_packed, kCflEmpty);
     c->done_blocks = 0;
+#ifdef NHF_REAL_DOUBLE
+    c->cfl_min_bits = packed;
+    c->ndt = packed == kCflEmpty ? __longlong_as_double(0x7ff0000000000000LL) : __longlong_as_double((long long)packed);
+    c->cfl_arg_min = m.s_num;
+#else
     if (packed == kCflEmpty) {
         c->ndt = __uint_as_float(0x7f800000u);
         c->cfl_arg = 0;
@@ -560,23 +582,79 @@ __global__ void k_cfl(Dev d, int finish)
         c->cfl_arg = (int32_t)(packed & 0xffffffffu);
     }
     if (finish) finish_step(c);
+#endif
 }
+
+#ifdef NHF_REAL_DOUBLE
+// The lowest interior side whose CFL value equals the minimum (0 when there
+// is none), then finish_step.
+__global__ void k_cfl_arg(Dev d, int finish)
+{
+    __shared__ int sh[32];
+    __shared__ bool last;
+    const nhf_mesh &m = d.m;
+    Ctl *c = d.ctl;
+    if (!c->active) {
+        if (finish && blockIdx.x == 0 && threadIdx.x == 0) c->slot += 1;
+        return;
+    }
+    const unsigned long long target = c->cfl_min_bits;
+    int best = m.s_num;
+    if (target != kCflEmpty) {
+        for (int si = blockIdx.x * blockDim.x + threadIdx.x + 1; si < m.s_num; si += gridDim.x * blockDim.x) {
+            int el = m.topology[3 * si + 1], eh = m.topology[3 * si + 2];
+            if (el != 0 && eh != 0) {
+                real h = cfl_face_depth(m.bed[el], m.depth[el], m.bed[eh], m.depth[eh]);
+                real cfl = cfl_value(d.afa, d.g, m.length[si], m.q[si], h);
+                if ((unsigned long long)__double_as_longlong(cfl) == target && si < best) best = si;
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        int w = __shfl_down_sync(0xffffffffu, best, o);
+        best = w < best ? w : best;
+    }
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sh[warp] = best;
+    __syncthreads();
+    if (warp == 0) {
+        best = lane < (int)(blockDim.x >> 5) ? sh[lane] : m.s_num;
+        for (int o = 16; o > 0; o >>= 1) {
+            int w = __shfl_down_sync(0xffffffffu, best, o);
+            best = w < best ? w : best;
+        }
+        if (lane == 0) {
+            if (best < m.s_num) atomicMin(&c->cfl_arg_min, best);
+            __threadfence();
+            unsigned ticket = atomicAdd(&c->done_blocks, 1u);
+            last = ticket == gridDim.x - 1;
+        }
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    c->done_blocks = 0;
+    const int arg = atomicExch(&c->cfl_arg_min, m.s_num);
+    c->cfl_arg = arg >= m.s_num ? 0 : arg;
+    if (finish) finish_step(c);
+}
+#endif
 
 // ------------------------------------------------------- setup and sampling
 
 // apply_initial_levels (solver_compact.py:412-420)
-__global__ void __launch_bounds__(kBlock) k_apply_levels(Dev d, const float *targets)
+__global__ void __launch_bounds__(kBlock) k_apply_levels(Dev d, const real *targets)
 {
     __shared__ double sh[kBlock];
     const nhf_mesh &m = d.m;
     const int T = d.terms;
     int blk = blockIdx.x, ei = blk * kBlock + threadIdx.x;
     int bi = -1;
-    float val = 0.0f;
+    real val = RC(0.0);
     if (ei >= 1 && ei < m.e_num) {
         bi = m.boundary_id[ei];
         if (bi >= 0 && m.kind[bi] == 0) {
-            float previous = m.depth[ei];
+            real previous = m.depth[ei];
             m.depth[ei] = targets[ei];
             val = (targets[ei] - previous) * m.area[ei];
         } else {
@@ -584,8 +662,8 @@ __global__ void __launch_bounds__(kBlock) k_apply_levels(Dev d, const float *tar
         }
     }
     for (int b = 0; b < m.b_num; ++b) {
-        float v = b == bi ? val : 0.0f;
-        if (!__syncthreads_or(v != 0.0f)) continue;
+        real v = b == bi ? val : RC(0.0);
+        if (!__syncthreads_or(v != RC(0.0))) continue;
         double sum = block_tree((double)v, sh);
         int t = 4 + 5 * b;
         if (threadIdx.x == 0) acc_add(d.acc_sum + (size_t)blk * T + t, d.acc_comp + (size_t)blk * T + t, sum);
@@ -598,9 +676,9 @@ __global__ void k_initial_diag(Dev d)
     const nhf_mesh &m = d.m;
     int ei = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (ei >= m.e_num) return;
-    float fl[4];
+    real fl[4];
     for (int dd = 0; dd < 4; ++dd) {
-        float total = 0.0f;
+        real total = RC(0.0);
         int p = m.face_ptr[4 * ei + dd], cnt = m.face_count[4 * ei + dd];
         for (int j = 0; j < cnt; ++j) {
             int si = m.isl_data[p + j];
@@ -608,16 +686,16 @@ __global__ void k_initial_diag(Dev d)
         }
         fl[dd] = total;
     }
-    reinterpret_cast<float4 *>(d.eq)[ei] = make_float4(fl[0], fl[1], fl[2], fl[3]);
-    float depth = m.depth[ei];
-    float h = maxf(depth, 0.01f);
-    float u = 0.0f, v = 0.0f;
+    store4(d.eq + 4 * (size_t)ei, fl[0], fl[1], fl[2], fl[3]);
+    real depth = m.depth[ei];
+    real h = rmax(depth, RC(0.01));
+    real u = RC(0.0), v = RC(0.0);
     if (depth >= d.min_h) {
-        u = (fl[0] + fl[1]) / m.height[ei] / h / 2.0f;
-        v = (fl[2] + fl[3]) / m.width[ei] / h / 2.0f;
+        u = (fl[0] + fl[1]) / m.height[ei] / h / RC(2.0);
+        v = (fl[2] + fl[3]) / m.width[ei] / h / RC(2.0);
     }
     m.u[ei] = u; m.v[ei] = v;
-    m.max_speed[ei] = maxf(m.max_speed[ei], sqrtf(u * u + v * v));
+    m.max_speed[ei] = rmax(m.max_speed[ei], sqrt(u * u + v * v));
     if (depth > m.max_depth[ei]) {
         m.max_depth[ei] = depth;
         m.peak_hi[ei] = d.ctl->now[0]; m.peak_lo[ei] = d.ctl->now[1];
@@ -631,13 +709,13 @@ __global__ void k_reset_extrema(Dev d)
     int ei = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (ei >= m.e_num) return;
     m.max_depth[ei] = m.depth[ei];
-    float u = m.u[ei], v = m.v[ei];
-    m.max_speed[ei] = sqrtf(u * u + v * v);
+    real u = m.u[ei], v = m.v[ei];
+    m.max_speed[ei] = sqrt(u * u + v * v);
     m.peak_hi[ei] = d.ctl->now[0]; m.peak_lo[ei] = d.ctl->now[1];
 }
 
 // sample_stations (solver_compact.py:681-687)
-__global__ void k_sample(Dev d, const int32_t *ids, int n, float *out)
+__global__ void k_sample(Dev d, const int32_t *ids, int n, real *out)
 {
     const nhf_mesh &m = d.m;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -649,12 +727,13 @@ __global__ void k_sample(Dev d, const int32_t *ids, int n, float *out)
     out[4 * i + 3] = m.v[ei];
 }
 
-__global__ void k_cfl_edge(Dev d, float *out)
+// ndt, flow depth of the limiting side, and the side (an int32 after the two values)
+__global__ void k_cfl_edge(Dev d, real *out)
 {
     const Ctl *c = d.ctl;
     out[0] = c->ndt;
-    out[1] = __int_as_float(c->cfl_arg);
-    out[2] = flow_depth_of(d.m, d.m.depth, c->cfl_arg);
+    out[1] = flow_depth_of(d.m, d.m.depth, c->cfl_arg);
+    *reinterpret_cast<int32_t *>(out + 2) = c->cfl_arg;
 }
 
 // eq_t from the current discharges (solver_compact.py:548-559 face sums)
@@ -663,9 +742,9 @@ __global__ void k_eq(Dev d)
     const nhf_mesh &m = d.m;
     int ei = blockIdx.x * blockDim.x + threadIdx.x + 1;
     if (ei >= m.e_num) return;
-    float fl[4];
+    real fl[4];
     for (int dd = 0; dd < 4; ++dd) {
-        float total = 0.0f;
+        real total = RC(0.0);
         int p = m.face_ptr[4 * ei + dd], cnt = m.face_count[4 * ei + dd];
         for (int j = 0; j < cnt; ++j) {
             int si = m.isl_data[p + j];
@@ -673,7 +752,7 @@ __global__ void k_eq(Dev d)
         }
         fl[dd] = total;
     }
-    reinterpret_cast<float4 *>(d.eq)[ei] = make_float4(fl[0], fl[1], fl[2], fl[3]);
+    store4(d.eq + 4 * (size_t)ei, fl[0], fl[1], fl[2], fl[3]);
 }
 
 }  // namespace
@@ -705,6 +784,17 @@ int fail(nhf_handle *h, int code, const char *fmt, ...)
     } while (0)
 
 inline int grid_for(int n, int b) { return n <= 0 ? 1 : (n + b - 1) / b; }
+
+// compute_cfl, and finish_step when `finish`: one pass, or two in the FP64 build
+void enqueue_cfl(nhf_handle *h, cudaStream_t s, int finish)
+{
+    int gc = grid_for(h->m.s_num - 1, 256);
+    if (gc > 148 * 8) gc = 148 * 8;
+    k_cfl<<<gc, 256, 0, s>>>(h->dev, finish);
+#ifdef NHF_REAL_DOUBLE
+    k_cfl_arg<<<gc, 256, 0, s>>>(h->dev, finish);
+#endif
+}
 
 int enter(nhf_handle *h)
 {
@@ -747,9 +837,7 @@ void enqueue_step(nhf_handle *h)
     } else {
         k_cells<false><<<d.blocks, kBlock, 0, s>>>(d, h->gate);
     }
-    int gc = grid_for(m.s_num - 1, 256);
-    if (gc > 148 * 8) gc = 148 * 8;
-    k_cfl<<<gc, 256, 0, s>>>(d, 1);
+    enqueue_cfl(h, s, 1);
 }
 
 int build_graph(nhf_handle *h)
@@ -757,6 +845,7 @@ int build_graph(nhf_handle *h)
     cudaGraph_t g = nullptr;
     CK(h, cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
     k_begin<<<1, 256, 0, h->s>>>(h->dev, 0u, 0u, 0u, 0u, h->tiled ? 1 : 0);
+#ifndef NHF_REAL_DOUBLE
     if (h->tiled) {
         tiled_enqueue_batch_start(h->dev, h->s);
         for (int i = 0; i < h->p.batch_size; ++i) {
@@ -777,7 +866,9 @@ int build_graph(nhf_handle *h)
             }
         }
         tiled_enqueue_batch_end(h->dev, h->s);
-    } else {
+    } else
+#endif
+    {
         for (int i = 0; i < h->p.batch_size; ++i) enqueue_step(h);
     }
     cudaMemcpyAsync(h->h_trace, h->ctl->trace, sizeof(uint32_t) * NHF_TRACE_COLS * h->p.batch_size,
@@ -843,7 +934,13 @@ int member_graph_launch(nhf_handle *h, const uint32_t target[2], const uint32_t 
 
 extern "C" {
 
-const char *nhf_version(void) { return "nhflood-b200 0.1 (sm_100a)"; }
+#ifdef NHF_REAL_DOUBLE
+const char *nhf_version(void) { return "nhflood-b200 0.2 (sm_100a, FP64 build)"; }
+#else
+const char *nhf_version(void) { return "nhflood-b200 0.2 (sm_100a)"; }
+#endif
+
+int nhf_real_bytes(void) { return (int)sizeof(nhf_real); }
 
 const char *nhf_last_error(const nhf_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
@@ -855,7 +952,7 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
         return fail(nullptr, NHF_EINVAL, "invalid mesh sizes");
     if (params->batch_size < 1 || params->batch_size > NHF_MAX_BATCH)
         return fail(nullptr, NHF_EINVAL, "batch_size must be between 1 and %d", NHF_MAX_BATCH);
-    if (params->sita != 1.0f && !mesh->open_face)
+    if (params->sita != RC(1) && !mesh->open_face)
         return fail(nullptr, NHF_EINVAL, "theta < 1 needs open_face fractions");
     if (mesh->hang_cells > 0 && (!mesh->edge_index || !mesh->offsets || !mesh->slots || !mesh->hcells || !mesh->axes))
         return fail(nullptr, NHF_EINVAL, "hanging geometry arrays missing");
@@ -881,10 +978,13 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     const int blocks = (e + kBlock - 1) / kBlock;
     const int hc = mesh->hang_cells > 0 ? mesh->hang_cells : 1;
     const int nr = mesh->n_rates > 0 ? mesh->n_rates : 1;
-    const bool theta_one = params->sita == 1.0f;
+    const bool theta_one = params->sita == RC(1);
     // The caller may still be writing the mesh arrays on its stream.
     CKC(cudaEventRecord(h->ev_in, h->user));
     CKC(cudaStreamWaitEvent(h->s, h->ev_in, 0));
+#ifdef NHF_REAL_DOUBLE
+    h->path = "multipass (FP64 build)";
+#else
     // Fused tiled step when the mesh allows it (params->path 0, or a tile size).
     if (params->path == 0 || params->path == 256 || params->path == 512 || params->path == 1024) {
         char why[256] = {0};
@@ -903,25 +1003,26 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
             h->path = std::string("multipass (") + why + ")";
         }
     }
+#endif
     // scratch layout (bytes, 256-aligned pieces)
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
     size_t o_ctl = take(sizeof(Ctl));
-    size_t o_coef = take(sizeof(float) * 2 * bb);
-    size_t o_val = take(sizeof(float) * bb);
-    size_t o_lvl = take(sizeof(float) * bb);
-    size_t o_rain = take(sizeof(float) * nr);
-    size_t o_sdc = take(sizeof(float) * sn);
-    size_t o_donor = take(sizeof(float) * e);
-    size_t o_fqn = take(theta_one ? 16 : sizeof(float) * 4 * (size_t)e);
-    size_t o_eq = take(sizeof(float) * 4 * (size_t)e);
-    size_t o_grad = take(sizeof(float) * 2 * hc);
+    size_t o_coef = take(sizeof(real) * 2 * bb);
+    size_t o_val = take(sizeof(real) * bb);
+    size_t o_lvl = take(sizeof(real) * bb);
+    size_t o_rain = take(sizeof(real) * nr);
+    size_t o_sdc = take(sizeof(real) * sn);
+    size_t o_donor = take(sizeof(real) * e);
+    size_t o_fqn = take(theta_one ? 32 : sizeof(real) * 4 * (size_t)e);
+    size_t o_eq = take(sizeof(real) * 4 * (size_t)e);
+    size_t o_grad = take(sizeof(real) * 2 * hc);
     size_t o_accs = take(sizeof(double) * (size_t)blocks * T);
     size_t o_accc = take(sizeof(double) * (size_t)blocks * T);
-    size_t o_begin = take(sizeof(uint32_t) * 4);
-    size_t o_db = h->tiled ? take(sizeof(float) * (size_t)e) : 0;
-    size_t o_qb = h->tiled ? take(sizeof(float) * (size_t)sn) : 0;
-    size_t o_rb = h->tiled ? take(sizeof(float) * (size_t)e) : 0;
+    size_t o_begin = take(sizeof(real) * 4);  // also the staging of nhf_get_cfl's three words
+    size_t o_db = h->tiled ? take(sizeof(real) * (size_t)e) : 0;
+    size_t o_qb = h->tiled ? take(sizeof(real) * (size_t)sn) : 0;
+    size_t o_rb = h->tiled ? take(sizeof(real) * (size_t)e) : 0;
     size_t o_sdn = h->tiled ? take(sizeof(float2) * (size_t)sn) : 0;
     CKC(cudaMalloc(&h->scratch, off));
     CKC(cudaMemsetAsync(h->scratch, 0, off, h->s));
@@ -930,7 +1031,7 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     h->d_begin = (uint32_t *)(base + o_begin);
     CKC(cudaMallocHost(&h->h_begin, 4 * sizeof(uint32_t)));
     CKC(cudaMallocHost(&h->h_trace, sizeof(uint32_t) * NHF_TRACE_COLS * NHF_MAX_BATCH));
-    CKC(cudaMallocHost(&h->h_small, sizeof(float) * (2 * bb + nr + 64)));
+    CKC(cudaMallocHost(&h->h_small, sizeof(real) * (2 * bb + nr + 64)));
     CKC(cudaMallocHost(&h->h_acc, sizeof(double) * 2 * (size_t)blocks * T + 16));
     Dev &d = h->dev;
     d.m = *mesh;
@@ -938,8 +1039,8 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     d.neg_g = -params->g;
     d.afa = params->afa;
     d.sita = params->sita;
-    d.half_rest = (float)((1.0 - (double)params->sita) / 2.0);
-    d.seven_thirds = (float)(7.0 / 3.0);
+    d.half_rest = (real)((1.0 - (double)params->sita) / 2.0);
+    d.seven_thirds = (real)(7.0 / 3.0);
     d.min_h = params->min_h;
     d.min_dt = params->min_dt;
     d.terms = T;
@@ -947,21 +1048,21 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     d.batch_size = params->batch_size;
     d.theta_one = theta_one ? 1 : 0;
     d.ctl = h->ctl;
-    d.coef = (const float *)(base + o_coef);
-    d.values = (float *)(base + o_val);
-    d.level_values = (float *)(base + o_lvl);
-    d.rain_rates = (float *)(base + o_rain);
-    d.sdc = (float *)(base + o_sdc);
-    d.donor_scale = (float *)(base + o_donor);
-    d.face_qn = (float *)(base + o_fqn);
-    d.eq = (float *)(base + o_eq);
-    d.gradients = (float *)(base + o_grad);
+    d.coef = (const real *)(base + o_coef);
+    d.values = (real *)(base + o_val);
+    d.level_values = (real *)(base + o_lvl);
+    d.rain_rates = (real *)(base + o_rain);
+    d.sdc = (real *)(base + o_sdc);
+    d.donor_scale = (real *)(base + o_donor);
+    d.face_qn = (real *)(base + o_fqn);
+    d.eq = (real *)(base + o_eq);
+    d.gradients = (real *)(base + o_grad);
     d.acc_sum = (double *)(base + o_accs);
     d.acc_comp = (double *)(base + o_accc);
     if (h->tiled) {
-        d.depth_b = (float *)(base + o_db);
-        d.q_b = (float *)(base + o_qb);
-        d.rain_time_b = (float *)(base + o_rb);
+        d.depth_b = (real *)(base + o_db);
+        d.q_b = (real *)(base + o_qb);
+        d.rain_time_b = (real *)(base + o_rb);
         d.sdn = (float2 *)(base + o_sdn);
         d.plan = h->tb.plan;
     }
@@ -969,7 +1070,9 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
     Ctl init{};
     init.limit_value[0] = __builtin_inff();
     init.cfl_packed = kCflEmpty;
-    init.ndt = 0.0f;
+    init.ndt = RC(0);
+    init.cfl_min_bits = kCflEmpty;
+    init.cfl_arg_min = mesh->s_num;
     CKC(cudaMemcpyAsync(h->ctl, &init, sizeof(Ctl), cudaMemcpyHostToDevice, h->s));
     CKC(cudaStreamSynchronize(h->s));
 #undef CKC
@@ -1039,19 +1142,19 @@ int nhf_set_active(nhf_handle *h, int32_t active)
     return leave(h);
 }
 
-int nhf_set_forcing(nhf_handle *h, const float *coefficients, const float *rain_rates, int32_t raining)
+int nhf_set_forcing(nhf_handle *h, const nhf_real *coefficients, const nhf_real *rain_rates, int32_t raining)
 {
     if (!h) return NHF_EINVAL;
     int rc = enter(h); if (rc) return rc;
     const int bb = h->m.b_num > 0 ? h->m.b_num : 1;
-    float *stage = h->h_small;
+    real *stage = h->h_small;
     if (coefficients) {
-        memcpy(stage, coefficients, sizeof(float) * 2 * bb);
-        CK(h, cudaMemcpyAsync((void *)h->dev.coef, stage, sizeof(float) * 2 * bb, cudaMemcpyHostToDevice, h->s));
+        memcpy(stage, coefficients, sizeof(real) * 2 * bb);
+        CK(h, cudaMemcpyAsync((void *)h->dev.coef, stage, sizeof(real) * 2 * bb, cudaMemcpyHostToDevice, h->s));
     }
     if (rain_rates && h->m.n_rates > 0) {
-        memcpy(stage + 2 * bb, rain_rates, sizeof(float) * h->m.n_rates);
-        CK(h, cudaMemcpyAsync(h->dev.rain_rates, stage + 2 * bb, sizeof(float) * h->m.n_rates,
+        memcpy(stage + 2 * bb, rain_rates, sizeof(real) * h->m.n_rates);
+        CK(h, cudaMemcpyAsync(h->dev.rain_rates, stage + 2 * bb, sizeof(real) * h->m.n_rates,
                               cudaMemcpyHostToDevice, h->s));
     }
     memcpy(stage + 2 * bb + h->m.n_rates, &raining, sizeof(int32_t));
@@ -1061,7 +1164,7 @@ int nhf_set_forcing(nhf_handle *h, const float *coefficients, const float *rain_
     return leave(h);
 }
 
-int nhf_apply_initial_levels(nhf_handle *h, const float *targets)
+int nhf_apply_initial_levels(nhf_handle *h, const nhf_real *targets)
 {
     if (!h || !targets) return NHF_EINVAL;
     int rc = enter(h); if (rc) return rc;
@@ -1073,9 +1176,7 @@ int nhf_compute_cfl(nhf_handle *h)
 {
     if (!h) return NHF_EINVAL;
     int rc = enter(h); if (rc) return rc;
-    int gc = grid_for(h->m.s_num - 1, 256);
-    if (gc > 148 * 8) gc = 148 * 8;
-    k_cfl<<<gc, 256, 0, h->s>>>(h->dev, 0);
+    enqueue_cfl(h, h->s, 0);
     return leave(h);
 }
 
@@ -1160,6 +1261,9 @@ int nhf_budget_flush(nhf_handle *h, double *totals)
 int nhf_gate_attach(nhf_handle *h, const nhf_gate *gate)
 {
     if (!h || !gate) return NHF_EINVAL;
+#ifdef NHF_REAL_DOUBLE
+    return fail(h, NHF_EINVAL, "the FP64 build has no gate controller");
+#endif
     if (h->tiled && !(h->tb.plan.tile == 256 && h->tb.plan.split))
         return fail(h, NHF_EINVAL, "gate control runs on the multi-pass step or on the fused step with 256-cell "
                                    "tiles and the separate CFL pass (nhf_params.path = 1, or 256 with cfl_mode 2)");
@@ -1235,28 +1339,29 @@ int nhf_gate_flush(nhf_handle *h, double *totals)
     return leave(h);
 }
 
-int nhf_get_cfl(nhf_handle *h, float *ndt, int32_t *arg, float *flow_depth)
+int nhf_get_cfl(nhf_handle *h, nhf_real *ndt, int32_t *arg, nhf_real *flow_depth)
 {
     if (!h) return NHF_EINVAL;
     int rc = enter(h); if (rc) return rc;
-    float *out = (float *)h->d_begin;  // 3 words of device staging; graph not running
+    real *out = (real *)h->d_begin;  // 3 words of device staging; graph not running
     CK(h, cudaStreamSynchronize(h->s));
     k_cfl_edge<<<1, 1, 0, h->s>>>(h->dev, out);
-    CK(h, cudaMemcpyAsync(h->h_small, out, 3 * sizeof(float), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaMemcpyAsync(h->h_small, out, 3 * sizeof(real), cudaMemcpyDeviceToHost, h->s));
     CK(h, cudaStreamSynchronize(h->s));
     if (ndt) *ndt = h->h_small[0];
-    if (arg) memcpy(arg, &h->h_small[1], sizeof(int32_t));
-    if (flow_depth) *flow_depth = h->h_small[2];
+    if (flow_depth) *flow_depth = h->h_small[1];
+    if (arg) memcpy(arg, &h->h_small[2], sizeof(int32_t));
     return leave(h);
 }
 
-int nhf_limits(nhf_handle *h, float values[5], int32_t ids[3])
+int nhf_limits(nhf_handle *h, nhf_real values[5], int32_t ids[3])
 {
     if (!h) return NHF_EINVAL;
     int rc = enter(h); if (rc) return rc;
-    CK(h, cudaMemcpyAsync(h->h_small, h->ctl->limit_value, 8 * sizeof(float), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaMemcpyAsync(h->h_small, h->ctl->limit_value, 5 * sizeof(real), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaMemcpyAsync(h->h_small + 5, h->ctl->limit_ids, 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, h->s));
     CK(h, cudaStreamSynchronize(h->s));
-    if (values) memcpy(values, h->h_small, 5 * sizeof(float));
+    if (values) memcpy(values, h->h_small, 5 * sizeof(real));
     if (ids) memcpy(ids, h->h_small + 5, 3 * sizeof(int32_t));
     return leave(h);
 }
@@ -1265,13 +1370,13 @@ int nhf_reset_limits(nhf_handle *h)
 {
     if (!h) return NHF_EINVAL;
     int rc = enter(h); if (rc) return rc;
-    h->h_small[0] = __builtin_inff();
-    CK(h, cudaMemcpyAsync(&h->ctl->limit_value[0], h->h_small, sizeof(float), cudaMemcpyHostToDevice, h->s));
+    h->h_small[0] = (real)__builtin_inf();
+    CK(h, cudaMemcpyAsync(&h->ctl->limit_value[0], h->h_small, sizeof(real), cudaMemcpyHostToDevice, h->s));
     CK(h, cudaStreamSynchronize(h->s));
     return leave(h);
 }
 
-int nhf_sample_stations(nhf_handle *h, const int32_t *ids, int32_t n, float *out)
+int nhf_sample_stations(nhf_handle *h, const int32_t *ids, int32_t n, nhf_real *out)
 {
     if (!h || n < 0 || (n > 0 && (!ids || !out))) return NHF_EINVAL;
     if (n == 0) return NHF_OK;
@@ -1281,33 +1386,33 @@ int nhf_sample_stations(nhf_handle *h, const int32_t *ids, int32_t n, float *out
         if (h->d_samples) cudaFree(h->d_samples);
         h->d_ids = nullptr; h->d_samples = nullptr;
         CK(h, cudaMalloc(&h->d_ids, sizeof(int32_t) * n));
-        CK(h, cudaMalloc(&h->d_samples, sizeof(float) * 4 * n));
+        CK(h, cudaMalloc(&h->d_samples, sizeof(real) * 4 * n));
         h->ids_cap = n;
     }
     for (int i = 0; i < n; ++i)
         if (ids[i] < 1 || ids[i] >= h->m.e_num) return fail(h, NHF_EINVAL, "station cell %d out of range", ids[i]);
     CK(h, cudaMemcpyAsync(h->d_ids, ids, sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->s));
     k_sample<<<grid_for(n, 128), 128, 0, h->s>>>(h->dev, h->d_ids, n, h->d_samples);
-    CK(h, cudaMemcpyAsync(out, h->d_samples, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaMemcpyAsync(out, h->d_samples, sizeof(real) * 4 * n, cudaMemcpyDeviceToHost, h->s));
     CK(h, cudaStreamSynchronize(h->s));
     return leave(h);
 }
 
-int nhf_read_eq(nhf_handle *h, float *eq)
+int nhf_read_eq(nhf_handle *h, nhf_real *eq)
 {
     if (!h || !eq) return NHF_EINVAL;
     int rc = enter(h); if (rc) return rc;
     k_eq<<<grid_for(h->m.e_num - 1, 256), 256, 0, h->s>>>(h->dev);
-    CK(h, cudaMemcpyAsync(eq, h->dev.eq, sizeof(float) * 4 * (size_t)h->m.e_num, cudaMemcpyDeviceToDevice, h->s));
+    CK(h, cudaMemcpyAsync(eq, h->dev.eq, sizeof(real) * 4 * (size_t)h->m.e_num, cudaMemcpyDeviceToDevice, h->s));
     return leave(h);
 }
 
-int nhf_read_gradients(nhf_handle *h, float *gradients)
+int nhf_read_gradients(nhf_handle *h, nhf_real *gradients)
 {
     if (!h || !gradients) return NHF_EINVAL;
     if (h->m.hang_cells <= 0) return NHF_OK;
     int rc = enter(h); if (rc) return rc;
-    CK(h, cudaMemcpyAsync(gradients, h->dev.gradients, sizeof(float) * 2 * (size_t)h->m.hang_cells,
+    CK(h, cudaMemcpyAsync(gradients, h->dev.gradients, sizeof(real) * 2 * (size_t)h->m.hang_cells,
                           cudaMemcpyDeviceToDevice, h->s));
     return leave(h);
 }

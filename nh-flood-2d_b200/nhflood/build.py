@@ -1,4 +1,7 @@
-"""Build the sm_100a step library in-tree (nhflood/_lib/libnhflood.so).
+"""Build the sm_100a step libraries in-tree: nhflood/_lib/libnhflood.so
+(every step form, F32 physics) and nhflood/_lib/libnhflood_f64.so (the
+multi-pass step compiled with -DNHF_REAL_DOUBLE: the same kernels with F64
+physics, for the precision study).
 
 Flags: --fmad=false keeps the reference's F32 operation sequence (no
 multiply-add contraction), which the CPU restatement reproduces bit for bit;
@@ -17,6 +20,8 @@ ROOT = PACKAGE.parent
 CSRC = ROOT / 'csrc'
 LIBDIR = PACKAGE / '_lib'
 LIBRARY = LIBDIR / 'libnhflood.so'
+LIBRARY_F64 = LIBDIR / 'libnhflood_f64.so'
+F64_SOURCES = ('nhf_step.cu',)  # the FP64 build: the multi-pass step only
 INCLUDE = ROOT.parent / 'include'
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
@@ -32,10 +37,10 @@ def sources() -> list[Path]:
     return sorted(CSRC.glob('*.cu'))
 
 
-def needs_build() -> bool:
-    if not LIBRARY.exists():
+def needs_build(library: Path = LIBRARY) -> bool:
+    if not library.exists():
         return True
-    stamp = LIBRARY.stat().st_mtime
+    stamp = library.stat().st_mtime
     deps = sources() + sorted(CSRC.glob('*.cuh')) + sorted(INCLUDE.glob('*.h'))
     return any(p.stat().st_mtime > stamp for p in deps)
 
@@ -63,18 +68,23 @@ def build_host(verbose: bool = False, force: bool = False) -> Path:
     return PREP_LIBRARY
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    build_host(verbose, force)
-    if not force and not needs_build():
-        return LIBRARY
+def _nvcc_shared(library: Path, files, defines=(), verbose=False) -> None:
     LIBDIR.mkdir(exist_ok=True)
-    tmp = LIBDIR / f'.libnhflood.{os.getpid()}.so'
+    tmp = LIBDIR / f'.{library.stem}.{os.getpid()}.so'
     cmd = [nvcc(), *ARCH, '-lineinfo', '-O3', '--fmad=false', '-std=c++17', '-Xcompiler', '-fPIC',
-           '-shared', f'-I{INCLUDE}', '-o', str(tmp), *map(str, sources())]
+           *defines, '-shared', f'-I{INCLUDE}', '-o', str(tmp), *map(str, files)]
     if verbose:
         print(' '.join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
-    os.replace(tmp, LIBRARY)
+    os.replace(tmp, library)
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    build_host(verbose, force)
+    if force or needs_build(LIBRARY):
+        _nvcc_shared(LIBRARY, sources(), verbose=verbose)
+    if force or needs_build(LIBRARY_F64):
+        _nvcc_shared(LIBRARY_F64, [CSRC / f for f in F64_SOURCES], ['-DNHF_REAL_DOUBLE'], verbose)
     return LIBRARY
 
 

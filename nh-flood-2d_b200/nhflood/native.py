@@ -28,9 +28,17 @@ class NhfMesh(ctypes.Structure):
     _fields_ = [(n, c_int32) for n in _MESH_INTS] + [(n, c_void_p) for n in _MESH_PTRS]
 
 
-class NhfParams(ctypes.Structure):
-    _fields_ = [('g', c_float), ('afa', c_float), ('sita', c_float), ('min_h', c_float),
-                ('min_dt', c_float), ('batch_size', c_int32), ('path', c_int32), ('cfl_mode', c_int32)]
+def _params_type(real):
+    class Params(ctypes.Structure):
+        _fields_ = [('g', real), ('afa', real), ('sita', real), ('min_h', real),
+                    ('min_dt', c_float), ('batch_size', c_int32), ('path', c_int32), ('cfl_mode', c_int32)]
+    return Params
+
+
+NhfParams = _params_type(c_float)
+# nhf_real of each build: the F32 step (libnhflood.so) and its FP64 build
+# (libnhflood_f64.so, the multi-pass kernels with double physics)
+PRECISIONS = {'f32': (c_float, np.float32, NhfParams), 'f64': (c_double, np.float64, _params_type(c_double))}
 
 
 _GATE_TABLES = ('cell_gate', 'pond', 'closed', 'targets', 'controls', 'flux_sides')
@@ -44,23 +52,25 @@ class NhfGate(ctypes.Structure):
                 + [(n, c_void_p) for n in _GATE_WORDS])
 
 
-_LIB = None
+_LIBS = {}
 
 
-def library(path=None):
-    """Load (and declare) libnhflood.so; raises if it is missing."""
-    global _LIB
-    if _LIB is not None:
-        return _LIB
-    from .build import LIBRARY
-    path = path or LIBRARY
+def library(path=None, precision: str = 'f32'):
+    """Load (and declare) libnhflood.so, or with precision='f64' its FP64
+    build libnhflood_f64.so; raises if it is missing."""
+    if precision in _LIBS and path is None:
+        return _LIBS[precision]
+    from .build import LIBRARY, LIBRARY_F64
+    path = path or (LIBRARY if precision == 'f32' else LIBRARY_F64)
     if not path.exists():
         raise RuntimeError(f'{path} is missing: build it with `python -m nhflood.build` '
                            '(the CUDA step has no CPU fallback)')
     lib = ctypes.CDLL(str(path))
+    real, _, params_type = PRECISIONS[precision]
     H = c_void_p
     sig = {
-        'nhf_create': (c_int32, [POINTER(NhfMesh), POINTER(NhfParams), c_void_p, POINTER(c_void_p)]),
+        'nhf_create': (c_int32, [POINTER(NhfMesh), POINTER(params_type), c_void_p, POINTER(c_void_p)]),
+        'nhf_real_bytes': (c_int32, []),
         'nhf_destroy': (c_int32, [H]),
         'nhf_last_error': (ctypes.c_char_p, [H]),
         'nhf_version': (ctypes.c_char_p, []),
@@ -68,7 +78,7 @@ def library(path=None):
         'nhf_set_clock': (c_int32, [H, POINTER(c_uint32)]),
         'nhf_get_clock': (c_int32, [H, POINTER(c_uint32)]),
         'nhf_set_active': (c_int32, [H, c_int32]),
-        'nhf_set_forcing': (c_int32, [H, POINTER(c_float), POINTER(c_float), c_int32]),
+        'nhf_set_forcing': (c_int32, [H, POINTER(real), POINTER(real), c_int32]),
         'nhf_apply_initial_levels': (c_int32, [H, c_void_p]),
         'nhf_compute_cfl': (c_int32, [H]),
         'nhf_initial_diagnostics': (c_int32, [H]),
@@ -78,10 +88,10 @@ def library(path=None):
         'nhf_read_trace': (c_int32, [H, POINTER(c_uint32)]),
         'nhf_budget_flush': (c_int32, [H, POINTER(c_double)]),
         'nhf_budget_terms': (c_int32, [H]),
-        'nhf_get_cfl': (c_int32, [H, POINTER(c_float), POINTER(c_int32), POINTER(c_float)]),
-        'nhf_limits': (c_int32, [H, POINTER(c_float), POINTER(c_int32)]),
+        'nhf_get_cfl': (c_int32, [H, POINTER(real), POINTER(c_int32), POINTER(real)]),
+        'nhf_limits': (c_int32, [H, POINTER(real), POINTER(c_int32)]),
         'nhf_reset_limits': (c_int32, [H]),
-        'nhf_sample_stations': (c_int32, [H, POINTER(c_int32), c_int32, POINTER(c_float)]),
+        'nhf_sample_stations': (c_int32, [H, POINTER(c_int32), c_int32, POINTER(real)]),
         'nhf_read_eq': (c_int32, [H, c_void_p]),
         'nhf_read_gradients': (c_int32, [H, c_void_p]),
         'nhf_synchronize': (c_int32, [H]),
@@ -103,17 +113,22 @@ def library(path=None):
         'nhf_ensemble_run_batch_async': (c_int32, [H, POINTER(c_uint32), POINTER(c_uint32)]),
         'nhf_ensemble_read_trace': (c_int32, [H, POINTER(c_uint32)]),
     }
+    if precision == 'f64':  # the FP64 build has the single-mesh entry points only
+        sig = {k: v for k, v in sig.items() if not k.startswith(('nhf_ensemble', 'nhf_cfl_noalloc'))}
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    _LIB = lib
+    if lib.nhf_real_bytes() != ctypes.sizeof(real):
+        raise RuntimeError(f'{path}: nhf_real of {lib.nhf_real_bytes()} bytes, expected {ctypes.sizeof(real)}')
+    _LIBS[precision] = lib
     return lib
 
 
 def exported_symbols() -> list[str]:
     """Names declared in include/nhflood.h that the library must export."""
-    return ['nhf_create', 'nhf_destroy', 'nhf_last_error', 'nhf_version', 'nhf_initialize', 'nhf_set_clock',
+    return ['nhf_create', 'nhf_destroy', 'nhf_last_error', 'nhf_version', 'nhf_real_bytes', 'nhf_initialize',
+            'nhf_set_clock',
             'nhf_get_clock', 'nhf_set_active', 'nhf_set_forcing', 'nhf_apply_initial_levels',
             'nhf_compute_cfl', 'nhf_initial_diagnostics', 'nhf_reset_extrema', 'nhf_run_batch',
             'nhf_run_batch_async', 'nhf_read_trace', 'nhf_budget_flush', 'nhf_budget_terms', 'nhf_get_cfl',
@@ -147,18 +162,25 @@ class CudaEngine(Engine):
 
     backend = 'cuda'
 
-    def __init__(self, arrays: StepArrays, params: StepParams, device='cuda:0'):
+    def __init__(self, arrays: StepArrays, params: StepParams, device='cuda:0', precision: str = 'f32'):
+        """precision 'f64' runs the FP64 build of the multi-pass kernels
+        (libnhflood_f64.so): the same F32 inputs, every physics quantity in
+        double, the clock and its trace in F32."""
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError('CudaEngine needs a CUDA device; the step has no CPU fallback')
         self.torch = torch
-        self.lib = library()
+        self.precision = precision
+        self.creal, self.real, self._params_type = PRECISIONS[precision]
+        self.lib = library(precision=precision)
         self.arrays = arrays
         self.params = params
         self.device = torch.device(device)
         self.device_name = torch.cuda.get_device_name(self.device)
         self.batch_size = params.batch_size
         dev = self.device
+        real = self.real
+        self.treal = torch.float32 if precision == 'f32' else torch.float64
 
         def put(a, dtype=None):
             if a is None:
@@ -168,22 +190,24 @@ class CudaEngine(Engine):
 
         e, s = arrays.e_num, arrays.s_num
         self.t = {
-            'x': put(arrays.x), 'y': put(arrays.y), 'area': put(arrays.area), 'width': put(arrays.width),
-            'height': put(arrays.height), 'f0': put(arrays.f0), 'fc': put(arrays.fc), 'k': put(arrays.k),
-            'weight': put(arrays.weight), 'boundary_id': put(arrays.boundary_id),
+            'x': put(arrays.x, real), 'y': put(arrays.y, real), 'area': put(arrays.area, real),
+            'width': put(arrays.width, real), 'height': put(arrays.height, real), 'f0': put(arrays.f0, real),
+            'fc': put(arrays.fc, real), 'k': put(arrays.k, real),
+            'weight': put(arrays.weight, real), 'boundary_id': put(arrays.boundary_id),
             'rain_index': put(arrays.rain_index), 'face_ptr': put(arrays.face_ptr),
             'face_count': put(arrays.face_count),
             'isl_data': put(arrays.isl_data if len(arrays.isl_data) else np.zeros(1, np.int32)),
-            'topology': put(arrays.topology), 'length': put(arrays.length), 'side_n': put(arrays.side_n),
-            'sbf': put(arrays.sbf), 'kind': put(arrays.kind), 'open_face': put(arrays.open_face),
-            'edge_index': put(arrays.edge_index), 'offsets': put(arrays.offsets), 'slots': put(arrays.slots),
+            'topology': put(arrays.topology), 'length': put(arrays.length, real),
+            'side_n': put(arrays.side_n, real),
+            'sbf': put(arrays.sbf), 'kind': put(arrays.kind), 'open_face': put(arrays.open_face, real),
+            'edge_index': put(arrays.edge_index), 'offsets': put(arrays.offsets, real), 'slots': put(arrays.slots),
             'hcells': put(arrays.hcells), 'axes': put(arrays.axes),
-            'bed': put(arrays.bed),
+            'bed': put(arrays.bed, real),
         }
         with torch.cuda.device(dev):
             for name in STATE_F32:
                 if name != 'bed':
-                    self.t[name] = torch.zeros(s if name == 'q' else e, dtype=torch.float32, device=dev)
+                    self.t[name] = torch.zeros(s if name == 'q' else e, dtype=self.treal, device=dev)
             for name in STATE_U32:
                 self.t[name] = torch.zeros(e, dtype=torch.int32, device=dev)
         mesh = NhfMesh()
@@ -203,8 +227,10 @@ class CudaEngine(Engine):
                 raise ValueError('gate control needs path "auto", "tile256" or "multipass" and a separate CFL pass')
             if path != 1:
                 path, cfl_mode = 256, 2
-        p = NhfParams(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size, path,
-                      cfl_mode)
+        if precision == 'f64' and arrays.gate is not None:
+            raise ValueError('the FP64 build has no gate controller')
+        p = self._params_type(params.g, params.afa, params.sita, params.min_h, params.min_dt, params.batch_size,
+                              path, cfl_mode)
         handle = c_void_p()
         with torch.cuda.device(dev):
             stream = torch.cuda.current_stream(dev).cuda_stream
@@ -229,7 +255,7 @@ class CudaEngine(Engine):
         self.gt = {}
         for name in _GATE_TABLES:
             a = getattr(tables, name)
-            a = np.ascontiguousarray(a, dtype=np.float32 if name == 'closed' else np.int32)
+            a = np.ascontiguousarray(a, dtype=self.real if name == 'closed' else np.int32)
             t = torch.from_numpy(a if len(a) else np.zeros(1, a.dtype)).to(dev)
             self.gt[name] = t
             setattr(gate, name, t.data_ptr())
@@ -284,7 +310,7 @@ class CudaEngine(Engine):
         if name in STATE_U32:
             arr = arr.astype(np.uint32).view(np.int32)
         else:
-            arr = arr.astype(np.float32)
+            arr = arr.astype(self.real)
         if arr.shape != tuple(t.shape):
             raise ValueError(f'{name}: shape {arr.shape} differs from {tuple(t.shape)}')
         t.copy_(self.torch.from_numpy(arr))
@@ -305,19 +331,19 @@ class CudaEngine(Engine):
         self._check(self.lib.nhf_set_active(self.h, int(active)), 'nhf_set_active')
 
     def set_forcing(self, coefficients, rain_rates, raining):
-        coef = None if coefficients is None else np.ascontiguousarray(coefficients, dtype=np.float32)
-        rates = None if rain_rates is None else np.ascontiguousarray(rain_rates, dtype=np.float32)
+        coef = None if coefficients is None else np.ascontiguousarray(coefficients, dtype=self.real)
+        rates = None if rain_rates is None else np.ascontiguousarray(rain_rates, dtype=self.real)
         if coef is not None and coef.shape != (max(1, self.arrays.b_num), 2):
             raise ValueError(f'coefficients must be [{max(1, self.arrays.b_num)}, 2], got {coef.shape}')
         if rates is not None and rates.shape != (self.arrays.n_rates,):
             raise ValueError(f'rain rates must be [{self.arrays.n_rates}], got {rates.shape}')
         self._check(self.lib.nhf_set_forcing(
-            self.h, coef.ctypes.data_as(POINTER(c_float)) if coef is not None else None,
-            rates.ctypes.data_as(POINTER(c_float)) if rates is not None else None, int(bool(raining))),
+            self.h, coef.ctypes.data_as(POINTER(self.creal)) if coef is not None else None,
+            rates.ctypes.data_as(POINTER(self.creal)) if rates is not None else None, int(bool(raining))),
             'nhf_set_forcing')
 
     def apply_initial_levels(self, targets):
-        t = self.torch.from_numpy(np.ascontiguousarray(targets, dtype=np.float32)).to(self.device)
+        t = self.torch.from_numpy(np.ascontiguousarray(targets, dtype=self.real)).to(self.device)
         self._check(self.lib.nhf_apply_initial_levels(self.h, c_void_p(t.data_ptr())), 'nhf_apply_initial_levels')
         self.torch.cuda.current_stream(self.device).synchronize()  # t stays alive until the kernel has read it
 
@@ -352,14 +378,14 @@ class CudaEngine(Engine):
         return out
 
     def cfl(self):
-        ndt, arg, h = c_float(), c_int32(), c_float()
+        ndt, arg, h = self.creal(), c_int32(), self.creal()
         self._check(self.lib.nhf_get_cfl(self.h, ctypes.byref(ndt), ctypes.byref(arg), ctypes.byref(h)), 'nhf_get_cfl')
         return float(ndt.value), int(arg.value), float(h.value)
 
     def limits(self):
-        values = np.zeros(5, np.float32)
+        values = np.zeros(5, self.real)
         ids = np.zeros(3, np.int32)
-        self._check(self.lib.nhf_limits(self.h, values.ctypes.data_as(POINTER(c_float)),
+        self._check(self.lib.nhf_limits(self.h, values.ctypes.data_as(POINTER(self.creal)),
                                         ids.ctypes.data_as(POINTER(c_int32))), 'nhf_limits')
         return values, ids
 
@@ -368,14 +394,14 @@ class CudaEngine(Engine):
 
     def sample_stations(self, ids):
         ids = np.ascontiguousarray(ids, dtype=np.int32)
-        out = np.zeros((len(ids), 4), np.float32)
+        out = np.zeros((len(ids), 4), self.real)
         if len(ids):
             self._check(self.lib.nhf_sample_stations(self.h, ids.ctypes.data_as(POINTER(c_int32)), len(ids),
-                                                     out.ctypes.data_as(POINTER(c_float))), 'nhf_sample_stations')
+                                                     out.ctypes.data_as(POINTER(self.creal))), 'nhf_sample_stations')
         return out
 
     def read_eq(self):
-        out = self.torch.zeros((self.arrays.e_num, 4), dtype=self.torch.float32, device=self.device)
+        out = self.torch.zeros((self.arrays.e_num, 4), dtype=self.treal, device=self.device)
         self._check(self.lib.nhf_read_eq(self.h, c_void_p(out.data_ptr())), 'nhf_read_eq')
         return out.cpu().numpy()
 

@@ -95,6 +95,14 @@ double ora_exp(double y)
     return p * bits_to_double((uint64_t)(ni + 1023) << 52);
 }
 
+/* x ** y in F64 through the same two series (the FP64 build of the step) */
+double ora_pow(double x, double y)
+{
+    if (x != x) return x;
+    if (x == 0.0) return 0.0;
+    return ora_exp(y * ora_ln(x));
+}
+
 float ora_powf(float x, float y)
 {
     if (x != x) return x;

@@ -43,8 +43,8 @@ typedef ora_real real;
 #define R(x) x
 #define RABS(x) fabs(x)
 #define RSQRT(x) sqrt(x)
-#define RPOW(x, y) pow(x, y)
-#define REXP(x) exp(x)
+#define RPOW(x, y) ora_pow(x, y) /* the FP64 series of mathref.c, as the CUDA FP64 build */
+#define REXP(x) ora_exp(x)
 #else
 #define R(x) x##f
 #define RABS(x) fabsf(x)

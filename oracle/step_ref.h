@@ -141,6 +141,7 @@ void ora_gate_flush(ora_ctx *c, double *totals);
 /* mathref.c */
 double ora_ln(double x);
 double ora_exp(double y);
+double ora_pow(double x, double y);
 float ora_powf(float x, float y);
 float ora_expf(float a);
 

@@ -66,3 +66,17 @@ def test_kernels_compile_without_spills():
                          capture_output=True, text=True, check=True).stderr
     spills = [int(m) for m in re.findall(r'(\d+) bytes spill stores', out)]
     assert spills and max(spills) == 0, out
+
+
+def test_fp64_build_exports_the_single_mesh_entry_points(library_path):
+    """libnhflood_f64.so: the multi-pass step with nhf_real = double."""
+    from nhflood.build import LIBRARY_F64
+    from nhflood.native import exported_symbols, library
+    out = subprocess.run(['nm', '-D', '--defined-only', str(LIBRARY_F64)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    single = [s for s in exported_symbols() if not s.startswith(('nhf_ensemble', 'nhf_cfl_noalloc'))]
+    assert not [s for s in single if s not in exported]
+    lib = library(precision='f64')
+    assert lib.nhf_real_bytes() == 8 and b'FP64' in lib.nhf_version()
+    assert library().nhf_real_bytes() == 4

@@ -55,6 +55,58 @@ def test_noalloc_cfl_matches_the_handle_entry_point_on_two_calls(cuda_available)
         run.close()
 
 
+@pytest.mark.gpu
+def test_noalloc_cfl_without_interior_sides_then_a_flowing_mesh(tmp_path, cuda_available):
+    """The empty result (+inf and side 0, solver_compact.py:636-639) on a mesh
+    whose sides are all exterior and on a mesh without any side (s_num == 1,
+    one block that finds nothing), each against the handle entry point, and
+    then a flowing dam break, so that the ticket and the block slots are
+    shown to be reset between calls."""
+    import torch
+    from lockstep import workload_from_case
+    from nhflood.native import CudaEngine, library
+    from nhflood.plain import PlainRun
+    from nhflood.workloads import dambreak
+    from scenarios import all_cells_filtered, two_cell_case
+    lib = library()
+    cases = []
+    dc, fc = two_cell_case(tmp_path / 'isolated', [[6, 6]], 10)  # two cells, every side exterior
+    cases.append(workload_from_case(dc, fc, 'isolated'))
+    dc, fc = all_cells_filtered(tmp_path / 'empty')  # no cell and no side: s_num == 1
+    cases.append(workload_from_case(dc, fc, 'empty'))
+    cases.append(dambreak(n=96, dx=1.0, duration=30))
+    for w in cases:
+        run = PlainRun(w, lambda a, p: CudaEngine(a, p, device='cuda:0'))
+        try:
+            run.advance()
+            run.engine.compute_cfl()
+            ndt_ref, arg_ref, _ = run.engine.cfl()
+            stream = torch.cuda.current_stream(run.engine.device).cuda_stream
+            ndt, arg = _noalloc(lib, run.engine, stream)
+            assert np.float32(ndt).view(np.uint32) == np.float32(ndt_ref).view(np.uint32), (w.name, ndt, ndt_ref)
+            assert arg == arg_ref, (w.name, arg, arg_ref)
+            if w.name in ('isolated', 'empty'):
+                assert np.isinf(ndt) and ndt > 0 and arg == 0, w.name
+            else:
+                assert np.isfinite(ndt) and arg > 0
+        finally:
+            run.close()
+    assert cases[1].mesh.s_num == 1
+
+
+@pytest.mark.gpu
+def test_noalloc_cfl_refuses_host_pointers(cuda_available):
+    """A host array passed as an input is refused before any launch."""
+    from nhflood.native import library
+    lib = library()
+    host = np.zeros(16, np.float32)
+    import torch
+    dev = torch.zeros(16, device='cuda:0')
+    p = ctypes.c_void_p(dev.data_ptr())
+    rc = lib.nhf_cfl_noalloc(p, ctypes.c_void_p(host.ctypes.data), p, p, p, 4, 0.5, 9.81, None, p, p)
+    assert rc == -1 and b'bed is not' in lib.nhf_cfl_noalloc_error()
+
+
 def test_noalloc_cfl_rejects_meshes_beyond_its_fixed_scratch():
     """Checked on the host before any device work (runs without a GPU)."""
     from nhflood.native import library
