@@ -302,6 +302,32 @@ def ensemble_cpu_sample(runs, seconds_budget, threads=None):
                        f'at the timed start ({seconds:.1f} s of CPU restatement, OpenMP)')}
 
 
+def plain_breakdown(per_member, edges=(2e5, 7e5)):
+    """The plain form's members in three size buckets (cells below 200k,
+    200k to 700k, above): members, cells, share of the plain form's time and
+    cell-updates/s. The largest bucket's rate is about what the plain form
+    reaches once a mesh fills the GPU, so total plain time over (total
+    cell-updates / that rate) bounds what batching can gain."""
+    rows = np.array(per_member, dtype=np.float64).reshape(-1, 3)
+    total_s = rows[:, 2].sum()
+    names = ('small', 'mid', 'large')
+    bounds = (0,) + tuple(edges) + (np.inf,)
+    out = {}
+    for name, lo, hi in zip(names, bounds[:-1], bounds[1:]):
+        sel = rows[(rows[:, 0] >= lo) & (rows[:, 0] < hi)]
+        if not len(sel):
+            continue
+        out[name] = {'members': int(len(sel)), 'cells': int(sel[:, 0].sum()),
+                     'plain_time_share': float(sel[:, 2].sum() / total_s) if total_s else None,
+                     'plain_rate': float(sel[:, 1].sum() / sel[:, 2].sum()) if sel[:, 2].sum() else None}
+    if out:
+        large = out.get('large') or out[max(out, key=lambda k: out[k]['cells'])]
+        if large['plain_rate'] and total_s:
+            out['bound_if_every_member_ran_at_the_large_rate'] = float(
+                total_s / (rows[:, 1].sum() / large['plain_rate']))
+    return out
+
+
 def bench_batched(args, rank, world, local):
     """Batched form: 64 seeded quadtree scenarios (about 40M cells) in one
     ensemble (by default every scenario's own batch graph, all launched
@@ -359,7 +385,9 @@ def bench_batched(args, rank, world, local):
     from nhflood.plain import PlainRun
     plain_cells, plain_s = 0, 0.0
     plain_depth = []
+    per_member = []  # (cells, cell-updates, seconds) of each member's plain batches
     for member in ens.runs:
+        m_cells, m_s = plain_cells, plain_s
         r = PlainRun(member.w, lambda a, p: CudaEngine(a, p, device=str(device)), batch_size=member.params.batch_size)
         r.adopt(member)
         st = r.engine.stream()
@@ -375,6 +403,7 @@ def bench_batched(args, rank, world, local):
             b.synchronize()
             plain_s += a.elapsed_time(b) / 1e3
         plain_depth.append((r.elapsed, r.engine.get('depth')))
+        per_member.append((r.w.cells, plain_cells - m_cells, plain_s - m_s))
         r.close()
     # end to end through the public call (host words in, host traces out),
     # the same batches the plain engines just ran
@@ -416,6 +445,7 @@ def bench_batched(args, rank, world, local):
                                  'sample': f'{ENSEMBLE_PLAIN_BATCHES} plain batches of each member from its state '
                                            'after the timed batches, one member after another'},
             'batched_over_plain': value / plain if plain else None,
+            'plain_by_size': plain_breakdown(per_member),
             'max_depth_error_vs_plain_m': max_err,
             'members_compared_with_plain': compared,
             'gpu_launches': per_batch_kernels * recorded,
@@ -547,7 +577,7 @@ def main():
     ap.add_argument('--cpu-seconds', type=float, default=15.0)
     ap.add_argument('--form', default=os.environ.get('NHF_BENCH_FORM', 'batched'),
                     choices=['plain', 'batched', 'served'])
-    ap.add_argument('--requests', type=int, default=48, help='served: requests in the stream')
+    ap.add_argument('--requests', type=int, default=512, help='served: requests in the stream (config 5: 512)')
     ap.add_argument('--hbm-budget', type=float, default=150e9, help='served: admission budget in bytes')
     ap.add_argument('--members', type=int, default=64)
     ap.add_argument('--tile', type=int, default=None, help='batched: tile size (default: autotuned)')
