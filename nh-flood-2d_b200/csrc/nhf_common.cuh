@@ -36,16 +36,17 @@ struct Ctl {
     float dt, local, end_local;  // the clock's F32 values
     real ndt;
     int32_t active, slot, raining, cfl_arg;
-    uint32_t limited_cells, limited_faces, wet;
+    uint32_t limited_cells, limited_faces;
     scale_bits_t min_scale_bits;
+    uint32_t wet;
     unsigned long long cfl_packed;
-    unsigned long long cfl_min_bits;  // FP64 build: the CFL minimum's bits, then
-    int32_t cfl_arg_min;              // the lowest side id that attains it
     uint32_t done_blocks;
     int32_t parity;  // 1: the current depth/q/rain_time live in the second buffers
     real limit_value[5];
     int32_t limit_ids[3];
     uint32_t trace[NHF_MAX_BATCH * NHF_TRACE_COLS];
+    unsigned long long cfl_min_bits;  // FP64 build: the CFL minimum's bits, then
+    int32_t cfl_arg_min;              // the lowest side id that attains it
 };
 
 // Tile plan of the fused step (built on the host by nhf_tiled.cu).
@@ -234,10 +235,9 @@ __device__ __forceinline__ void prepare_step(const Dev &d, Ctl *c, const real *d
     c->limited_cells = 0; c->limited_faces = 0;
     c->min_scale_bits = real_bits(RC(1.0));
     c->wet = 0;
-    const real local = c->local, end_local = c->end_local, dt = c->dt;
     for (int bi = 0; bi < m.b_num; ++bi) {
-        d.values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * (local + dt / RC(2.0));
-        d.level_values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * end_local;
+        d.values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * ((real)c->local + (real)c->dt / RC(2.0));
+        d.level_values[bi] = d.coef[2 * bi] + d.coef[2 * bi + 1] * (real)c->end_local;
     }
     if (c->ndt < c->limit_value[0]) {
         int si = c->cfl_arg;
