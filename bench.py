@@ -342,7 +342,7 @@ def bench_batched(args, rank, world, local):
     ws = ensemble_workloads(args, rank)
     t_gen = time.perf_counter() - t0
     t0 = time.perf_counter()
-    ens = EnsembleRun(ws, device=str(device), tile=args.tile, grid_blocks=args.grid)
+    ens = EnsembleRun(ws, device=str(device), tile=args.tile, grid_blocks=args.grid, tune=not args.no_tune)
     t_setup = time.perf_counter() - t0
     stream = ens.ensemble.stream()
     spin_to = min(r.w.duration for r in ens.runs) / 3 if args.spin_up is None else args.spin_up
@@ -440,7 +440,8 @@ def bench_batched(args, rank, world, local):
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'form': 'batched',
             'config': ensemble_config(ws, spin_to, world),
             'schedule': {'kind': ens.schedule, 'tile': ens.ensemble.tile or 'per member',
-                         'grid_blocks': ens.ensemble.grid, 'tiles': ens.ensemble.tiles},
+                         'grid_blocks': ens.ensemble.grid, 'tiles': ens.ensemble.tiles,
+                         'autotuner_trials_tile_grid_rate': ens.tuned.trials if ens.tuned else None},
             'plain_sequential': {'value': plain, 'unit': METRIC,
                                  'sample': f'{ENSEMBLE_PLAIN_BATCHES} plain batches of each member from its state '
                                            'after the timed batches, one member after another'},
@@ -455,7 +456,7 @@ def bench_batched(args, rank, world, local):
             'e2e': {'value': e2e_cells / e2e_s if e2e_s else None, 'unit': METRIC,
                     'h2d_bytes_per_step': h2d // max(1, ENSEMBLE_PLAIN_BATCHES), 'd2h_bytes_per_step': trace_bytes},
             'clocks': clocks.summary(),
-            'setup_seconds': {'generate': round(t_gen, 1), 'engines': round(t_setup, 1),
+            'setup_seconds': {'generate': round(t_gen, 1), 'tuning_and_engines': round(t_setup, 1),
                               'spin_up': round(t_spin, 1)},
         }
         if cpu is not None:
@@ -580,8 +581,10 @@ def main():
     ap.add_argument('--requests', type=int, default=512, help='served: requests in the stream (config 5: 512)')
     ap.add_argument('--hbm-budget', type=float, default=150e9, help='served: admission budget in bytes')
     ap.add_argument('--members', type=int, default=64)
-    ap.add_argument('--tile', type=int, default=None, help='batched: tile size (default: autotuned)')
-    ap.add_argument('--grid', type=int, default=None, help='batched: 0 persistent, -1 block per tile')
+    ap.add_argument('--tile', type=int, default=None, help='batched: one-launch tile size (default: autotuned)')
+    ap.add_argument('--grid', type=int, default=None,
+                    help='batched: 0 persistent, -1 block per tile, -2 member graphs (default: autotuned)')
+    ap.add_argument('--no-tune', action='store_true', help='batched: member graphs without the autotuner')
     ap.add_argument('--path', default='auto', help="plain form's step: 'auto', 'multipass', 'tile256', 'tile512', 'tile1024'")
     ap.add_argument('--spin-up', type=float, default=None,
                     help='simulated seconds advanced (untimed) before the warm-up; default a third of the run')

@@ -837,21 +837,16 @@ __global__ void __launch_bounds__(256) k_cfl_tiled_gate(const __grid_constant__ 
 // takes items blockIdx.x, + gridDim.x, ...) or one block per item. The
 // member's descriptor is staged in shared memory once per change of member.
 template <bool kThetaOne, int NT, int CPT>
-__global__ void __launch_bounds__(NT, kEnsembleMinBlocks<NT>) k_step_ensemble(const Dev *devs, const int2 *items, int n_items)
+__global__ void __launch_bounds__(NT, kEnsembleMinBlocks<NT>)
+    k_step_ensemble(const Dev *__restrict__ devs, const int2 *__restrict__ items, int n_items)
 {
-    __shared__ __align__(16) Dev sd;
-    int current = -1;
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const int2 w = items[it];
-        if (w.x != current) {
-            __syncthreads();
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(devs + w.x);
-            uint32_t *dst = reinterpret_cast<uint32_t *>(&sd);
-            for (int i = threadIdx.x; i < (int)(sizeof(Dev) / 4); i += NT) dst[i] = src[i];
-            current = w.x;
-        }
-        __syncthreads();
-        step_tile<kThetaOne, 2, NT, CPT>(sd, w.y, (unsigned)sd.plan.n_tiles);
+        // the member's descriptor is read in place through the read-only
+        // data path (it does not change during the launch)
+        const Dev &md = devs[w.x];
+        __syncthreads();  // the previous item's shared arrays are dead
+        step_tile<kThetaOne, 2, NT, CPT>(md, w.y, (unsigned)md.plan.n_tiles);
     }
 }
 

@@ -49,13 +49,20 @@ def plain_factory(device: str = 'cuda:0'):
 
 
 class EnsembleRun:
-    """With neither tile nor grid_blocks (or grid_blocks = -2) the member
-    graphs; otherwise the one-launch schedule, the autotuner filling in what
-    is not given."""
+    """grid_blocks = -2: the member graphs. A tile size and/or a grid: the
+    one-launch schedule, the autotuner filling in what is not given. Neither
+    (tune=True): the autotuner's choice among all of them; with tune=False
+    the member graphs."""
 
     def __init__(self, workloads, *, tile: int | None = None, grid_blocks: int | None = None,
-                 batch_size: int = 32, device: str = 'cuda:0', tuning_cache=None):
+                 batch_size: int = 32, device: str = 'cuda:0', tuning_cache=None, tune: bool = False):
         self.workloads = list(workloads)
+        self.tuned = None
+        if tile is None and grid_blocks is None and tune:
+            from .autotune import choose_schedule
+            self.tuned = choose_schedule(self.workloads, batch_size=batch_size, device=device, cache=tuning_cache)
+            tile, grid_blocks = (None, MEMBER_GRAPHS) if self.tuned.grid == MEMBER_GRAPHS else \
+                (self.tuned.tile, self.tuned.grid)
         if grid_blocks == MEMBER_GRAPHS or (tile is None and grid_blocks is None):
             self.schedule = 'member graphs'
             tile, grid_blocks = None, MEMBER_GRAPHS
@@ -64,7 +71,8 @@ class EnsembleRun:
             self.schedule = 'one launch'
             if tile is None or grid_blocks is None:
                 from .autotune import choose_schedule
-                tuned = choose_schedule(self.workloads, batch_size=batch_size, device=device, cache=tuning_cache)
+                tuned = choose_schedule(self.workloads, batch_size=batch_size, device=device, cache=tuning_cache,
+                                        member_graphs_fn=lambda *a: None)
                 tile = tuned.tile if tile is None else tile
                 grid_blocks = tuned.grid if grid_blocks is None else grid_blocks
             factory = tiled_factory(tile, device)
