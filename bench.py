@@ -86,6 +86,8 @@ def launches_per_batch(run) -> int:
     the hanging-edge and theta pre-passes, and the gate controller's
     passes."""
     eng = run.engine
+    if eng.path.startswith('lattice'):  # gather, begin, scatter, velocity; per step the step and its CFL pass
+        return 4 + run.params.batch_size * 2
     tiled = eng.path.startswith('tiled')
     pre = (1 if run.arrays.hang_cells else 0) + (0 if run.w.sita == 1.0 else 1)
     gate = run.arrays.gate

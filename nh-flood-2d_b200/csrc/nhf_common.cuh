@@ -63,6 +63,30 @@ struct TilePlan {
     const uint16_t *face_idx;  // local side indices in the reference's CSR order
 };
 
+// Lattice form (nhf_lattice.cu) of a uniform mesh: the cells renumbered into
+// a padded 2-D lattice (a 2-cell border and tile padding of holes), the
+// state kept in lattice order during a batch. Lattice index of real cell
+// (i, j): (j + 2) * lx + (i + 2); the west face of a lattice cell is its
+// "v" side, the south face its "h" side.
+struct LatticePlan {
+    int32_t nx, ny, lx, ly, tiles_x, tiles_y, rain_cells, horton;
+    real sdc_v, sdc_h, len_v, len_h, area, width, height;
+    const int32_t *cell;            // [lx*ly] global cell id (0: hole, border, padding)
+    const int32_t *side_v, *side_h; // [lx*ly] global id of the west / south side (0: none)
+    const uint8_t *live;            // [lx*ly] 1 for a real cell
+    const int32_t *glat;            // [e_num] lattice index of each cell
+    const int32_t *gside;           // [s_num] lattice index << 1 | 1 for a south side
+    real *h[2], *qv[2], *qh[2];     // double-buffered depth and side discharges
+    real *z, *nv, *nh;              // bed (refreshed each batch), Manning n of the sides
+    int16_t *bi;                    // boundary id, -1 for none
+    int32_t *rain;                  // rain pixel (rain_cells only)
+    real *rain_time, *infil, *max_depth, *max_speed;
+    uint32_t *peak_hi, *peak_lo;
+    real *f0, *fc, *k;              // Horton (horton only)
+    float *terms;                   // [terms][e_num] budget terms of a step by global id, else zero
+    uint32_t *touched;              // [blocks] terms some cell of a 256-cell budget block holds
+};
+
 // Gate controller (core/gate.py:35-206): the caller's tables and controller
 // words plus the library's budget partials [blocks][terms].
 struct GateDev {
@@ -89,6 +113,7 @@ struct Dev {
     real *depth_b, *q_b, *rain_time_b;
     float2 *sdn;  // per side {centre distance, Manning n} (tiled form; filled by initialize)
     TilePlan plan;
+    LatticePlan lat;
 };
 
 __device__ __forceinline__ float maxf(float a, float b) { return a > b ? a : b; }
@@ -378,6 +403,25 @@ void tiled_enqueue_cfl(const Dev &d, const TiledBuild &b, cudaStream_t s, const 
 void tiled_enqueue_batch_end(const Dev &d, cudaStream_t s);
 // Copy the caller's rain_time into the second buffer (batch start).
 void tiled_enqueue_batch_start(const Dev &d, cudaStream_t s);
+
+// u, v of every cell from the caller's arrays (after a batch of the tiled or
+// lattice form has brought its state back).
+void tiled_enqueue_velocity(const Dev &d, cudaStream_t s);
+
+struct LatticeBuild {
+    LatticePlan plan{};
+    void *device_memory = nullptr;  // owned lattice arrays (cudaFree on destroy)
+};
+// Plan the lattice form when the mesh is a uniform grid the form covers
+// (theta = 1, no hanging edges, at most four boundaries, one side per face,
+// uniform cell size, side length and centre distance); 0 on success, else
+// nonzero with `why` set. `d` supplies the mesh and the sizes of the budget.
+int lattice_build(const Dev &d, cudaStream_t s, LatticeBuild *out, char *why, size_t why_len);
+void lattice_enqueue_batch_start(const Dev &d, cudaStream_t s);
+// One step: the fused lattice step, then the pass that reduces its budget
+// blocks, takes the CFL candidate, commits the step and prepares the next.
+void lattice_enqueue_step(const Dev &d, cudaStream_t s);
+void lattice_enqueue_batch_end(const Dev &d, cudaStream_t s);
 
 // Ensemble form: several meshes (members) on the fused tiled step with one
 // common tile size, advanced together. Work lists are (member, index) pairs:

@@ -28,6 +28,8 @@ struct nhf_handle {
     cudaGraphNode_t begin_node = nullptr;
     cudaKernelNodeParams begin_params{};
     nhf::TiledBuild tb{};
+    nhf::LatticeBuild lb{};
+    bool lattice = false;
     nhf::GateDev gate{};
     bool gate_on = false;
     void *gate_mem = nullptr;   // gate budget partials

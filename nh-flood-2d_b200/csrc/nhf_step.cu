@@ -844,9 +844,13 @@ int build_graph(nhf_handle *h)
 {
     cudaGraph_t g = nullptr;
     CK(h, cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
-    k_begin<<<1, 256, 0, h->s>>>(h->dev, 0u, 0u, 0u, 0u, h->tiled ? 1 : 0);
+    k_begin<<<1, 256, 0, h->s>>>(h->dev, 0u, 0u, 0u, 0u, (h->tiled || h->lattice) ? 1 : 0);
 #ifndef NHF_REAL_DOUBLE
-    if (h->tiled) {
+    if (h->lattice) {
+        lattice_enqueue_batch_start(h->dev, h->s);
+        for (int i = 0; i < h->p.batch_size; ++i) lattice_enqueue_step(h->dev, h->s);
+        lattice_enqueue_batch_end(h->dev, h->s);
+    } else if (h->tiled) {
         tiled_enqueue_batch_start(h->dev, h->s);
         for (int i = 0; i < h->p.batch_size; ++i) {
             if (h->gate_on) {
@@ -919,7 +923,7 @@ int member_graph_launch(nhf_handle *h, const uint32_t target[2], const uint32_t 
     CK(h, cudaStreamWaitEvent(h->s, start, 0));
     Dev d = h->dev;
     uint32_t w[4] = {target[0], target[1], origin[0], origin[1]};
-    int prepare_first = h->tiled ? 1 : 0;
+    int prepare_first = (h->tiled || h->lattice) ? 1 : 0;
     void *args[6] = {&d, &w[0], &w[1], &w[2], &w[3], &prepare_first};
     cudaKernelNodeParams kp = h->begin_params;
     kp.kernelParams = args;
@@ -985,15 +989,36 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
 #ifdef NHF_REAL_DOUBLE
     h->path = "multipass (FP64 build)";
 #else
+    // Lattice form when the mesh is a uniform grid it covers (params->path 0 or 2).
+    if (params->path == 0 || params->path == 2) {
+        Dev probe{};
+        probe.m = *mesh;
+        probe.terms = 4 + 6 * mesh->b_num;
+        probe.blocks = (mesh->e_num + kBlock - 1) / kBlock;
+        probe.theta_one = params->sita == RC(1) ? 1 : 0;
+        char why[256] = {0};
+        if (lattice_build(probe, h->s, &h->lb, why, sizeof(why)) == 0) {
+            h->lattice = true;
+            char buf[160];
+            snprintf(buf, sizeof(buf), "lattice(%dx%d,tiles=%dx%d)", h->lb.plan.nx, h->lb.plan.ny,
+                     h->lb.plan.tiles_x, h->lb.plan.tiles_y);
+            h->path = buf;
+        } else {
+            if (h->lb.device_memory) { cudaFree(h->lb.device_memory); h->lb.device_memory = nullptr; }
+            h->path = std::string("multipass (lattice: ") + why + ")";
+        }
+    }
     // Fused tiled step when the mesh allows it (params->path 0, or a tile size).
-    if (params->path == 0 || params->path == 256 || params->path == 512 || params->path == 1024) {
+    if (!h->lattice && (params->path == 0 || params->path == 3 || params->path == 256 || params->path == 512 ||
+                        params->path == 1024)) {
         char why[256] = {0};
         if (params->cfl_mode < 0 || params->cfl_mode > 2) {
             rc = fail(nullptr, NHF_EINVAL, "cfl_mode must be 0, 1 or 2");
             nhf_destroy(h);
             return rc;
         }
-        if (tiled_build(*mesh, h->s, &h->tb, why, sizeof(why), params->path, params->cfl_mode) == 0) {
+        if (tiled_build(*mesh, h->s, &h->tb, why, sizeof(why), params->path == 3 ? 0 : params->path,
+                        params->cfl_mode) == 0) {
             h->tiled = true;
             char buf[160];
             snprintf(buf, sizeof(buf), "tiled(tile=%d,patterns=%d,smem=%zu,cfl=%s)", h->tb.plan.tile,
@@ -1066,6 +1091,9 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
         d.sdn = (float2 *)(base + o_sdn);
         d.plan = h->tb.plan;
     }
+#ifndef NHF_REAL_DOUBLE
+    if (h->lattice) d.lat = h->lb.plan;
+#endif
     // control block initial values
     Ctl init{};
     init.limit_value[0] = __builtin_inff();
@@ -1087,6 +1115,7 @@ int nhf_destroy(nhf_handle *h)
     if (h->graph) cudaGraphExecDestroy(h->graph);
     if (h->graph_def) cudaGraphDestroy(h->graph_def);
     if (h->tb.device_memory) cudaFree(h->tb.device_memory);
+    if (h->lb.device_memory) cudaFree(h->lb.device_memory);
     if (h->scratch) cudaFree(h->scratch);
     if (h->h_begin) cudaFreeHost(h->h_begin);
     if (h->h_trace) cudaFreeHost(h->h_trace);
@@ -1203,7 +1232,7 @@ int nhf_run_batch_async(nhf_handle *h, const uint32_t target[2], const uint32_t 
     if (!h->graph) { rc = build_graph(h); if (rc) return rc; }
     Dev d = h->dev;
     uint32_t w[4] = {target[0], target[1], origin[0], origin[1]};
-    int prepare_first = h->tiled ? 1 : 0;
+    int prepare_first = (h->tiled || h->lattice) ? 1 : 0;
     void *args[6] = {&d, &w[0], &w[1], &w[2], &w[3], &prepare_first};
     cudaKernelNodeParams kp = h->begin_params;
     kp.kernelParams = args;
@@ -1264,6 +1293,9 @@ int nhf_gate_attach(nhf_handle *h, const nhf_gate *gate)
 #ifdef NHF_REAL_DOUBLE
     return fail(h, NHF_EINVAL, "the FP64 build has no gate controller");
 #endif
+    if (h->lattice)
+        return fail(h, NHF_EINVAL, "gate control runs on the multi-pass step or the fused tiled step, not the "
+                                   "lattice form (nhf_params.path = 1, or 256 with cfl_mode 2)");
     if (h->tiled && !(h->tb.plan.tile == 256 && h->tb.plan.split))
         return fail(h, NHF_EINVAL, "gate control runs on the multi-pass step or on the fused step with 256-cell "
                                    "tiles and the separate CFL pass (nhf_params.path = 1, or 256 with cfl_mode 2)");

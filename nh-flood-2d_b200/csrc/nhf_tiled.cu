@@ -1581,6 +1581,13 @@ void ensemble_enqueue_batch_end(const EnsembleLaunch &e, cudaStream_t s)
     k_ens_finish<<<e.members, 256, 0, s>>>(e.devs, e.trace, e.batch);
 }
 
+void tiled_enqueue_velocity(const Dev &d, cudaStream_t s)
+{
+    int grid = (d.m.e_num + 255) / 256;
+    if (grid > 148 * 16) grid = 148 * 16;
+    k_velocity<<<grid, 256, 0, s>>>(d);
+}
+
 void tiled_enqueue_batch_end(const Dev &d, cudaStream_t s)
 {
     int n = d.m.e_num > d.m.s_num ? d.m.e_num : d.m.s_num;

@@ -28,7 +28,10 @@ class StepParams:
     batch_size: int = 32
     g: float = float(G)
     min_dt: float = float(np.float32(MIN_DT))
-    path: str = 'auto'  # 'auto': fused tiled step when the mesh allows it; 'multipass'
+    # 'auto': the lattice form on uniform grids, else the fused tiled step when
+    # the mesh allows it, else multi-pass; 'lattice', 'tiled', 'tile256' /
+    # 'tile512' / 'tile1024', 'multipass' ask for one form
+    path: str = 'auto'
     # fused step: where the next step's CFL candidate is computed. 'auto': in
     # the step on meshes of less than two waves of tiles, else in a separate
     # pass; 'fused': always in the step; 'pass': always a separate pass

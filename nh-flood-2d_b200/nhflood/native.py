@@ -141,12 +141,17 @@ def exported_symbols() -> list[str]:
 
 
 def path_code(path) -> int:
-    """nhf_params.path for a StepParams.path: 'auto', 'multipass' or
-    'tile256' / 'tile512' / 'tile1024' (fused step with that tile size)."""
+    """nhf_params.path for a StepParams.path: 'auto', 'multipass', 'lattice'
+    (uniform grids), 'tiled' (the fused tiled step, tile size by mesh size)
+    or 'tile256' / 'tile512' / 'tile1024' (fused step with that tile size)."""
     if path == 'auto':
         return 0
     if path == 'multipass':
         return 1
+    if path == 'lattice':
+        return 2
+    if path == 'tiled':
+        return 3
     if isinstance(path, str) and path.startswith('tile') and path[4:] in ('256', '512', '1024'):
         return int(path[4:])
     raise ValueError(f'unknown step path {path!r}')

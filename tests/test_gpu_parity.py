@@ -48,15 +48,17 @@ CASES = {
 
 
 def cuda_engine(path):
-    """'auto': the fused step as chosen for the mesh (these small meshes
-    keep the CFL in the step); 'pass': the fused step with the separate CFL
-    pass; 'multipass': the reference's pass structure."""
+    """'auto': the form chosen for the mesh (the lattice form on uniform
+    grids of at least 1024 cells, else the fused tiled step, which keeps the
+    CFL in the step on these small meshes); 'pass': the fused tiled step with
+    the separate CFL pass; 'multipass': the reference's pass structure."""
     def factory(arrays, params):
         from nhflood.native import CudaEngine
-        params.path = 'multipass' if path == 'multipass' else 'auto'
+        params.path = {'multipass': 'multipass', 'pass': 'tiled'}.get(path, 'auto')
         params.cfl = 'pass' if path == 'pass' else 'auto'
         engine = CudaEngine(arrays, params)
-        assert engine.path.startswith('multipass' if path == 'multipass' else 'tiled'), engine.path
+        want = ('multipass',) if path == 'multipass' else ('tiled',) if path == 'pass' else ('tiled', 'lattice')
+        assert engine.path.startswith(want), engine.path
         if path == 'pass':
             assert 'cfl=pass' in engine.path, engine.path
         return engine
@@ -214,8 +216,9 @@ def test_tile_1024_both_cfl_forms_bit_exact(cuda_available, cfl):
         r.close()
 
 
-@pytest.mark.parametrize('name,batches', [('multires_quadtree', 2), ('multires_quadtree_4m', 1), ('dambreak_4096', 1)])
-def test_full_size_configurations_bit_exact(cuda_available, name, batches):
+@pytest.mark.parametrize('name,batches,path', [('multires_quadtree', 2, 'auto'), ('multires_quadtree_4m', 1, 'auto'),
+                                               ('dambreak_4096', 1, 'pass'), ('dambreak_4096', 2, 'auto')])
+def test_full_size_configurations_bit_exact(cuda_available, name, batches, path):
     """The bench's full-size meshes, 1,362,175 quadtree cells (20 km, 2:1,
     hanging edges), the 4.0 M-cell quadtree (36.6 km) and 16,777,216
     dam-break cells (33.5 M sides, 1024-cell tiles, the separate CFL pass):
@@ -228,9 +231,10 @@ def test_full_size_configurations_bit_exact(cuda_available, name, batches):
     from runner import oracle_factory
     workload = {'multires_quadtree': multires_quadtree, 'multires_quadtree_4m': multires_quadtree_4m,
                 'dambreak_4096': dambreak}[name]()
-    runs = [PlainRun(workload, factory, batch_size=32) for factory in (oracle_factory, cuda_engine('auto'))]
+    runs = [PlainRun(workload, factory, batch_size=32) for factory in (oracle_factory, cuda_engine(path))]
     try:
-        assert 'cfl=pass' in runs[1].engine.path, runs[1].engine.path
+        form = runs[1].engine.path
+        assert form.startswith('lattice') if name.startswith('dambreak') and path == 'auto' else 'cfl=pass' in form, form
         for _ in range(batches):
             rows = []
             for run in runs:

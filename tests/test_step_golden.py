@@ -143,14 +143,14 @@ def test_oracle_matches_the_reference_source(golden, tmp_path, name):
 def cuda_factory(path):
     def factory(arrays, params):
         from nhflood.native import CudaEngine
-        params.path = 'multipass' if path == 'multipass' else 'auto'
+        params.path = {'multipass': 'multipass', 'pass': 'tiled', 'lattice': 'lattice'}.get(path, 'auto')
         params.cfl = 'pass' if path == 'pass' else 'auto'
         return CudaEngine(arrays, params)
     return factory
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('path', ['auto', 'pass', 'multipass'])
+@pytest.mark.parametrize('path', ['auto', 'pass', 'multipass', 'lattice'])
 @pytest.mark.parametrize('name', sorted(step_cases.CASES))
 def test_cuda_step_matches_the_reference_source(golden, tmp_path, cuda_available, name, path):
     """The CUDA step, through the C ABI, against the reference's kernels."""
