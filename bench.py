@@ -76,7 +76,9 @@ def algorithmic_bytes(w):
 
 # DRAM bytes (read + write) of one fused step launch, from the ncu captures
 # summarised in profiles/ (k_step_tiled_<workload>.md).
-TRAFFIC_PER_LAUNCH = {'multires_quadtree': 148.207616e6 + 18.244352e6}
+# Timed state (the bench's NVTX timed region); keyed by workload and step form.
+TRAFFIC_PER_LAUNCH = {('multires_quadtree', 'tiled'): 148.976896e6 + 20.993792e6,
+                      ('dambreak_4096', 'tiled'): 1022.048512e6 + 189.920512e6}
 
 
 def launches_per_batch(run) -> int:
@@ -711,7 +713,7 @@ def main():
             'gpu_launches': launches,
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak if achieved else None,
-                         'traffic': TRAFFIC_PER_LAUNCH.get(w.name),
+                         'traffic': TRAFFIC_PER_LAUNCH.get((w.name, eng.path.split('(')[0])),
                          'traffic_unit': 'bytes per step launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)',
                          'algorithmic_bytes_per_launch': b_alg * w.cells,
                          'peak_kind': kind, 'algorithmic_bytes_per_cell_update': b_alg,
