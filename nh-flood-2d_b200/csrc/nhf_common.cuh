@@ -69,7 +69,7 @@ struct TilePlan {
 // (i, j): (j + 2) * lx + (i + 2); the west face of a lattice cell is its
 // "v" side, the south face its "h" side.
 struct LatticePlan {
-    int32_t nx, ny, lx, ly, tiles_x, tiles_y, rain_cells, horton;
+    int32_t nx, ny, lx, ly, tiles_x, tiles_y, rain_cells, horton, blocks_per_sm;
     real sdc_v, sdc_h, len_v, len_h, area, width, height;
     const int32_t *cell;            // [lx*ly] global cell id (0: hole, border, padding)
     const int32_t *side_v, *side_h; // [lx*ly] global id of the west / south side (0: none)

@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -77,7 +78,10 @@ __device__ __forceinline__ real lattice_momentum(const Dev &d, real dt, real za,
     return new_q;
 }
 
-__global__ void __launch_bounds__(kNT, 2) k_lattice_step(const __grid_constant__ Dev d)
+// kMinBlocks resident blocks per SM: 2 (64 registers, no spills) or 3 (40
+// registers, 12 bytes of spills); LatticePlan.blocks_per_sm picks one.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kNT, kMinBlocks) k_lattice_step(const __grid_constant__ Dev d)
 {
     __shared__ real sh_h[kRY][kRX], sh_z[kRY][kRX];
     __shared__ real sh_qv[kVY][kVX], sh_qh[kHY][kHX];  // q*, then the final discharge
@@ -668,6 +672,9 @@ int lattice_build(const Dev &d, cudaStream_t st, LatticeBuild *out, char *why, s
         return no("copy of the cell parameters failed");
     P.rain_cells = 0;
     P.horton = 0;
+    // resident blocks per SM of the step kernel (a tuning knob, default 2)
+    const char *occ = getenv("NHF_LATTICE_BLOCKS");
+    P.blocks_per_sm = (occ && atoi(occ) == 3) ? 3 : 2;
     for (int c = 1; c < e; ++c) {
         if (rain[c] != 0) P.rain_cells = 1;
         if (f0[c] != 0.0f || fc[c] != 0.0f || kk[c] != 0.0f) P.horton = 1;
@@ -733,7 +740,8 @@ void lattice_enqueue_batch_start(const Dev &d, cudaStream_t s)
 
 void lattice_enqueue_step(const Dev &d, cudaStream_t s)
 {
-    k_lattice_step<<<dim3(d.lat.tiles_x, d.lat.tiles_y), kNT, 0, s>>>(d);
+    if (d.lat.blocks_per_sm == 3) k_lattice_step<3><<<dim3(d.lat.tiles_x, d.lat.tiles_y), kNT, 0, s>>>(d);
+    else k_lattice_step<2><<<dim3(d.lat.tiles_x, d.lat.tiles_y), kNT, 0, s>>>(d);
     int grid = std::max(1, std::min(148 * 8, (int)(((long long)(d.lat.nx + 1) * (d.lat.ny + 1) + 255) / 256)));
     k_lattice_cfl<<<grid, 256, 0, s>>>(d);
 }
