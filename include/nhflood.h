@@ -107,8 +107,9 @@ typedef struct nhf_params {
     nhf_real min_h;   /* wet threshold */
     float min_dt;     /* F32(1e-4) CFL floor (solver_compact.py:31) */
     int32_t batch_size; /* steps per batch, 1..64 (clock.py:48-51) */
-    int32_t path;       /* 0: the lattice form on a uniform grid it covers,
-                           else the fused tiled step when the mesh allows it,
+    int32_t path;       /* 0: the lattice form on a uniform grid it covers
+                           of at least 2^20 cells, else the fused tiled step
+                           when the mesh allows it,
                            else multi-pass; 1: always the multi-pass step;
                            2: the lattice form when the mesh allows it, else
                            multi-pass; 3: the fused tiled step (tile size by

@@ -69,7 +69,8 @@ struct TilePlan {
 // (i, j): (j + 2) * lx + (i + 2); the west face of a lattice cell is its
 // "v" side, the south face its "h" side.
 struct LatticePlan {
-    int32_t nx, ny, lx, ly, tiles_x, tiles_y, rain_cells, horton, blocks_per_sm;
+    int32_t nx, ny, lx, ly, strips, chunks, rows, block_warps, min_blocks, rain_cells, horton;
+    int32_t buffer_stride;          // elements from the first to the second buffer of h, qv and qh
     real sdc_v, sdc_h, len_v, len_h, area, width, height;
     const int32_t *cell;            // [lx*ly] global cell id (0: hole, border, padding)
     const int32_t *side_v, *side_h; // [lx*ly] global id of the west / south side (0: none)
@@ -85,6 +86,8 @@ struct LatticePlan {
     real *f0, *fc, *k;              // Horton (horton only)
     float *terms;                   // [terms][e_num] budget terms of a step by global id, else zero
     uint32_t *touched;              // [blocks] terms some cell of a 256-cell budget block holds
+    uint32_t *part;                 // [4][strips*chunks] per-warp limited cells, limited faces, wet cells, min scale bits
+    unsigned long long *part_cfl;   // [strips*chunks] per-warp CFL key
 };
 
 // Gate controller (core/gate.py:35-206): the caller's tables and controller

@@ -3,32 +3,30 @@
 // A uniform NE/NS mesh (one cell size, one side length per orientation,
 // one side per face) is a 2-D lattice whatever its numbering. The planner
 // below recognises it from the mesh tables and numbers it into a padded
-// lattice: a 2-cell border of holes and padding up to whole 32 x 16 tiles.
-// During a batch the library keeps its own lattice-ordered copies of the
-// state (depth and side discharges double-buffered, rain time, infiltration,
-// extrema), gathered from the caller's arrays at the batch start and
-// scattered back at its end. Inside the batch every neighbour is found by
-// arithmetic: no index tables, rows of 32 cells per warp, coalesced loads.
+// lattice: a border of holes (3 columns west, 2 rows south) and padding up
+// to whole strips of 27 columns and chunks of rows. During a batch the
+// library keeps its own lattice-ordered copies of the state (depth and side
+// discharges double-buffered, rain time, infiltration, extrema), gathered
+// from the caller's arrays at the batch start and scattered back at its
+// end. Inside the batch every neighbour is found by arithmetic: no index
+// tables, rows of 32 cells per warp, coalesced loads.
 //
-// One step is two launches. k_lattice_step: a block owns a 32 x 16 tile and
-// stages depth and bed of the tile and two rings of neighbours, then, as
-// the reference's passes do (solver_compact.py:439-613):
-//   momentum q* of the sides the donor factors need (rings <= 1),
-//   donor factors of rings <= 1,
-//   the final discharge of the tile's faces,
-//   sources and depth update of the tile's cells, extrema, budget terms.
-// k_lattice_cfl: the canonical 256-cell budget trees of the blocks the step
-// touched, then compute_cfl (617-641) over the interior sides, and its last
-// block commits the step and prepares the next one. Each quantity is
-// computed in the reference's operation order with the same expressions as
-// the tiled and multi-pass steps, so the three forms and the CPU
-// restatement agree bit for bit.
+// One step is two launches. k_lattice_march: each warp marches up a strip
+// of the lattice with the rows it needs in registers and does, row by row,
+// what the reference's passes do (solver_compact.py:439-641): momentum q*,
+// donor factors, final discharges, sources and depth update, extrema,
+// budget terms and the CFL candidate of the new state; the last block to
+// finish commits the step and prepares the next one. k_lattice_budget: the
+// canonical 256-cell budget trees of the blocks the step touched. Each
+// quantity is computed in the reference's operation order with the same
+// expressions as the tiled and multi-pass steps, so the three forms and the
+// CPU restatement agree bit for bit.
 //
 // Budget terms are sums over the reference's 256-cell blocks of global ids
-// (ei // 256), which a lattice tile does not follow: the step writes each
+// (ei // 256), which a lattice strip does not follow: the step writes each
 // nonzero per-cell term into a scratch array by global id and marks its
-// block; the CFL pass reduces the marked blocks with the canonical tree and
-// clears them.
+// block; the budget pass reduces the marked blocks with the canonical tree
+// and clears them.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,24 +43,22 @@
 namespace nhf {
 namespace {
 
-constexpr int kTX = 32, kTY = 16, kNT = kTX * kTY;  // tile of the step, one thread per cell
-constexpr int kRX = kTX + 4, kRY = kTY + 4;         // staged region: the tile and two rings
-constexpr int kVX = kRX - 1, kVY = kRY - 2;         // west faces of region x 1..35, rows 1..18
-constexpr int kHX = kRX - 2, kHY = kRY - 1;         // south faces of region x 1..34, rows 1..19
-constexpr int kDX = kRX - 2, kDY = kRY - 2;         // donor cells: region x 1..34, rows 1..18
+constexpr int kLanes = 32;                        // a warp marches a strip of 32 lattice columns
+constexpr int kOut = 28;                          // and owns the 28 of lanes 2..29
+constexpr int kWarps = 8, kNT = kLanes * kWarps;  // a block: up to 8 strips side by side
+constexpr int kWest = 2;                          // border columns west of cell column 0
 
-// Momentum (solver_compact.py:439-486) of one side from the staged cells
-// (a: lower, b: higher); the same expressions as the tiled step's P1.
+// Momentum (solver_compact.py:439-486) of one side from the cells either
+// side of it (a: lower, b: higher) and the side's discharge xq and Manning
+// n; the same expressions as the tiled step's P1.
 __device__ __forceinline__ real lattice_momentum(const Dev &d, real dt, real za, real ha, real zb, real hb,
-                                                 bool live_a, bool live_b, const real *q_in, const real *n_arr,
+                                                 bool live_a, bool live_b, real xq, real n,
                                                  const int32_t *side_ids, size_t L, real sdc)
 {
     real hl = za + ha, hr = zb + hb;
     real xwh = rmax(hl, hr) - rmax(rmax(za, zb), kDh);
     real new_q = RC(0);
     if (!(xwh < d.min_h)) {
-        real xq = q_in[L];
-        real n = n_arr[L];
         const bool exterior = live_a != live_b;
         real dx = exterior ? d.sdc[side_ids[L]] : sdc;
         real bf = exterior ? RC(0) : RC(1);
@@ -78,251 +74,149 @@ __device__ __forceinline__ real lattice_momentum(const Dev &d, real dt, real za,
     return new_q;
 }
 
-// kMinBlocks resident blocks per SM: 2 (64 registers, no spills) or 3 (40
-// registers, 12 bytes of spills); LatticePlan.blocks_per_sm picks one.
-template <int kMinBlocks>
-__global__ void __launch_bounds__(kNT, kMinBlocks) k_lattice_step(const __grid_constant__ Dev d)
+// Donor factor (solver_compact.py:491-514) of the cell at lattice index L
+// (boundary id bi) from its depth and the q* of its west, east, south and
+// north faces; sets ``limited`` when the outflow had to be scaled.
+__device__ __forceinline__ real lattice_donor(const Dev &d, const LatticePlan &P, size_t L, int bi, real h, real dt,
+                                              int raining, real qw, real qe, real qs, real qn, bool &limited)
 {
-    __shared__ real sh_h[kRY][kRX], sh_z[kRY][kRX];
-    __shared__ real sh_qv[kVY][kVX], sh_qh[kHY][kHX];  // q*, then the final discharge
-    __shared__ real sh_s[kDY][kDX];                    // donor factors
-    __shared__ uint8_t sh_live[kRY][kRX];
-    __shared__ uint32_t sh_cnt[3], sh_minbits;
-    const LatticePlan &P = d.lat;
     const nhf_mesh &m = d.m;
-    Ctl *c = d.ctl;
-    if (!c->active) return;
-    const int tid = threadIdx.x;
-    if (tid == 0) { sh_cnt[0] = sh_cnt[1] = sh_cnt[2] = 0u; sh_minbits = __float_as_uint(1.0f); }
-    const int parity = c->parity;
-    const real dt = c->dt;
-    const int raining = c->raining;
-    const real *h_in = P.h[parity];
-    real *h_out = P.h[parity ^ 1];
-    const real *qv_in = P.qv[parity], *qh_in = P.qh[parity];
-    real *qv_out = P.qv[parity ^ 1], *qh_out = P.qh[parity ^ 1];
-    const int lx = P.lx;
-    // memory index of region cell (rx, ry): (y0 + ry) * lx + (x0 + rx)
-    const size_t base = (size_t)blockIdx.y * kTY * lx + (size_t)blockIdx.x * kTX;
-
-    for (int i = tid; i < kRX * kRY; i += kNT) {
-        const int rx = i % kRX, ry = i / kRX;
-        const size_t L = base + (size_t)ry * lx + rx;
-        sh_h[ry][rx] = h_in[L];
-        sh_z[ry][rx] = P.z[L];
-        sh_live[ry][rx] = P.live[L];
+    int kind = -1;
+    real discharge = RC(0);
+    if (bi >= 0) {
+        kind = m.kind[bi];
+        if (kind == 1) discharge = d.values[bi] * m.weight[__ldg(P.cell + L)];
     }
-    __syncthreads();
-
-    // momentum of the west faces (region x 1..35) and south faces (x 1..34) of rows 1..18 / 1..19
-    for (int i = tid; i < kVX * kVY + kHX * kHY; i += kNT) {
-        if (i < kVX * kVY) {
-            const int rx = i % kVX + 1, ry = i / kVX + 1;
-            const bool la = sh_live[ry][rx - 1], lb = sh_live[ry][rx];
-            real q = RC(0);
-            if (la || lb)
-                q = lattice_momentum(d, dt, sh_z[ry][rx - 1], sh_h[ry][rx - 1], sh_z[ry][rx], sh_h[ry][rx], la, lb,
-                                     qv_in, P.nv, P.side_v, base + (size_t)ry * lx + rx, P.sdc_v);
-            sh_qv[ry - 1][rx - 1] = q;
-        } else {
-            const int k = i - kVX * kVY;
-            const int rx = k % kHX + 1, ry = k / kHX + 1;
-            const bool la = sh_live[ry - 1][rx], lb = sh_live[ry][rx];
-            real q = RC(0);
-            if (la || lb)
-                q = lattice_momentum(d, dt, sh_z[ry - 1][rx], sh_h[ry - 1][rx], sh_z[ry][rx], sh_h[ry][rx], la, lb,
-                                     qh_in, P.nh, P.side_h, base + (size_t)ry * lx + rx, P.sdc_h);
-            sh_qh[ry - 1][rx - 1] = q;
-        }
-    }
-    __syncthreads();
-
-    // donor factors (solver_compact.py:491-514) of rings <= 1: region x 1..34, rows 1..18
-    {
-        uint32_t my_limited = 0, my_min = __float_as_uint(1.0f);
-        for (int i = tid; i < kDX * kDY; i += kNT) {
-            const int rx = i % kDX + 1, ry = i / kDX + 1;
-            real sc = RC(0);  // holes: the sentinel's donor factor
-            if (sh_live[ry][rx]) {
-                const size_t L = base + (size_t)ry * lx + rx;
-                const int bi = P.bi[L];
-                int kind = -1;
-                real discharge = RC(0);
-                if (bi >= 0) {
-                    kind = m.kind[bi];
-                    if (kind == 1) discharge = d.values[bi] * m.weight[P.cell[L]];
-                }
-                const real rainq = raining ? d.rain_rates[P.rain_cells ? P.rain[L] : 0] : RC(0);
-                real pipe = RC(0);
-                real positive = (rmax(pipe, RC(0)) + rmax(discharge, RC(0))) * dt;
-                real area = P.area;
-                real available = sh_h[ry][rx] * area + positive + rainq * dt * area;
-                real outgoing = (rmax(-pipe, RC(0)) + rmax(-discharge, RC(0))) * dt;
-                const real face[4] = {sh_qv[ry - 1][rx - 1] * P.len_v, sh_qv[ry - 1][rx] * P.len_v,
-                                      sh_qh[ry - 1][rx - 1] * P.len_h, sh_qh[ry][rx - 1] * P.len_h};
+    const real rainq = raining ? d.rain_rates[P.rain_cells ? __ldg(P.rain + L) : 0] : RC(0);
+    real pipe = RC(0);
+    real positive = (rmax(pipe, RC(0)) + rmax(discharge, RC(0))) * dt;
+    real area = P.area;
+    real available = h * area + positive + rainq * dt * area;
+    real outgoing = (rmax(-pipe, RC(0)) + rmax(-discharge, RC(0))) * dt;
+    const real face[4] = {qw * P.len_v, qe * P.len_v, qs * P.len_h, qn * P.len_h};
 #pragma unroll
-                for (int dd = 0; dd < 4; ++dd) {
-                    real signed_q = face[dd];
-                    if (dd == 0 || dd == 2) signed_q = -signed_q;
-                    outgoing += rmax(signed_q, RC(0)) * dt;
-                }
-                sc = RC(1);
-                if (outgoing > available && kind != 0) {
-                    sc = available / outgoing;
-                    if (rx >= 2 && rx < 2 + kTX && ry >= 2 && ry < 2 + kTY) {
-                        my_limited += 1;
-                        uint32_t bits = __float_as_uint(sc);
-                        my_min = bits < my_min ? bits : my_min;
-                    }
-                }
-            }
-            sh_s[ry - 1][rx - 1] = sc;
-        }
-        if (my_limited) {
-            atomicAdd(&sh_cnt[0], my_limited);
-            atomicMin(&sh_minbits, my_min);
-        }
+    for (int dd = 0; dd < 4; ++dd) {
+        real signed_q = face[dd];
+        if (dd == 0 || dd == 2) signed_q = -signed_q;
+        outgoing += rmax(signed_q, RC(0)) * dt;
     }
-    __syncthreads();
+    real sc = RC(1);
+    limited = false;
+    if (outgoing > available && kind != 0) {
+        sc = available / outgoing;
+        limited = true;
+    }
+    return sc;
+}
 
-    // final discharge (solver_compact.py:516-522) of the faces of the tile's
-    // cells: west faces x 2..34 of rows 2..17, south faces x 2..33 of rows 2..18
-    {
-        uint32_t my_faces = 0;
-        constexpr int nv = (kTX + 1) * kTY, nh = kTX * (kTY + 1);
-        for (int i = tid; i < nv + nh; i += kNT) {
-            if (i < nv) {
-                const int rx = i % (kTX + 1) + 2, ry = i / (kTX + 1) + 2;
-                const real q = sh_qv[ry - 1][rx - 1];
-                const real sc = q >= RC(0) ? sh_s[ry - 1][rx - 2] : sh_s[ry - 1][rx - 1];
-                if (rx < 2 + kTX && q != RC(0) && sc < RC(1)) my_faces += 1;
-                sh_qv[ry - 1][rx - 1] = q * sc;
-            } else {
-                const int k = i - nv;
-                const int rx = k % kTX + 2, ry = k / kTX + 2;
-                const real q = sh_qh[ry - 1][rx - 1];
-                const real sc = q >= RC(0) ? sh_s[ry - 2][rx - 1] : sh_s[ry - 1][rx - 1];
-                if (ry < 2 + kTY && q != RC(0) && sc < RC(1)) my_faces += 1;
-                sh_qh[ry - 1][rx - 1] = q * sc;
-            }
-        }
-        if (my_faces) atomicAdd(&sh_cnt[1], my_faces);
-    }
-    __syncthreads();
+// The per-cell inputs of a depth update, loaded a row ahead of their use.
+struct LatticeCell {
+    int g, bi;
+    real rain_time, infil, max_speed, max_depth;
+};
 
-    // sources and depth update (solver_compact.py:525-610) of this thread's cell
-    const int rx = tid % kTX + 2, ry = tid / kTX + 2;
-    const size_t L = base + (size_t)ry * lx + rx;
-    uint32_t wet = 0;
-    if (sh_live[ry][rx]) {
-        const int g = P.cell[L];
-        const int B = m.b_num;
-        const int bi = P.bi[L];
-        const int kind = bi >= 0 ? m.kind[bi] : -1;
-        const real sc = sh_s[ry - 1][rx - 1];
-        real pq = RC(0);
-        real pipe = rmax(pq, RC(0)) + rmin(pq, RC(0)) * sc;
-        real discharge = RC(0), t_discharge = RC(0);
-        if (kind == 1) {
-            real requested = d.values[bi] * m.weight[g];
-            discharge = rmax(requested, RC(0)) + rmin(requested, RC(0)) * sc;
-            t_discharge = discharge * dt;
-        }
-        real ssq = pipe + discharge;
-        const real rainq = raining ? d.rain_rates[P.rain_cells ? P.rain[L] : 0] : RC(0);
-        real infil;
-        if (rainq > RC(0)) {
-            real rt = P.rain_time[L] + dt;
-            P.rain_time[L] = rt;
-            // without Horton classes every f0, fc and k is zero (checked by the planner)
-            real f0 = P.horton ? P.f0[L] : RC(0), fc = P.horton ? P.fc[L] : RC(0);
-            real diff = f0 - fc;
-            const real old = P.infil[L];
-            infil = diff == RC(0) ? fc + RC(0) : fc + diff * exp_real(-(P.horton ? P.k[L] : RC(0)) * rt / RC(3600.0));
-            if (__float_as_uint(infil) != __float_as_uint(old)) P.infil[L] = infil;
-        } else {
-            infil = P.infil[L];
-        }
-        real ql = RC(0) + sh_qv[ry - 1][rx - 1] * P.len_v, qr = RC(0) + sh_qv[ry - 1][rx] * P.len_v;
-        real qb = RC(0) + sh_qh[ry - 1][rx - 1] * P.len_h, qt = RC(0) + sh_qh[ry][rx - 1] * P.len_h;
-        real tq = ql - qr + qb - qt + ssq;
-        real ea = P.area;
-        real rain_depth = rainq * dt;
-        real flux = tq * dt;
-        real increment = (flux == RC(0) ? flux : flux / ea) + rain_depth;
-        real previous = sh_h[ry][rx];
-        real raw_depth = previous + increment;
-        real removed = rmin(infil * dt, rmax(raw_depth, RC(0)));
-        raw_depth -= removed;
-        real floor_v = rmax(-raw_depth, RC(0));
-        real level[5] = {RC(0), RC(0), RC(0), RC(0), RC(0)};
-        real depth;
-        if (kind == 0) {
-            real target = rmax(d.level_values[bi] - sh_z[ry][rx], RC(0));
-            level[0] = (target - previous) * ea;
-            level[1] = -(ql - qr + qb - qt) * dt;
-            level[2] = -pipe * dt;
-            level[3] = -rain_depth * ea;
-            level[4] = removed * ea;
-            depth = target;
-        } else {
-            depth = rmax(raw_depth, RC(0));
-        }
-        h_out[L] = depth;
-        real h = rmax(depth, RC(0.01));
-        real u = RC(0), v = RC(0);
-        if (depth >= d.min_h) {
-            u = (ql + qr) / P.height / h * RC(0.5);
-            v = (qb + qt) / P.width / h * RC(0.5);
-        }
-        real s2 = u * u + v * v;
-        real speed = s2 == RC(0) ? RC(0) : sqrt(s2);
-        if (speed > P.max_speed[L]) P.max_speed[L] = speed;
-        if (depth > P.max_depth[L]) {
-            P.max_depth[L] = depth;
-            P.peak_hi[L] = c->step_end[0];
-            P.peak_lo[L] = c->step_end[1];
-        }
-        wet = depth >= d.min_h ? 1u : 0u;
-        // budget terms of this cell by global id: 0 removed, 1 / 2 bed clamp
-        // off / on level cells, 3 pipe (none), 4 + 5 b + k level, 4 + 5 B + b discharge
-        uint32_t mask = 0;
-        float *terms = P.terms;
-        const size_t e = (size_t)m.e_num;
-        const real removed_v = removed * ea, floor_a = floor_v * ea;
-        if (removed_v != RC(0)) { terms[0 * e + g] = removed_v; mask |= 1u; }
-        if (floor_a != RC(0)) {
-            const int t = kind == 0 ? 2 : 1;
-            terms[t * e + g] = floor_a;
-            mask |= 1u << t;
-        }
-        if (kind == 0)
-            for (int q5 = 0; q5 < 5; ++q5)
-                if (level[q5] != RC(0)) {
-                    const int t = 4 + 5 * bi + q5;
-                    terms[t * e + g] = level[q5];
-                    mask |= 1u << t;
-                }
-        if (kind == 1 && t_discharge != RC(0)) {
-            const int t = 4 + 5 * B + bi;
-            terms[t * e + g] = t_discharge;
-            mask |= 1u << t;
-        }
-        if (mask) atomicOr(&P.touched[g >> 8], mask);
+// Sources and depth update (solver_compact.py:525-610) of the cell at
+// lattice index L from its old depth, its donor factor and the final
+// discharges of its four faces; writes the cell's rain time, infiltration,
+// extrema and budget terms and returns the new depth.
+__device__ __forceinline__ real lattice_update(const Dev &d, const LatticePlan &P, size_t L, real dt, int raining,
+                                               real previous, real z, real sc, real fw, real fe, real fs, real fn,
+                                               const LatticeCell &k, const uint32_t *step_end)
+{
+    const nhf_mesh &m = d.m;
+    const int g = k.g, bi = k.bi;
+    const int B = m.b_num;
+    const int kind = bi >= 0 ? m.kind[bi] : -1;
+    real pq = RC(0);
+    real pipe = rmax(pq, RC(0)) + rmin(pq, RC(0)) * sc;
+    real discharge = RC(0), t_discharge = RC(0);
+    if (kind == 1) {
+        real requested = d.values[bi] * m.weight[g];
+        discharge = rmax(requested, RC(0)) + rmin(requested, RC(0)) * sc;
+        t_discharge = discharge * dt;
     }
-    // the tile's own faces: west and south of each cell
-    if (sh_live[ry][rx - 1] || sh_live[ry][rx]) qv_out[L] = sh_qv[ry - 1][rx - 1];
-    if (sh_live[ry - 1][rx] || sh_live[ry][rx]) qh_out[L] = sh_qh[ry - 1][rx - 1];
-    const unsigned wet_warp = __popc(__ballot_sync(0xffffffffu, wet));
-    if ((tid & 31) == 0 && wet_warp) atomicAdd(&sh_cnt[2], wet_warp);
-    __syncthreads();
-    if (tid == 0) {
-        if (sh_cnt[0]) {
-            atomicAdd(&c->limited_cells, sh_cnt[0]);
-            atomicMin(&c->min_scale_bits, sh_minbits);
-        }
-        if (sh_cnt[1]) atomicAdd(&c->limited_faces, sh_cnt[1]);
-        if (sh_cnt[2]) atomicAdd(&c->wet, sh_cnt[2]);
+    real ssq = pipe + discharge;
+    const real rainq = raining ? d.rain_rates[P.rain_cells ? __ldg(P.rain + L) : 0] : RC(0);
+    real infil;
+    if (rainq > RC(0)) {
+        real rt = k.rain_time + dt;
+        P.rain_time[L] = rt;
+        // without Horton classes every f0, fc and k is zero (checked by the planner)
+        real f0 = P.horton ? P.f0[L] : RC(0), fc = P.horton ? P.fc[L] : RC(0);
+        real diff = f0 - fc;
+        infil = diff == RC(0) ? fc + RC(0) : fc + diff * exp_real(-(P.horton ? P.k[L] : RC(0)) * rt / RC(3600.0));
+        if (__float_as_uint(infil) != __float_as_uint(k.infil)) P.infil[L] = infil;
+    } else {
+        infil = k.infil;
+    }
+    real ql = RC(0) + fw * P.len_v, qr = RC(0) + fe * P.len_v;
+    real qb = RC(0) + fs * P.len_h, qt = RC(0) + fn * P.len_h;
+    real tq = ql - qr + qb - qt + ssq;
+    real ea = P.area;
+    real rain_depth = rainq * dt;
+    real flux = tq * dt;
+    real increment = (flux == RC(0) ? flux : flux / ea) + rain_depth;
+    real raw_depth = previous + increment;
+    real removed = rmin(infil * dt, rmax(raw_depth, RC(0)));
+    raw_depth -= removed;
+    real floor_v = rmax(-raw_depth, RC(0));
+    real depth = kind == 0 ? rmax(d.level_values[bi] - z, RC(0)) : rmax(raw_depth, RC(0));
+    real h = rmax(depth, RC(0.01));
+    real u = RC(0), v = RC(0);
+    if (depth >= d.min_h) {
+        u = (ql + qr) / P.height / h * RC(0.5);
+        v = (qb + qt) / P.width / h * RC(0.5);
+    }
+    real s2 = u * u + v * v;
+    real speed = s2 == RC(0) ? RC(0) : sqrt(s2);
+    if (speed > k.max_speed) P.max_speed[L] = speed;
+    if (depth > k.max_depth) {
+        P.max_depth[L] = depth;
+        P.peak_hi[L] = __ldg(step_end);  // the clock words are not written during the march
+        P.peak_lo[L] = __ldg(step_end + 1);
+    }
+    // budget terms of this cell by global id: 0 removed, 1 / 2 bed clamp
+    // off / on level cells, 3 pipe (none), 4 + 5 b + k level, 4 + 5 B + b discharge
+    uint32_t mask = 0;
+    float *terms = P.terms;
+    const size_t e = (size_t)m.e_num;
+    const real removed_v = removed * ea, floor_a = floor_v * ea;
+    if (removed_v != RC(0)) { terms[0 * e + g] = removed_v; mask |= 1u; }
+    if (floor_a != RC(0)) {
+        const int t = kind == 0 ? 2 : 1;
+        terms[t * e + g] = floor_a;
+        mask |= 1u << t;
+    }
+    if (kind == 0) {
+        const real level[5] = {(depth - previous) * ea, -(ql - qr + qb - qt) * dt, -pipe * dt, -rain_depth * ea,
+                               removed * ea};
+        for (int q5 = 0; q5 < 5; ++q5)
+            if (level[q5] != RC(0)) {
+                const int t = 4 + 5 * bi + q5;
+                terms[t * e + g] = level[q5];
+                mask |= 1u << t;
+            }
+    }
+    if (kind == 1 && t_discharge != RC(0)) {
+        const int t = 4 + 5 * B + bi;
+        terms[t * e + g] = t_discharge;
+        mask |= 1u << t;
+    }
+    if (mask) atomicOr(&P.touched[g >> 8], mask);
+    return depth;
+}
+
+// CFL candidate (solver_compact.py:617-641) of one interior side, folded
+// into the running minimum key (dt bits << 32 | side id); the side id is
+// read only for a candidate at or below the minimum.
+__device__ __forceinline__ void lattice_cfl(const Dev &d, real len, real q, real za, real ha, real zb, real hb,
+                                            const int32_t *side_ids, size_t L, unsigned long long &best)
+{
+    const real fd = cfl_face_depth(za, ha, zb, hb);
+    const uint32_t bits = __float_as_uint(cfl_value(d.afa, d.g, len, q, fd));
+    if (bits <= (uint32_t)(best >> 32)) {
+        const unsigned long long key = ((unsigned long long)bits << 32) | (unsigned)__ldg(side_ids + L);
+        best = key < best ? key : best;
     }
 }
 
@@ -359,78 +253,248 @@ __device__ void lattice_prepare(const Dev &d, Ctl *c)
         c->limit_ids[0] = si; c->limit_ids[1] = el; c->limit_ids[2] = eh;
     }
 }
-
-// Budget blocks the step touched (the canonical 256-cell tree), then the CFL
-// candidate of the new state over the interior sides; the last block commits
-// the step and prepares the next.
-__global__ void __launch_bounds__(256) k_lattice_cfl(const __grid_constant__ Dev d)
+// One step of the lattice form (solver_compact.py:439-641) but the CFL of
+// the sides on strip and chunk edges, which k_lattice_close takes.
+//
+// A warp owns a strip of 32 lattice columns and P.rows rows and marches up
+// it one row per iteration, the rows it needs held in registers and the
+// west/east neighbours taken by shuffles. Iteration y forms q* of the south
+// faces of row y + 2 and the west faces of row y + 1 (439-486), the donor
+// factors of row y + 1 (491-514), the final discharge of the south faces
+// of row y + 1 and the west faces of row y (516-522), the update of row y
+// (525-610) and the CFL candidates (617-641) of row y's west and south
+// sides whose cells this warp updated; and it loads what iteration y + 1
+// will need (row y + 3 and the side discharges and Manning n first, the
+// update inputs of row y + 1 after the update), so the loads of a row are
+// in flight while the row before it is computed. Lanes 2..29 own the
+// strip's 28 columns; lanes 0, 1, 30 and 31 are the halo the donor factors
+// need. The first three iterations, below the chunk's rows, only fill the
+// registers. No shared memory and no block barrier: each warp writes its
+// counters and CFL minimum for the close pass and leaves.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kNT, kMinBlocks) k_lattice_march(const __grid_constant__ Dev d)
+{
+    constexpr unsigned kAll = 0xffffffffu;
+    const LatticePlan &P = d.lat;
+    Ctl *c = d.ctl;
+    if (!c->active) return;
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    const int strip = blockIdx.x * warps + (threadIdx.x >> 5);
+    if (strip >= P.strips) return;
+    // limited cells, limited faces and wet cells of this lane, 10 bits each
+    // (at most 2 x 256 rows), and the smallest donor factor's bits
+    uint32_t counts = 0, min_bits = __float_as_uint(1.0f);
+    unsigned long long best = kCflEmpty;
+    {
+        const real dt = c->dt;
+        const int raining = c->raining;
+        const int parity = c->parity;
+        // the second buffer of depth, west and south discharge lies
+        // P.buffer_stride elements after the first: one offset selects the
+        // state a step reads (rd) and the one it writes (wr), the bases stay
+        // kernel parameters
+        const int rd = parity ? P.buffer_stride : 0, wr = P.buffer_stride - rd;
+        const int lx = P.lx;  // lattice indices fit 30 bits (checked by the planner)
+        const int x = strip * kOut + lane;  // lattice column of this lane
+        const bool own = lane >= 2 && lane < 2 + kOut;
+        const int y0 = 2 + blockIdx.y * P.rows, y1 = y0 + P.rows;  // the rows this warp updates
+        // iteration y holds row y (h0 z0 l0), row y + 1 (h1 z1 l1), row y + 2
+        // (h2 z2 l2), the inputs of the south side of row y + 2 (xs ns), of
+        // the west side of row y + 1 (xw nw), the boundary id of row y + 1
+        // (b1) and the update inputs of row y (k0); it loads row y + 3 and
+        // the side inputs first, the update inputs of row y + 1 last
+        int L1 = (y0 - 2) * lx + x;
+        int L2 = L1 + lx;
+        real h1 = __ldg(P.h[0] + rd + L1), z1 = __ldg(P.z + L1);
+        bool l1 = __ldg(P.live + L1);
+        real h2 = __ldg(P.h[0] + rd + L2), z2 = __ldg(P.z + L2);
+        bool l2 = __ldg(P.live + L2);
+        real xs = __ldg(P.qh[0] + rd + L2), ns = __ldg(P.nh + L2);
+        real xw = __ldg(P.qv[0] + rd + L1), nw = __ldg(P.nv + L1);
+        int b1 = __ldg(P.bi + L1);
+        LatticeCell k0{0, -1, RC(0), RC(0), RC(0), RC(0)};
+        real h0 = RC(0), z0 = RC(0), hm = RC(0), zm = RC(0);
+        bool l0 = false, lm = false;
+        real qs1 = RC(0), qw0 = RC(0), d0 = RC(0), fs0 = RC(0);  // q* south y+1, q* west y, donor y, final south y
+        for (int y = y0 - 3; y < y1; ++y) {
+            const int L0 = L1 - lx, L3 = L2 + lx;
+            // what iteration y + 1 needs
+            const real h3 = __ldg(P.h[0] + rd + L3), z3 = __ldg(P.z + L3);
+            const bool l3 = __ldg(P.live + L3);
+            const real xs3 = __ldg(P.qh[0] + rd + L3), ns3 = __ldg(P.nh + L3);
+            const real xw2 = __ldg(P.qv[0] + rd + L2), nw2 = __ldg(P.nv + L2);
+            const int b2 = __ldg(P.bi + L2);
+            // q* of the south side of row y + 2 and of the west side of row y + 1
+            real qs2 = RC(0);
+            if (l1 || l2) qs2 = lattice_momentum(d, dt, z1, h1, z2, h2, l1, l2, xs, ns, P.side_h, L2, P.sdc_h);
+            const real hw = __shfl_up_sync(kAll, h1, 1), zw = __shfl_up_sync(kAll, z1, 1);
+            const bool lw = __shfl_up_sync(kAll, (int)l1, 1) != 0;
+            real qw1 = RC(0);
+            if (lane > 0 && (lw || l1)) qw1 = lattice_momentum(d, dt, zw, hw, z1, h1, lw, l1, xw, nw, P.side_v, L1, P.sdc_v);
+            const real qe1 = __shfl_down_sync(kAll, qw1, 1);
+            const bool out1 = own && y + 1 >= y0 && y + 1 < y1, out0 = own && y >= y0;
+            // donor factor of row y + 1 (holes: the sentinel's factor 0)
+            real d1 = RC(0);
+            if (l1) {
+                bool limited;
+                d1 = lattice_donor(d, P, L1, b1, h1, dt, raining, qw1, qe1, qs1, qs2, limited);
+                if (limited && out1) {
+                    counts += 1u;
+                    const uint32_t bits = __float_as_uint(d1);
+                    min_bits = bits < min_bits ? bits : min_bits;
+                }
+            }
+            // final discharge of the south side of row y + 1 and the west side of row y
+            const real ss = qs1 >= RC(0) ? d0 : d1;
+            const real fs1 = qs1 * ss;
+            if (out1 && qs1 != RC(0) && ss < RC(1)) counts += 1u << 10;
+            const real dwest = __shfl_up_sync(kAll, d0, 1);
+            const real sw = qw0 >= RC(0) ? dwest : d0;
+            const real fw0 = qw0 * sw;
+            if (out0 && qw0 != RC(0) && sw < RC(1)) counts += 1u << 10;
+            const real fe0 = __shfl_down_sync(kAll, fw0, 1);
+            // update of row y
+            real hn = h0;
+            if (out0 && l0) {
+                hn = lattice_update(d, P, L0, dt, raining, h0, z0, d0, fw0, fe0, fs0, fs1, k0, c->step_end);
+                P.h[0][wr + L0] = hn;
+                if (hn >= d.min_h) counts += 1u << 20;
+            }
+            const real hnw = __shfl_up_sync(kAll, hn, 1), zw0 = __shfl_up_sync(kAll, z0, 1);
+            const bool lw0 = __shfl_up_sync(kAll, (int)l0, 1) != 0;
+            if (out0) {
+                if (l0 || lw0) P.qv[0][wr + L0] = fw0;
+                if (l0 || lm) P.qh[0][wr + L0] = fs0;
+                // interior sides both of whose cells this warp updated
+                if (l0 && lw0 && lane > 2) lattice_cfl(d, P.len_v, fw0, zw0, hnw, z0, hn, P.side_v, L0, best);
+                if (l0 && lm && y > y0) lattice_cfl(d, P.len_h, fs0, zm, hm, z0, hn, P.side_h, L0, best);
+            }
+            // the update inputs of row y + 1, half an iteration ahead of their use
+            k0 = LatticeCell{0, b1, RC(0), RC(0), RC(0), RC(0)};
+            if (own && l1 && y + 1 >= y0 && y + 1 < y1) {
+                k0.g = __ldg(P.cell + L1);
+                k0.rain_time = P.rain_time[L1];
+                k0.infil = P.infil[L1];
+                k0.max_speed = P.max_speed[L1];
+                k0.max_depth = P.max_depth[L1];
+            }
+            hm = hn; zm = z0; lm = l0;
+            h0 = h1; z0 = z1; l0 = l1;
+            h1 = h2; z1 = z2; l1 = l2;
+            h2 = h3; z2 = z3; l2 = l3;
+            xs = xs3; ns = ns3; xw = xw2; nw = nw2;
+            b1 = b2;
+            qs1 = qs2; qw0 = qw1; d0 = d1; fs0 = fs1;
+            L1 += lx; L2 += lx;
+        }
+    }
+    // counters and the CFL candidate of the warp, for the close pass: no
+    // block barrier, so a warp leaves as soon as its strip is done
+    const uint32_t n_lim = __reduce_add_sync(kAll, counts & 1023u);
+    const uint32_t n_faces = __reduce_add_sync(kAll, (counts >> 10) & 1023u);
+    const uint32_t n_wet = __reduce_add_sync(kAll, counts >> 20);
+    min_bits = __reduce_min_sync(kAll, min_bits);
+    best = warp_min_u64(best);
+    if (lane == 0) {
+        const size_t w = (size_t)blockIdx.y * P.strips + strip, W = (size_t)P.strips * P.chunks;
+        P.part[w] = n_lim;
+        P.part[W + w] = n_faces;
+        P.part[2 * W + w] = n_wet;
+        P.part[3 * W + w] = min_bits;
+        P.part_cfl[w] = best;
+    }
+}
+// After the march: the budget blocks the step touched (the canonical
+// 256-cell tree of each term a block holds, device_budget.py:28-84, added
+// into the compensated partials; scratch and marks cleared), the CFL
+// candidates (solver_compact.py:617-641) of the sides on strip and chunk
+// edges, whose two cells two different warps updated, and in the last block
+// to finish the commit of the step and the prepare of the next.
+__global__ void __launch_bounds__(256, 3) k_lattice_close(const __grid_constant__ Dev d)
 {
     __shared__ double sh_tree[256];
     __shared__ unsigned long long sh_min[8];
+    __shared__ uint32_t sh_cnt[8][4];
     __shared__ bool last;
     const LatticePlan &P = d.lat;
     const nhf_mesh &m = d.m;
     Ctl *c = d.ctl;
-    const int active = c->active;
     const int tid = threadIdx.x;
-    if (active) {
-        const size_t e = (size_t)m.e_num;
-        const int T = d.terms;
-        for (int b = blockIdx.x; b < d.blocks; b += gridDim.x) {
-            const uint32_t mask = P.touched[b];
-            if (!mask) continue;
-            const int g = b * 256 + tid;
-            for (uint32_t rest = mask; rest; rest &= rest - 1) {
-                const int t = __ffs(rest) - 1;
-                float v = 0.0f;
-                if (g < m.e_num) {
-                    v = P.terms[t * e + g];
-                    if (v != 0.0f) P.terms[t * e + g] = 0.0f;
-                }
-                const double sum = block_tree((double)v, sh_tree);
-                if (tid == 0) acc_add(d.acc_sum + (size_t)b * T + t, d.acc_comp + (size_t)b * T + t, sum);
+    const size_t e = (size_t)m.e_num;
+    const int T = d.terms;
+    for (int b = blockIdx.x; b < d.blocks; b += gridDim.x) {
+        const uint32_t mask = P.touched[b];
+        if (!mask) continue;
+        const int g = b * 256 + tid;
+        for (uint32_t rest = mask; rest; rest &= rest - 1) {
+            const int t = __ffs(rest) - 1;
+            float v = 0.0f;
+            if (g < m.e_num) {
+                v = P.terms[t * e + g];
+                if (v != 0.0f) P.terms[t * e + g] = 0.0f;
             }
-            if (tid == 0) P.touched[b] = 0u;
+            const double sum = block_tree((double)v, sh_tree);
+            if (tid == 0) acc_add(d.acc_sum + (size_t)b * T + t, d.acc_comp + (size_t)b * T + t, sum);
         }
+        if (tid == 0) P.touched[b] = 0u;
     }
+    const int active = c->active;
     unsigned long long best = kCflEmpty;
+    uint32_t lim = 0, faces = 0, wet = 0, mb = __float_as_uint(1.0f);
     if (active) {
-        const int p = c->parity ^ 1;  // the state the step just wrote
+        // the march's per-warp counters and CFL minima
+        const long long W = (long long)P.strips * P.chunks;
+        for (long long w = (long long)blockIdx.x * 256 + tid; w < W; w += (long long)gridDim.x * 256) {
+            lim += P.part[w];
+            faces += P.part[W + w];
+            wet += P.part[2 * W + w];
+            mb = P.part[3 * W + w] < mb ? P.part[3 * W + w] : mb;
+            best = P.part_cfl[w] < best ? P.part_cfl[w] : best;
+        }
+        const int p = c->parity ^ 1;  // the state the march just wrote
         const real *h = P.h[p], *qv = P.qv[p], *qh = P.qh[p];
-        const int nx = P.nx, ny = P.ny, lx = P.lx;
-        const long long n = (long long)(nx + 1) * (ny + 1);
-        for (long long idx = (long long)blockIdx.x * 256 + tid; idx < n; idx += (long long)gridDim.x * 256) {
-            const int x = (int)(idx % (nx + 1)), y = (int)(idx / (nx + 1));
-            const size_t L = (size_t)(y + 2) * lx + (x + 2);
-            const bool here = P.live[L];
-            if (!here) continue;
-            if (P.live[L - 1]) {  // west side
-                const real fd = cfl_face_depth(P.z[L - 1], h[L - 1], P.z[L], h[L]);
-                const real cfl = cfl_value(d.afa, d.g, P.len_v, qv[L], fd);
-                const uint32_t bits = __float_as_uint(cfl);
-                if (bits <= (uint32_t)(best >> 32)) {
-                    const unsigned long long key = ((unsigned long long)bits << 32) | (unsigned)P.side_v[L];
-                    best = key < best ? key : best;
-                }
-            }
-            if (P.live[L - lx]) {  // south side
-                const real fd = cfl_face_depth(P.z[L - lx], h[L - lx], P.z[L], h[L]);
-                const real cfl = cfl_value(d.afa, d.g, P.len_h, qh[L], fd);
-                const uint32_t bits = __float_as_uint(cfl);
-                if (bits <= (uint32_t)(best >> 32)) {
-                    const unsigned long long key = ((unsigned long long)bits << 32) | (unsigned)P.side_h[L];
-                    best = key < best ? key : best;
-                }
+        const size_t lx = (size_t)P.lx;
+        const long long rows = (long long)P.chunks * P.rows, cols = (long long)P.strips * kOut;
+        const long long n_west = (long long)P.strips * rows, n = n_west + (long long)P.chunks * cols;
+        for (long long i = (long long)blockIdx.x * 256 + tid; i < n; i += (long long)gridDim.x * 256) {
+            if (i < n_west) {  // west side of the first column of a strip
+                const long long s = i / rows, y = 2 + i % rows;
+                const size_t L = (size_t)y * lx + (size_t)(s * kOut + 2);
+                if (P.live[L] && P.live[L - 1])
+                    lattice_cfl(d, P.len_v, qv[L], P.z[L - 1], h[L - 1], P.z[L], h[L], P.side_v, L, best);
+            } else {  // south side of the first row of a chunk
+                const long long k = i - n_west, ch = k / cols, x = 2 + k % cols;
+                const size_t L = (size_t)(2 + ch * P.rows) * lx + (size_t)x;
+                if (P.live[L] && P.live[L - lx])
+                    lattice_cfl(d, P.len_h, qh[L], P.z[L - lx], h[L - lx], P.z[L], h[L], P.side_h, L, best);
             }
         }
     }
     best = warp_min_u64(best);
-    if ((tid & 31) == 0) sh_min[tid >> 5] = best;
+    lim = __reduce_add_sync(0xffffffffu, lim);
+    faces = __reduce_add_sync(0xffffffffu, faces);
+    wet = __reduce_add_sync(0xffffffffu, wet);
+    mb = __reduce_min_sync(0xffffffffu, mb);
+    if ((tid & 31) == 0) {
+        sh_min[tid >> 5] = best;
+        sh_cnt[tid >> 5][0] = lim; sh_cnt[tid >> 5][1] = faces; sh_cnt[tid >> 5][2] = wet; sh_cnt[tid >> 5][3] = mb;
+    }
     __syncthreads();
     if (tid == 0) {
         unsigned long long bmin = kCflEmpty;
-        for (int w = 0; w < 8; ++w) bmin = sh_min[w] < bmin ? sh_min[w] : bmin;
+        uint32_t l = 0, f = 0, wt = 0, m2 = __float_as_uint(1.0f);
+        for (int w = 0; w < 8; ++w) {
+            bmin = sh_min[w] < bmin ? sh_min[w] : bmin;
+            l += sh_cnt[w][0]; f += sh_cnt[w][1]; wt += sh_cnt[w][2];
+            m2 = sh_cnt[w][3] < m2 ? sh_cnt[w][3] : m2;
+        }
         if (bmin != kCflEmpty) atomicMin(&c->cfl_packed, bmin);
+        if (l) {
+            atomicAdd(&c->limited_cells, l);
+            atomicMin(&c->min_scale_bits, m2);
+        }
+        if (f) atomicAdd(&c->limited_faces, f);
+        if (wt) atomicAdd(&c->wet, wt);
         __threadfence();
         const unsigned ticket = atomicAdd(&c->done_blocks, 1u);
         last = ticket == gridDim.x - 1;
@@ -547,6 +611,39 @@ int stream_grid(size_t n)
 
 // ------------------------------------------------------------------ planner
 
+// Rows per chunk, warps per block and resident warps per SM of the march.
+// A warp marches its rows after three rows of warm-up; chunks of 16 rows
+// measured fastest on the 4096 x 4096 grid (the many short strips keep
+// every SM busy to the end of a step), fewer rows when that would leave
+// fewer than two waves of blocks. NHF_LATTICE_ROWS, NHF_LATTICE_WARPS
+// (warps per block, 1..8) and NHF_LATTICE_BLOCKS (2, 3 or 4: 512, 768 or
+// 1024 resident threads per SM, the register budget) override the choice.
+static void lattice_shape(LatticePlan *P)
+{
+    // warps leave independently (no block barrier): small blocks free their
+    // slots as soon as their strips are done
+    const char *bw = getenv("NHF_LATTICE_WARPS");
+    const int warps = (bw && atoi(bw) >= 1 && atoi(bw) <= kWarps) ? atoi(bw) : 2;
+    const int per_row = (P->strips + warps - 1) / warps;  // blocks across the strips
+    P->block_warps = (P->strips + per_row - 1) / per_row;  // <= warps, as even as the strips allow
+    const char *occ = getenv("NHF_LATTICE_BLOCKS");
+    const int want = occ ? atoi(occ) : 0;
+    P->min_blocks = (want >= 2 && want <= 4) ? want : 4;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 148;
+    }
+    const long long waves2 = 2LL * sms * P->min_blocks * kWarps / P->block_warps;
+    const int need = P->ny + 1;
+    int rows = 16;
+    while (rows > 4 && (long long)((need + rows - 1) / rows) * per_row < waves2) rows /= 2;
+    const char *env = getenv("NHF_LATTICE_ROWS");
+    if (env && atoi(env) >= 1 && atoi(env) <= 256) rows = atoi(env);  // a lane's counters hold 10 bits
+    P->rows = rows;
+    P->chunks = (need + rows - 1) / rows;
+}
+
 int lattice_build(const Dev &d, cudaStream_t st, LatticeBuild *out, char *why, size_t why_len)
 {
     const nhf_mesh &m = d.m;
@@ -595,13 +692,15 @@ int lattice_build(const Dev &d, cudaStream_t st, LatticeBuild *out, char *why, s
     if ((double)nx * ny > 1.5 * (e - 1)) return no("lattice mostly empty");
     LatticePlan P{};
     P.nx = nx; P.ny = ny;
-    P.tiles_x = (nx + 1 + kTX - 1) / kTX;  // the tiles cover columns 0..nx and rows 0..ny
-    P.tiles_y = (ny + 1 + kTY - 1) / kTY;
-    P.lx = P.tiles_x * kTX + 4;
-    P.ly = P.tiles_y * kTY + 4;
+    // strips of 27 columns cover cell columns 0..nx (column nx: the east
+    // sides), chunks of P.rows rows cover cell rows 0..ny
+    P.strips = (nx + 1 + kOut - 1) / kOut;
+    lattice_shape(&P);
+    P.lx = P.strips * kOut + kWest + 2;
+    P.ly = P.chunks * P.rows + 5;  // 2 rows below, 3 above: the march loads a row ahead
     const size_t nl = (size_t)P.lx * P.ly;
     if (nl >= ((size_t)1 << 30)) return no("lattice too large");
-    auto at = [&](int i, int j) { return (size_t)(j + 2) * P.lx + (i + 2); };
+    auto at = [&](int i, int j) { return (size_t)(j + 2) * P.lx + (i + kWest); };
     std::vector<int32_t> cell(nl, 0), side_v(nl, 0), side_h(nl, 0), glat(e, 0), gside(s, 0);
     std::vector<uint8_t> live(nl, 0);
     for (int c = 1; c < e; ++c) {
@@ -672,9 +771,6 @@ int lattice_build(const Dev &d, cudaStream_t st, LatticeBuild *out, char *why, s
         return no("copy of the cell parameters failed");
     P.rain_cells = 0;
     P.horton = 0;
-    // resident blocks per SM of the step kernel (a tuning knob, default 2)
-    const char *occ = getenv("NHF_LATTICE_BLOCKS");
-    P.blocks_per_sm = (occ && atoi(occ) == 3) ? 3 : 2;
     for (int c = 1; c < e; ++c) {
         if (rain[c] != 0) P.rain_cells = 1;
         if (f0[c] != 0.0f || fc[c] != 0.0f || kk[c] != 0.0f) P.horton = 1;
@@ -693,6 +789,8 @@ int lattice_build(const Dev &d, cudaStream_t st, LatticeBuild *out, char *why, s
     size_t o_f0 = 0, o_fc = 0, o_k = 0;
     if (P.horton) { o_f0 = take(4 * nl); o_fc = take(4 * nl); o_k = take(4 * nl); }
     const size_t o_terms = take(4 * (size_t)d.terms * e), o_touch = take(4 * (size_t)d.blocks);
+    const size_t n_warps = (size_t)P.strips * P.chunks;
+    const size_t o_part = take(16 * n_warps), o_pcfl = take(8 * n_warps);
     char *mem = nullptr;
     if (cudaMalloc((void **)&mem, off)) { cudaGetLastError(); return no("no device memory for the lattice"); }
     out->device_memory = mem;
@@ -716,6 +814,10 @@ int lattice_build(const Dev &d, cudaStream_t st, LatticeBuild *out, char *why, s
         P.qv[k] = (real *)(mem + o_qv[k]);
         P.qh[k] = (real *)(mem + o_qh[k]);
     }
+    // the three pairs are allocated as h0 qv0 qh0 h1 qv1 qh1 of equal size
+    P.buffer_stride = (int32_t)(P.h[1] - P.h[0]);
+    if (P.qv[1] - P.qv[0] != P.buffer_stride || P.qh[1] - P.qh[0] != P.buffer_stride)
+        return no("lattice buffers not evenly spaced");
     P.z = (real *)(mem + o_z); P.nv = (real *)(mem + o_nv); P.nh = (real *)(mem + o_nh);
     P.bi = (int16_t *)(mem + o_bi);
     P.rain = P.rain_cells ? (int32_t *)(mem + o_rain) : nullptr;
@@ -725,6 +827,8 @@ int lattice_build(const Dev &d, cudaStream_t st, LatticeBuild *out, char *why, s
     if (P.horton) { P.f0 = (real *)(mem + o_f0); P.fc = (real *)(mem + o_fc); P.k = (real *)(mem + o_k); }
     P.terms = (float *)(mem + o_terms);
     P.touched = (uint32_t *)(mem + o_touch);
+    P.part = (uint32_t *)(mem + o_part);
+    P.part_cfl = (unsigned long long *)(mem + o_pcfl);
     Dev dd = d;
     dd.lat = P;
     k_lattice_setup<<<stream_grid(nl), 256, 0, st>>>(dd);
@@ -740,10 +844,15 @@ void lattice_enqueue_batch_start(const Dev &d, cudaStream_t s)
 
 void lattice_enqueue_step(const Dev &d, cudaStream_t s)
 {
-    if (d.lat.blocks_per_sm == 3) k_lattice_step<3><<<dim3(d.lat.tiles_x, d.lat.tiles_y), kNT, 0, s>>>(d);
-    else k_lattice_step<2><<<dim3(d.lat.tiles_x, d.lat.tiles_y), kNT, 0, s>>>(d);
-    int grid = std::max(1, std::min(148 * 8, (int)(((long long)(d.lat.nx + 1) * (d.lat.ny + 1) + 255) / 256)));
-    k_lattice_cfl<<<grid, 256, 0, s>>>(d);
+    const LatticePlan &P = d.lat;
+    const int per_block = (P.strips + P.block_warps - 1) / P.block_warps;
+    const dim3 grid(per_block, P.chunks), block(32 * P.block_warps);
+    if (P.min_blocks == 2) k_lattice_march<2><<<grid, block, 0, s>>>(d);
+    else if (P.min_blocks == 3) k_lattice_march<3><<<grid, block, 0, s>>>(d);
+    else k_lattice_march<4><<<grid, block, 0, s>>>(d);
+    const long long edges = (long long)P.strips * P.chunks * (P.rows + kOut);
+    const long long work = std::max<long long>(edges / 256, d.blocks / 8);
+    k_lattice_close<<<(int)std::max<long long>(1, std::min<long long>(148 * 8, work)), 256, 0, s>>>(d);
 }
 
 void lattice_enqueue_batch_end(const Dev &d, cudaStream_t s)

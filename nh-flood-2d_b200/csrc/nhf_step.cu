@@ -989,8 +989,10 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
 #ifdef NHF_REAL_DOUBLE
     h->path = "multipass (FP64 build)";
 #else
-    // Lattice form when the mesh is a uniform grid it covers (params->path 0 or 2).
-    if (params->path == 0 || params->path == 2) {
+    // Lattice form when the mesh is a uniform grid it covers (params->path 2,
+    // or 0 from 2^20 cells on: on smaller grids a march of a few rows is
+    // latency-bound and the tiled step is faster).
+    if (params->path == 2 || (params->path == 0 && mesh->e_num - 1 >= (1 << 20))) {
         Dev probe{};
         probe.m = *mesh;
         probe.terms = 4 + 6 * mesh->b_num;
@@ -1000,8 +1002,9 @@ int nhf_create(const nhf_mesh *mesh, const nhf_params *params, void *stream, nhf
         if (lattice_build(probe, h->s, &h->lb, why, sizeof(why)) == 0) {
             h->lattice = true;
             char buf[160];
-            snprintf(buf, sizeof(buf), "lattice(%dx%d,tiles=%dx%d)", h->lb.plan.nx, h->lb.plan.ny,
-                     h->lb.plan.tiles_x, h->lb.plan.tiles_y);
+            snprintf(buf, sizeof(buf), "lattice(%dx%d,strips=%d,rows=%d,warps=%d,blocks=%d)", h->lb.plan.nx,
+                     h->lb.plan.ny, h->lb.plan.strips, h->lb.plan.rows, h->lb.plan.block_warps,
+                     h->lb.plan.min_blocks);
             h->path = buf;
         } else {
             if (h->lb.device_memory) { cudaFree(h->lb.device_memory); h->lb.device_memory = nullptr; }

@@ -62,15 +62,67 @@ def device_bytes_bound(workload) -> int:
 class Request:
     id: int
     arrival: float                 # seconds after the session start
-    workload: object               # nhflood.workloads.Workload
+    workload: object               # nhflood.workloads.Workload, or a Future of one
     arrays: object = None          # its StepArrays, built on first need
     need: int = 0                  # device bytes estimate
+    cells: int = 0
+
+    def resolve(self):
+        """The workload, waiting for it if it is still being made."""
+        if hasattr(self.workload, 'result'):
+            self.workload = self.workload.result()
+        self.cells = self.workload.cells
+        return self.workload
 
     def prepare(self):
         if self.arrays is None:
-            self.arrays = self.workload.step_arrays()
+            self.arrays = self.resolve().step_arrays()
             self.need = device_bytes_estimate(self.arrays)
         return self.need
+
+    def release(self):
+        """Drop the host copies once a run holds what it needs."""
+        self.workload = None
+        self.arrays = None
+
+
+class MadeAhead:
+    """The workloads of a request stream, made by an executor (a process
+    pool) in arrival order and only ``ahead`` requests beyond the last one
+    taken, so that host memory holds a window of the stream, not all of it.
+    ``requests`` gives Request objects whose workload is a ticket that
+    waits for its own future when the server first needs it."""
+
+    def __init__(self, make, stream, executor, ahead: int = 32):
+        self.make, self.stream, self.executor, self.ahead = make, list(stream), executor, max(1, ahead)
+        self.futures = {}
+        self.submitted = 0
+        self._fill(0)
+
+    def _fill(self, upto: int) -> None:
+        while self.submitted < len(self.stream) and self.submitted < upto + self.ahead:
+            self.futures[self.submitted] = self.executor.submit(self.make, self.stream[self.submitted]['params'])
+            self.submitted += 1
+
+    def take(self, index: int):
+        self._fill(index + 1)
+        return self.futures.pop(index).result()
+
+    def wait_first(self) -> None:
+        """Block until the first window is made (before a timed session)."""
+        for f in list(self.futures.values()):
+            f.result()
+
+    def requests(self) -> list[Request]:
+        return [Request(r['id'], r['arrival'], _Ticket(self, i)) for i, r in enumerate(self.stream)]
+
+
+class _Ticket:
+    def __init__(self, source: MadeAhead, index: int):
+        self.source, self.index = source, index
+
+    def result(self):
+        return self.source.take(self.index)
 
 
 @dataclass
@@ -133,7 +185,7 @@ class FloodServer:
         started = 0
         while self.waiting:
             req = self.waiting[0]
-            need = device_bytes_bound(req.workload)
+            need = device_bytes_bound(req.resolve())
             if need > self.budget:
                 raise ValueError(f'request {req.id} needs {need} B, more than the whole budget')
             if self.used + need > self.budget:
@@ -154,7 +206,7 @@ class FloodServer:
                        else tiled_factory(self.tile, str(self.device)))
             run = PlainRun(req.workload, factory, batch_size=self.batch_size, arrays=req.arrays)
         self.side.synchronize()
-        req.arrays = None  # the engine holds the device copy
+        req.release()  # the run holds the workload, the engine the device copy
         return run
 
     def _join_built(self, wait: bool) -> None:
@@ -261,7 +313,8 @@ def serve_sequential(requests, *, tile: int = 256, batch_size: int = 32, device:
             if wait > 0:
                 time.sleep(wait)
         started = clock() - t0
-        run = PlainRun(req.workload, tiled_factory(tile, device, cfl='auto'), batch_size=batch_size)
+        run = PlainRun(req.resolve(), tiled_factory(tile, device, cfl='auto'), batch_size=batch_size)
+        req.release()
         while not run.done:
             run.advance()
         out.append(Completed(req.id, req.arrival, started, clock() - t0, run.w.cells, run.steps,

@@ -49,7 +49,7 @@ CASES = {
 
 def cuda_engine(path):
     """'auto': the form chosen for the mesh (the lattice form on uniform
-    grids of at least 1024 cells, else the fused tiled step, which keeps the
+    grids of at least 2^20 cells, else the fused tiled step, which keeps the
     CFL in the step on these small meshes); 'pass': the fused tiled step with
     the separate CFL pass; 'multipass': the reference's pass structure."""
     def factory(arrays, params):
@@ -214,6 +214,62 @@ def test_tile_1024_both_cfl_forms_bit_exact(cuda_available, cfl):
     assert runs[1].elapsed > 0
     for r in runs:
         r.close()
+
+
+@pytest.mark.parametrize('rows,blocks', [(None, None), ('4', '2'), ('7', '4'), ('16', '3')])
+def test_lattice_march_with_horton_rain_and_level_bit_exact(cuda_available, monkeypatch, rows, blocks):
+    """The lattice form on a 90 x 90 grid (strips of 28 columns and chunks
+    that do not divide it) with Horton infiltration on one land class, rain,
+    a level boundary and a 1 m wet start (donor limiting, flows
+    across strip and chunk edges): rows per chunk and resident blocks per
+    SM forced through the planner's knobs, so that strip and chunk edges
+    (whose CFL sides the close pass takes) cut through the wet area. Traces
+    and every state array equal the oracle's after each of 30 batches."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / 'oracle'))
+    from engine import OracleEngine
+    from nhflood.input import HortonInfiltration, LandParameters
+    from nhflood.model import STATE_F32, STATE_U32
+    from nhflood.native import CudaEngine
+    from nhflood.plain import PlainRun
+    from nhflood.workloads import plain_uniform_256
+    for key, value in (('NHF_LATTICE_ROWS', rows), ('NHF_LATTICE_BLOCKS', blocks)):
+        if value is None:
+            monkeypatch.delenv(key, raising=False)
+        else:
+            monkeypatch.setenv(key, value)
+
+    def cuda(arrays, params):
+        params.path = 'lattice'
+        engine = CudaEngine(arrays, params)
+        assert engine.path.startswith('lattice(90x90'), engine.path
+        if rows:
+            assert f'rows={rows},' in engine.path and f'blocks={blocks})' in engine.path, engine.path
+        return engine
+
+    w = plain_uniform_256(n=90)
+    w.land_parameters[1] = LandParameters(manning_n=0.03, infiltration=HortonInfiltration(
+        f0_mm_h=60.0, fc_mm_h=10.0, k_per_h=4.0))
+    depth = np.full(w.mesh.e_num, 1.0, np.float32)
+    depth[0] = 0.0
+    w.initial_depth = depth
+    runs = [PlainRun(w, lambda a, p: OracleEngine(a, p)), PlainRun(w, cuda)]
+    try:
+        for _ in range(30):
+            out = []
+            for r in runs:
+                tw, ow = r.begin()
+                out.append(r.engine.run_batch(tw, ow))
+                r.finish(out[-1])
+            np.testing.assert_array_equal(out[0], out[1])
+            for name in STATE_F32 + STATE_U32:
+                assert runs[0].engine.get(name).tobytes() == runs[1].engine.get(name).tobytes(), name
+        np.testing.assert_array_equal(runs[0].engine.budget_flush(), runs[1].engine.budget_flush())
+        assert (runs[1].engine.get('infiltration') > 0).any()
+    finally:
+        for r in runs:
+            r.close()
 
 
 @pytest.mark.parametrize('name,batches,path', [('multires_quadtree', 2, 'auto'), ('multires_quadtree_4m', 1, 'auto'),

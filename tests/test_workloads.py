@@ -119,3 +119,41 @@ def test_gated_polder_resolves_its_gates_and_opens_them_on_the_oracle():
     bed = run.engine.get('bed')
     assert np.all(bed[gate.targets] == np.float32(-1.0))
     run.close()
+
+
+def test_made_ahead_keeps_a_window_of_the_stream():
+    """Served-stream meshes are made in arrival order, at most ``ahead``
+    beyond the last one taken, and a request drops its host copies once a
+    run holds them."""
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+    from nhflood.serving import MadeAhead
+
+    made, lock = [], threading.Lock()
+
+    class Fake:
+        def __init__(self, cells):
+            self.cells = cells
+
+    def make(params):
+        with lock:
+            made.append(params['n'])
+        return Fake(params['n'] * 10)
+
+    stream = [{'id': i, 'arrival': 0.5 * i, 'params': {'n': i}} for i in range(20)]
+    with ThreadPoolExecutor(2) as ex:
+        source = MadeAhead(make, stream, ex, ahead=4)
+        source.wait_first()
+        assert sorted(made) == [0, 1, 2, 3]
+        reqs = source.requests()
+        assert [r.id for r in reqs] == list(range(20))
+        w = reqs[0].resolve()
+        assert w.cells == 0 and reqs[0].cells == 0
+        assert source.submitted == 5           # the window moved by one
+        assert reqs[6].resolve().cells == 60   # taking ahead of order fills up to it
+        assert source.submitted == 11
+        reqs[0].release()
+        assert reqs[0].workload is None and reqs[0].arrays is None
+        for r in reqs[1:6] + reqs[7:]:
+            assert r.resolve().cells == 10 * r.id
+    assert sorted(made) == list(range(20))
