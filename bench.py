@@ -74,11 +74,13 @@ def algorithmic_bytes(w):
     return b
 
 
-# DRAM bytes (read + write) of one fused step launch, from the ncu captures
-# summarised in profiles/ (k_step_tiled_<workload>.md).
+# DRAM bytes (read + write) of one step launch (the fused tiled step, or the
+# lattice march), from the ncu captures summarised in profiles/
+# (k_step_tiled_<workload>.md, k_lattice_march_dambreak.md).
 # Timed state (the bench's NVTX timed region); keyed by workload and step form.
 TRAFFIC_PER_LAUNCH = {('multires_quadtree', 'tiled'): 148.976896e6 + 20.993792e6,
-                      ('dambreak_4096', 'tiled'): 1022.048512e6 + 189.920512e6}
+                      ('dambreak_4096', 'tiled'): 1022.048512e6 + 189.920512e6,
+                      ('dambreak_4096', 'lattice'): 1025.505024e6 + 201.589504e6}
 
 
 def launches_per_batch(run) -> int:
@@ -527,10 +529,11 @@ def bench_served(args, rank, world, local):
     t_gen = time.perf_counter() - t0
     reqs = source.requests()
     # warm-up: one small request through both paths (module loads, first graph)
-    warm = [Request(-1, 0.0, _request_workload(dict(stream[0]['params'], width=1000.0, duration=60)))]
+    warm_workload = _request_workload(dict(stream[0]['params'], width=1000.0, duration=60))
+    warm = [Request(-1, 0.0, warm_workload)]
     server = FloodServer(hbm_budget=args.hbm_budget, tile=args.tile or 256, device=str(device))
     serve(warm, server, realtime=False)
-    serve_sequential([Request(-1, 0.0, warm[0].workload)], tile=args.tile or 256, device=str(device), realtime=False)
+    serve_sequential([Request(-1, 0.0, warm_workload)], tile=args.tile or 256, device=str(device), realtime=False)
     server = FloodServer(hbm_budget=args.hbm_budget, tile=args.tile or 256, device=str(device))
     with ClockSampler(local) as clocks:
         t0 = time.perf_counter()

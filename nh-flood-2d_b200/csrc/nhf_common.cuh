@@ -88,6 +88,8 @@ struct LatticePlan {
     uint32_t *touched;              // [blocks] terms some cell of a 256-cell budget block holds
     uint32_t *part;                 // [4][strips*chunks] per-warp limited cells, limited faces, wet cells, min scale bits
     unsigned long long *part_cfl;   // [strips*chunks] per-warp CFL key
+    float4 *edge_first;             // [strips][chunks*rows] first column: new depth, bed, west discharge, live
+    float2 *edge_last;              // [strips][chunks*rows] last column: new depth (-1: hole), bed
 };
 
 // Gate controller (core/gate.py:35-206): the caller's tables and controller

@@ -221,7 +221,7 @@ __device__ __forceinline__ void lattice_cfl(const Dev &d, real len, real q, real
 }
 
 // prepare_step (solver_compact.py:364-382) with the state in lattice order.
-__device__ void lattice_prepare(const Dev &d, Ctl *c)
+__device__ __noinline__ void lattice_prepare(const Dev &d, Ctl *c)
 {
     const nhf_mesh &m = d.m;
     const LatticePlan &P = d.lat;
@@ -365,6 +365,12 @@ __global__ void __launch_bounds__(kNT, kMinBlocks) k_lattice_march(const __grid_
             if (out0) {
                 if (l0 || lw0) P.qv[0][wr + L0] = fw0;
                 if (l0 || lm) P.qh[0][wr + L0] = fs0;
+                // the strip's edge cells for the close pass: the first column
+                // (new depth, bed, discharge of its west side, liveness) and
+                // the last (new depth, -1 for a hole, and bed)
+                const size_t e_at = (size_t)strip * P.chunks * P.rows + (y - 2);
+                if (lane == 2) P.edge_first[e_at] = make_float4(hn, z0, fw0, l0 ? 1.0f : 0.0f);
+                if (lane == 1 + kOut) P.edge_last[e_at] = make_float2(l0 ? hn : -1.0f, z0);
                 // interior sides both of whose cells this warp updated
                 if (l0 && lw0 && lane > 2) lattice_cfl(d, P.len_v, fw0, zw0, hnw, z0, hn, P.side_v, L0, best);
                 if (l0 && lm && y > y0) lattice_cfl(d, P.len_h, fs0, zm, hm, z0, hn, P.side_h, L0, best);
@@ -410,9 +416,10 @@ __global__ void __launch_bounds__(kNT, kMinBlocks) k_lattice_march(const __grid_
 // candidates (solver_compact.py:617-641) of the sides on strip and chunk
 // edges, whose two cells two different warps updated, and in the last block
 // to finish the commit of the step and the prepare of the next.
-__global__ void __launch_bounds__(256, 3) k_lattice_close(const __grid_constant__ Dev d)
+__global__ void __launch_bounds__(256, 6) k_lattice_close(const __grid_constant__ Dev d)
 {
     __shared__ double sh_tree[256];
+    __shared__ uint32_t sh_mask[256];
     __shared__ unsigned long long sh_min[8];
     __shared__ uint32_t sh_cnt[8][4];
     __shared__ bool last;
@@ -422,29 +429,38 @@ __global__ void __launch_bounds__(256, 3) k_lattice_close(const __grid_constant_
     const int tid = threadIdx.x;
     const size_t e = (size_t)m.e_num;
     const int T = d.terms;
-    for (int b = blockIdx.x; b < d.blocks; b += gridDim.x) {
-        const uint32_t mask = P.touched[b];
-        if (!mask) continue;
-        const int g = b * 256 + tid;
-        for (uint32_t rest = mask; rest; rest &= rest - 1) {
-            const int t = __ffs(rest) - 1;
-            float v = 0.0f;
-            if (g < m.e_num) {
-                v = P.terms[t * e + g];
-                if (v != 0.0f) P.terms[t * e + g] = 0.0f;
+    // an even share of the marks per block (at most 256 per round, one per
+    // thread); the block then takes the marked budget blocks one by one
+    const int per = min(256, (d.blocks + (int)gridDim.x - 1) / (int)gridDim.x);
+    for (int base = blockIdx.x * per; base < d.blocks; base += gridDim.x * per) {
+        const uint32_t mine = (tid < per && base + tid < d.blocks) ? P.touched[base + tid] : 0u;
+        sh_mask[tid] = mine;
+        if (!__syncthreads_or(mine != 0u)) continue;
+        for (int j = 0; j < per; ++j) {
+            const uint32_t mask = sh_mask[j];
+            if (!mask) continue;
+            const int b = base + j, g = b * 256 + tid;
+            for (uint32_t rest = mask; rest; rest &= rest - 1) {
+                const int t = __ffs(rest) - 1;
+                float v = 0.0f;
+                if (g < m.e_num) {
+                    v = P.terms[t * e + g];
+                    if (v != 0.0f) P.terms[t * e + g] = 0.0f;
+                }
+                const double sum = block_tree((double)v, sh_tree);
+                if (tid == 0) acc_add(d.acc_sum + (size_t)b * T + t, d.acc_comp + (size_t)b * T + t, sum);
             }
-            const double sum = block_tree((double)v, sh_tree);
-            if (tid == 0) acc_add(d.acc_sum + (size_t)b * T + t, d.acc_comp + (size_t)b * T + t, sum);
+            if (tid == 0) P.touched[b] = 0u;
         }
-        if (tid == 0) P.touched[b] = 0u;
+        __syncthreads();  // sh_mask is rewritten next round
     }
     const int active = c->active;
     unsigned long long best = kCflEmpty;
     uint32_t lim = 0, faces = 0, wet = 0, mb = __float_as_uint(1.0f);
     if (active) {
         // the march's per-warp counters and CFL minima
-        const long long W = (long long)P.strips * P.chunks;
-        for (long long w = (long long)blockIdx.x * 256 + tid; w < W; w += (long long)gridDim.x * 256) {
+        const int W = P.strips * P.chunks;
+        for (int w = blockIdx.x * 256 + tid; w < W; w += gridDim.x * 256) {
             lim += P.part[w];
             faces += P.part[W + w];
             wet += P.part[2 * W + w];
@@ -452,18 +468,23 @@ __global__ void __launch_bounds__(256, 3) k_lattice_close(const __grid_constant_
             best = P.part_cfl[w] < best ? P.part_cfl[w] : best;
         }
         const int p = c->parity ^ 1;  // the state the march just wrote
-        const real *h = P.h[p], *qv = P.qv[p], *qh = P.qh[p];
+        const real *h = P.h[p], *qh = P.qh[p];
         const size_t lx = (size_t)P.lx;
-        const long long rows = (long long)P.chunks * P.rows, cols = (long long)P.strips * kOut;
-        const long long n_west = (long long)P.strips * rows, n = n_west + (long long)P.chunks * cols;
-        for (long long i = (long long)blockIdx.x * 256 + tid; i < n; i += (long long)gridDim.x * 256) {
-            if (i < n_west) {  // west side of the first column of a strip
-                const long long s = i / rows, y = 2 + i % rows;
-                const size_t L = (size_t)y * lx + (size_t)(s * kOut + 2);
-                if (P.live[L] && P.live[L - 1])
-                    lattice_cfl(d, P.len_v, qv[L], P.z[L - 1], h[L - 1], P.z[L], h[L], P.side_v, L, best);
+        // counts below 2^31: the planner keeps the lattice under 2^30 points
+        const int rows = P.chunks * P.rows, cols = P.strips * kOut;
+        const int n_west = P.strips * rows, n = n_west + P.chunks * cols;
+        for (int i = blockIdx.x * 256 + tid; i < n; i += gridDim.x * 256) {
+            if (i < n_west) {  // west side of the first column of a strip, from the march's edge records
+                const int s = i / rows, y = i % rows;
+                if (s == 0) continue;  // west of strip 0: the border
+                const float4 r = P.edge_first[i];
+                const float2 l = P.edge_last[i - rows];
+                if (r.w != 0.0f && l.x >= 0.0f) {
+                    const size_t L = (size_t)(y + 2) * lx + (size_t)(s * kOut + 2);
+                    lattice_cfl(d, P.len_v, r.z, l.y, l.x, r.y, r.x, P.side_v, L, best);
+                }
             } else {  // south side of the first row of a chunk
-                const long long k = i - n_west, ch = k / cols, x = 2 + k % cols;
+                const int k = i - n_west, ch = k / cols, x = 2 + k % cols;
                 const size_t L = (size_t)(2 + ch * P.rows) * lx + (size_t)x;
                 if (P.live[L] && P.live[L - lx])
                     lattice_cfl(d, P.len_h, qh[L], P.z[L - lx], h[L - lx], P.z[L], h[L], P.side_h, L, best);
@@ -791,6 +812,8 @@ int lattice_build(const Dev &d, cudaStream_t st, LatticeBuild *out, char *why, s
     const size_t o_terms = take(4 * (size_t)d.terms * e), o_touch = take(4 * (size_t)d.blocks);
     const size_t n_warps = (size_t)P.strips * P.chunks;
     const size_t o_part = take(16 * n_warps), o_pcfl = take(8 * n_warps);
+    const size_t n_edge = (size_t)P.strips * P.chunks * P.rows;
+    const size_t o_efirst = take(16 * n_edge), o_elast = take(8 * n_edge);
     char *mem = nullptr;
     if (cudaMalloc((void **)&mem, off)) { cudaGetLastError(); return no("no device memory for the lattice"); }
     out->device_memory = mem;
@@ -829,6 +852,8 @@ int lattice_build(const Dev &d, cudaStream_t st, LatticeBuild *out, char *why, s
     P.touched = (uint32_t *)(mem + o_touch);
     P.part = (uint32_t *)(mem + o_part);
     P.part_cfl = (unsigned long long *)(mem + o_pcfl);
+    P.edge_first = (float4 *)(mem + o_efirst);
+    P.edge_last = (float2 *)(mem + o_elast);
     Dev dd = d;
     dd.lat = P;
     k_lattice_setup<<<stream_grid(nl), 256, 0, st>>>(dd);
