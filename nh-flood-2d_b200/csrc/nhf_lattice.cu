@@ -3,29 +3,33 @@
 // A uniform NE/NS mesh (one cell size, one side length per orientation,
 // one side per face) is a 2-D lattice whatever its numbering. The planner
 // below recognises it from the mesh tables and numbers it into a padded
-// lattice: a border of holes (3 columns west, 2 rows south) and padding up
-// to whole strips of 27 columns and chunks of rows. During a batch the
-// library keeps its own lattice-ordered copies of the state (depth and side
-// discharges double-buffered, rain time, infiltration, extrema), gathered
-// from the caller's arrays at the batch start and scattered back at its
-// end. Inside the batch every neighbour is found by arithmetic: no index
-// tables, rows of 32 cells per warp, coalesced loads.
+// lattice: a border of holes (2 columns west, 2 rows south) and padding up
+// to whole strips of 28 columns and chunks of rows (3 rows above the last
+// chunk). During a batch the library keeps its own lattice-ordered copies
+// of the state (depth and side discharges double-buffered, rain time,
+// infiltration, extrema), gathered from the caller's arrays at the batch
+// start and scattered back at its end. Inside the batch every neighbour is
+// found by arithmetic: no index tables, rows of 32 cells per warp,
+// coalesced loads.
 //
 // One step is two launches. k_lattice_march: each warp marches up a strip
 // of the lattice with the rows it needs in registers and does, row by row,
 // what the reference's passes do (solver_compact.py:439-641): momentum q*,
 // donor factors, final discharges, sources and depth update, extrema,
-// budget terms and the CFL candidate of the new state; the last block to
-// finish commits the step and prepares the next one. k_lattice_budget: the
-// canonical 256-cell budget trees of the blocks the step touched. Each
-// quantity is computed in the reference's operation order with the same
-// expressions as the tiled and multi-pass steps, so the three forms and the
-// CPU restatement agree bit for bit.
+// budget terms and the CFL candidates of the sides inside its strip and
+// chunk; it writes its counters, its CFL minimum and its edge columns to
+// per-warp records. k_lattice_close: those records, the CFL candidates of
+// the sides on strip and chunk edges, the canonical 256-cell budget trees
+// of the blocks the step touched, and in its last block the commit of the
+// step and the prepare of the next. Each quantity is computed in the
+// reference's operation order with the same expressions as the tiled and
+// multi-pass steps, so the three forms and the CPU restatement agree bit
+// for bit.
 //
 // Budget terms are sums over the reference's 256-cell blocks of global ids
-// (ei // 256), which a lattice strip does not follow: the step writes each
+// (ei // 256), which a lattice strip does not follow: the march writes each
 // nonzero per-cell term into a scratch array by global id and marks its
-// block; the budget pass reduces the marked blocks with the canonical tree
+// block; the close pass reduces the marked blocks with the canonical tree
 // and clears them.
 #include <cuda_runtime.h>
 
@@ -713,7 +717,7 @@ int lattice_build(const Dev &d, cudaStream_t st, LatticeBuild *out, char *why, s
     if ((double)nx * ny > 1.5 * (e - 1)) return no("lattice mostly empty");
     LatticePlan P{};
     P.nx = nx; P.ny = ny;
-    // strips of 27 columns cover cell columns 0..nx (column nx: the east
+    // strips of 28 columns cover cell columns 0..nx (column nx: the east
     // sides), chunks of P.rows rows cover cell rows 0..ny
     P.strips = (nx + 1 + kOut - 1) / kOut;
     lattice_shape(&P);
