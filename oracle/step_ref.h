@@ -18,7 +18,7 @@
  * pinned bit for bit to the reference's own code by the golden vectors in
  * tests/golden/ (tests/test_golden_host.py).
  *
- * Differences from the reference that are deliberate (north-star design):
+ * Differences from the reference that are deliberate (this design's choices):
  *  - budget diagnostics are accumulated as FP64 per-block partials
  *    (fixed pairwise tree inside each 256-cell block, then TwoSum
  *    compensation across steps) instead of exact base-65536 integer digits
