@@ -148,13 +148,19 @@ class Completed:
 
 class FloodServer:
     def __init__(self, *, hbm_budget: float = 150e9, tile: int = 256, grid_blocks: int = -2,
-                 batch_size: int = 32, device: str = 'cuda:0', clock=None):
+                 batch_size: int = 32, device: str = 'cuda:0', clock=None, engine_factory=None,
+                 ensemble_factory=None):
+        """engine_factory(arrays, params) and ensemble_factory(engines,
+        grid_blocks) replace the CUDA step and CudaEnsemble (the scheduling
+        logic's CPU tests pass the CPU restatement and a sequential stand-in);
+        a device that is not CUDA gets no side stream."""
         import torch
         self.torch = torch
         self.device = torch.device(device)
         self.budget = float(hbm_budget)
         self.tile, self.grid_blocks, self.batch_size = tile, grid_blocks, batch_size
-        self.side = torch.cuda.Stream(self.device)
+        self.engine_factory, self.ensemble_factory = engine_factory, ensemble_factory
+        self.side = torch.cuda.Stream(self.device) if self.device.type == 'cuda' else None
         self.waiting: deque[Request] = deque()
         self.building: deque = deque()  # (request, future of its PlainRun, bytes reserved)
         self.builder = ThreadPoolExecutor(max_workers=1, thread_name_prefix='nhflood-build')
@@ -199,13 +205,16 @@ class FloodServer:
 
     def _build(self, req):
         """Builder thread: the solve's arrays, upload and plan on the side stream."""
-        with self.torch.cuda.device(self.device), self.torch.cuda.stream(self.side):
-            # member graphs (grid_blocks -2): the plain form's own step choice;
-            # one launch: the fused step with the server's tile size
-            factory = (plain_factory(str(self.device)) if self.grid_blocks == MEMBER_GRAPHS
-                       else tiled_factory(self.tile, str(self.device)))
+        # member graphs (grid_blocks -2): the plain form's own step choice;
+        # one launch: the fused step with the server's tile size
+        factory = self.engine_factory or (plain_factory(str(self.device)) if self.grid_blocks == MEMBER_GRAPHS
+                                          else tiled_factory(self.tile, str(self.device)))
+        if self.side is None:
             run = PlainRun(req.workload, factory, batch_size=self.batch_size, arrays=req.arrays)
-        self.side.synchronize()
+        else:
+            with self.torch.cuda.device(self.device), self.torch.cuda.stream(self.side):
+                run = PlainRun(req.workload, factory, batch_size=self.batch_size, arrays=req.arrays)
+            self.side.synchronize()
         req.release()  # the run holds the workload, the engine the device copy
         return run
 
@@ -243,7 +252,8 @@ class FloodServer:
         if self.dirty or self.ensemble is None:
             if self.ensemble is not None:
                 self.ensemble.close()
-            self.ensemble = CudaEnsemble([run.engine for _, run, _, _ in self.active], self.grid_blocks)
+            make = self.ensemble_factory or CudaEnsemble
+            self.ensemble = make([run.engine for _, run, _, _ in self.active], self.grid_blocks)
             self.dirty = False
         return self.ensemble
 
@@ -301,7 +311,7 @@ def serve(requests, server: FloodServer, realtime: bool = True) -> list[Complete
 
 
 def serve_sequential(requests, *, tile: int = 256, batch_size: int = 32, device: str = 'cuda:0',
-                     realtime: bool = True, clock=None) -> list[Completed]:
+                     realtime: bool = True, clock=None, engine_factory=None) -> list[Completed]:
     """The plain form, one solve at a time in arrival order (the baseline of
     the served form): each request waits for the previous one to finish."""
     clock = clock or time.perf_counter
@@ -313,7 +323,7 @@ def serve_sequential(requests, *, tile: int = 256, batch_size: int = 32, device:
             if wait > 0:
                 time.sleep(wait)
         started = clock() - t0
-        run = PlainRun(req.resolve(), tiled_factory(tile, device, cfl='auto'), batch_size=batch_size)
+        run = PlainRun(req.resolve(), engine_factory or tiled_factory(tile, device, cfl='auto'), batch_size=batch_size)
         req.release()
         while not run.done:
             run.advance()
