@@ -55,7 +55,12 @@ class EnsembleRun:
     the member graphs."""
 
     def __init__(self, workloads, *, tile: int | None = None, grid_blocks: int | None = None,
-                 batch_size: int = 32, device: str = 'cuda:0', tuning_cache=None, tune: bool = False):
+                 batch_size: int = 32, device: str = 'cuda:0', tuning_cache=None, tune: bool = False,
+                 engine_factory=None, ensemble_factory=None):
+        """engine_factory(arrays, params) and ensemble_factory(engines,
+        grid_blocks) replace the schedule's CUDA engines and CudaEnsemble
+        (the CPU tests of the batching logic pass the CPU restatement and a
+        sequential stand-in)."""
         self.workloads = list(workloads)
         self.tuned = None
         if tile is None and grid_blocks is None and tune:
@@ -77,9 +82,10 @@ class EnsembleRun:
                 grid_blocks = tuned.grid if grid_blocks is None else grid_blocks
             factory = tiled_factory(tile, device)
         self.tile, self.grid_blocks = tile, grid_blocks
+        factory = engine_factory or factory
         self.runs = [PlainRun(w, factory, batch_size=batch_size) for w in self.workloads]
         try:
-            self.ensemble = CudaEnsemble([r.engine for r in self.runs], grid_blocks)
+            self.ensemble = (ensemble_factory or CudaEnsemble)([r.engine for r in self.runs], grid_blocks)
         except Exception:
             for r in self.runs:
                 r.close()

@@ -18,6 +18,30 @@ def oracle_factory(arrays, params):
     return OracleEngine(arrays, params)
 
 
+class SequentialEnsemble:
+    """The ensemble launch's contract on CPU engines, one member after
+    another: a batch of every member from its own target and origin words,
+    one trace per member (what CudaEnsemble returns)."""
+
+    def __init__(self, engines, grid_blocks=None):
+        self.engines = list(engines)
+        self.members = len(self.engines)
+        self.rows = None
+
+    def run_batch_async(self, targets, origins):
+        self.rows = [e.run_batch(t, o) for e, t, o in zip(self.engines, targets, origins)]
+
+    def read_trace(self):
+        return self.rows
+
+    def run_batch(self, targets, origins):
+        self.run_batch_async(targets, origins)
+        return self.read_trace()
+
+    def close(self):
+        self.engines = []
+
+
 def cuda_factory(arrays, params):
     from nhflood.native import CudaEngine
     return CudaEngine(arrays, params)

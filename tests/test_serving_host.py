@@ -8,25 +8,6 @@ import numpy as np
 import pytest
 
 
-class SequentialEnsemble:
-    """The ensemble launch's contract, one member after another: a batch of
-    every member from its own target and origin words, traces per member."""
-
-    def __init__(self, engines, grid_blocks):
-        self.engines = list(engines)
-        self.members = len(self.engines)
-        self.rows = None
-
-    def run_batch_async(self, targets, origins):
-        self.rows = [e.run_batch(t, o) for e, t, o in zip(self.engines, targets, origins)]
-
-    def read_trace(self):
-        return self.rows
-
-    def close(self):
-        self.engines = []
-
-
 def requests():
     from nhflood.serving import Request
     from nhflood.workloads import multires_quadtree, plain_uniform_256
@@ -39,7 +20,7 @@ def requests():
 
 def server(budget, resident=None):
     from nhflood.serving import FloodServer
-    from runner import oracle_factory
+    from runner import SequentialEnsemble, oracle_factory
     s = FloodServer(hbm_budget=budget, device='cpu', engine_factory=oracle_factory,
                     ensemble_factory=SequentialEnsemble)
     if resident is not None:
